@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the SOP Langevin step on B200.
+
+Workload (default, one GPU): the ragged batch of 512 independent replicas,
+sizes log-normal in [60, 600] beads (seeded), each a synthetic globular chain
+with its own native map and RNG seed, force-clamp at U(100, 300) pN, pairlist
+every 10 steps at 20 A, FP32, no HI.  One bench "step" is `--chunk` Langevin
+steps of the whole batch (one pass of the resident kernel).  The plain path
+(one 200-bead force-ramp job at a time, same kernels) is measured beside it.
+
+Metric: bead-steps/s (sum over jobs of N_job x steps / s).  value: device
+time (CUDA events on the launching stream) with state resident in HBM and L2
+flushed between timed iterations; e2e: the same through the C ABI with the
+coordinates uploaded from pinned host memory and downloaded back every step.
+
+Multi-GPU: replicas only -- every rank advances its own batch, no collective
+on the data path; the time is the max over ranks and value is the total.
+
+--impl reference: the reference's step math on the host cores (the CPU
+restatement in oracle/, OpenMP over jobs), same workload, bounded sample.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for sub in ("sop-gpu_b200", "oracle"):
+    sys.path.insert(0, os.path.join(REPO, sub))
+
+import numpy as np  # noqa: E402
+
+METRIC = "bead-steps/s (batched ragged 512-replica stream)"
+UNIT = "bead-steps/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def plain_params(**kw):
+    import sopb
+    base = dict(timestep=0.08, zeta=50.0, temperature=0.6, pairs_freq=10, pairlist_cutoff=20.0, pairs_cutoff=20.0,
+                pairs_threshold=200.0, nav=1000)
+    base.update(kw)
+    return sopb.default_params(**base)
+
+
+def batch_specs(count=512, lo=60, hi=600, seed=2024, rank=0):
+    """The ragged force-clamp batch (one independent copy per rank)."""
+    import sopb
+    import sopb_synth as S
+    base = seed + 7919 * rank
+    sizes = S.lognormal_sizes(count, lo, hi, base)
+    rng = np.random.default_rng(base + 1)
+    f_pn = rng.uniform(100.0, 300.0, count)
+    specs = []
+    for k, n in enumerate(sizes):
+        n = int(n)
+        s = S.make_system(n, base * 1000 + k)
+        p = plain_params(pulling=1, fconst=float(f_pn[k] / 70.0), fixedEnd=0, pulledEnd=n - 1)
+        specs.append(sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[n - 1], seed=1119727 + k))
+    return specs
+
+
+def plain_spec(seed=2024):
+    """One 200-bead force-ramp pull: first bead fixed, last pulled."""
+    import sopb
+    import sopb_synth as S
+    s = S.make_system(200, seed)
+    p = plain_params(pulling=1, deltax=0.5, k_trans=0.05, pullFreq=1000, fixedEnd=0, pulledEnd=199)
+    return sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[199], seed=1119727)
+
+
+def list_stats(jobs, specs):
+    """Mean per-bead list lengths (for the algorithmic-bytes model)."""
+    tot = nb = nn = npl = npp = 0
+    for j, sp in zip(jobs, specs):
+        c_pl, _ = j.pairlist(False, cap=1)
+        c_pp, _ = j.pairlist(True, cap=1)
+        tot += sp.n
+        nb += 2 * sp.bonds.shape[0]
+        nn += 2 * sp.natives.shape[0]
+        npl += int(c_pl.sum())
+        npp += int(c_pp.sum())
+    return dict(beads=tot, n_bond=nb / tot, n_native=nn / tot, n_pair=npl / tot, n_possible=npp / tot)
+
+
+def alg_bytes_per_bead_step(st, pairs_freq):
+    # compulsory traffic of the reference data model per bead-step:
+    # coords r+w, RNG state r+w, ext-force/flag read, bond (int+float),
+    # native (int + 2 floats), pair index, and the amortised rebuild
+    # (possible-pair index read + pair index write per pairs_freq steps)
+    return (32 + 32 + 16 + 8 * st["n_bond"] + 12 * st["n_native"] + 4 * st["n_pair"]
+            + (4 * st["n_possible"] + 4 * st["n_pair"]) / pairs_freq)
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for l in self.lines:
+            t = [x.strip() for x in l.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                mx = float(t[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), t[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU restatement on the host cores
+# ---------------------------------------------------------------------------
+def cpu_rate(specs, target_s=10.0, nthreads=0):
+    """bead-steps/s of the oracle on the host cores over a bounded sample."""
+    import oracle_py as O
+    jobs = [O.OracleJob(sp) for sp in specs]
+    beads = sum(sp.n for sp in specs)
+    threads = nthreads or os.cpu_count()
+    t0 = time.perf_counter()
+    O.jobs_advance(jobs, 10, threads)      # includes the step-0 list builds
+    probe = time.perf_counter() - t0
+    steps = max(10, int(target_s / max(probe / 10, 1e-9)))
+    steps = min(steps, 5000)
+    t0 = time.perf_counter()
+    O.jobs_advance(jobs, steps, threads)
+    dt = time.perf_counter() - t0
+    for j in jobs:
+        j.close()
+    return beads * steps / dt, threads, "%d jobs (%d beads) x %d steps" % (len(specs), beads, steps)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    specs = batch_specs(rank=0)
+    threads = os.cpu_count()
+    vals = []
+    sample = ""
+    for k in range(args.warmup + args.steps):
+        v, threads, sample = cpu_rate(specs, target_s=args.ref_seconds, nthreads=threads)
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded globular chains)",
+        "config": {"workload": "batch512_lognormal_60-600_clamp", "replicas": len(specs), "pairs_freq": 10},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+    import sopb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = sopb.Context(dev, stream=stream.cuda_stream)
+
+    t0 = time.perf_counter()
+    specs = batch_specs(rank=rank)
+    log("rank %d: generated %d systems in %.1fs" % (rank, len(specs), time.perf_counter() - t0))
+    jobs = [ctx.job(sp) for sp in specs]
+    beads = sum(sp.n for sp in specs)
+    chunk = args.chunk
+    classes = sorted({j.shape()[1] for j in jobs})
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
+
+    def one(n=chunk):
+        ctx.run(jobs, n)
+
+    # warm-up (also builds the lists at step 0)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            one()
+    ctx.sync()
+    stats = list_stats(jobs, specs)
+    for j in jobs:
+        if j.status() != 0:
+            raise RuntimeError("job failed during warm-up: status %d" % j.status())
+
+    # timed: device events around each chunk, L2 flushed in between
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                starts[k].record(stream)
+                one()
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(ms)
+    if dist:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    bead_steps = beads * chunk * args.steps
+    value = world * bead_steps / (total_ms / 1e3)
+    launches = len(classes) * args.steps
+
+    # e2e through the C ABI with host buffers
+    host = torch.empty((beads, 4), dtype=torch.float32, pin_memory=True)
+    host_np = host.numpy()
+    ctx.download_coords(jobs, host_np)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        ctx.upload_coords(jobs, host_np)
+        one()
+        ctx.download_coords(jobs, host_np)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * bead_steps / e2e_s
+    for j in jobs:
+        if j.status() != 0:
+            raise RuntimeError("job failed: status %d" % j.status())
+
+    # plain path: one 200-bead job alone, same kernels
+    plain = None
+    if rank == 0:
+        pj = ctx.job(plain_spec())
+        with torch.cuda.stream(stream):
+            ctx.run([pj], 1000)
+        ctx.sync()
+        pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        psteps = 20000
+        with torch.cuda.stream(stream):
+            pe0.record(stream)
+            ctx.run([pj], psteps)
+            pe1.record(stream)
+        torch.cuda.synchronize()
+        pms = pe0.elapsed_time(pe1)
+        plain = {"workload": "plain_200bead_ramp", "value": 200 * psteps / (pms / 1e3), "unit": UNIT,
+                 "steps": psteps, "ms": pms}
+        pj.destroy()
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        bps = alg_bytes_per_bead_step(stats, 10)
+        avg_launch_s = (total_ms / 1e3) / args.steps
+        achieved = bps * beads * chunk / avg_launch_s / 1e9
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            sample = specs[:: max(1, len(specs) // 64)]
+            v, cores, desc = cpu_rate(sample, target_s=args.ref_seconds)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": "CPU restatement, OpenMP over jobs: " + desc}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded globular chains; no public dataset)",
+            "config": {"workload": "batch512_lognormal_60-600_clamp", "replicas": len(specs), "beads": beads,
+                       "langevin_steps_per_step": chunk, "pairs_freq": 10, "pairlist_cutoff_A": 20.0,
+                       "dt_tauH": 0.08, "parallelism": "replicas-dp%d" % world, "l2": "flushed between timed steps"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": beads * 16, "d2h_bytes_per_step": beads * 16},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "alg_bytes_per_bead_step": bps, "lists": stats},
+            "plain": plain,
+            "batched_over_plain": value / plain["value"] if plain else None,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--chunk", type=int, default=200, help="Langevin steps per bench step")
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

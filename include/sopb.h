@@ -1,0 +1,259 @@
+/*
+ * sopb.h — C ABI of the B200-native SOP Langevin step.
+ *
+ * This is the drop-in boundary for SOP-GPU's hot path: the overdamped
+ * Langevin step of the SOP C-alpha model (FENE bonds, native LJ 12-6,
+ * repulsive r^-6 pairs, possible-pairs and Verlet pairlist rebuilds, the
+ * Ermak-McCammon integrator with Hybrid Taus noise, force-ramp/force-clamp
+ * pulling, continuous-surface nanoindentation and RPY hydrodynamic noise by
+ * TEA or Cholesky).  Every entry point is plain C: pointers, sizes and int
+ * status codes; no CUDA or torch types appear in any signature.  A CUDA
+ * stream may be passed as an opaque pointer.
+ *
+ * Reference interfaces replaced (paths inside the SOP-GPU source tree):
+ *   - SOPPotential / SOPUpdater / SOPIntegrator and the time loop
+ *       src/gsop.h:69-105, src/gsop.cu:111-163
+ *   - per-plugin device maps uploaded by constructors
+ *       src/Potentials/covalent.cu:86-121, src/Potentials/native.cu:73-110,
+ *       src/Updaters/pairlist.cu:60-128, src/Integrators/ht.cu:29-56
+ *   - DIE()/exit(-1) error handling (src/Util/wrapper.cpp:28-42) becomes
+ *     status codes; nothing in the library exits the process.
+ *
+ * Threading: a context is used from one host thread at a time.  All work on
+ * a context is ordered on the context's stream.
+ */
+#ifndef SOPB_H
+#define SOPB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOPB_ABI_VERSION 1
+
+/* Status codes.  The reference DIE()s on each of these conditions. */
+enum {
+    SOPB_OK = 0,
+    SOPB_ERR_INVALID = 1,     /* bad argument or configuration               */
+    SOPB_ERR_CAPACITY = 2,    /* a neighbour list outgrew its capacity        */
+    SOPB_ERR_NONFINITE = 3,   /* a coordinate became NaN or Inf               */
+    SOPB_ERR_CUDA = 4,        /* CUDA runtime error                           */
+    SOPB_ERR_TIMEOUT = 5,     /* a bounded device wait ran out                */
+    SOPB_ERR_NOMEM = 6,       /* device arena exhausted                       */
+    SOPB_ERR_UNSUPPORTED = 7, /* feature combination not supported            */
+    SOPB_ERR_HI = 8,          /* TEA "capricious" abort (epsilon > 1 etc.)    */
+    SOPB_ERR_NODEVICE = 9     /* no CUDA device or library built without one  */
+};
+
+/* Pull direction (src/Potentials/pulling.h:21). */
+enum { SOPB_PULL_END_TO_END = 0, SOPB_PULL_VECTOR = 1 };
+
+/* HI noise treatment for hi_exact (src/Integrators/bdhitea_kernel.cu:303-361). */
+enum {
+    SOPB_HI_B_CHOLESKY = 0,   /* B = L, the true Cholesky factor of D         */
+    SOPB_HI_B_REFCOMPAT = 1   /* the reference's symmetrised upper 3x3 blocks */
+};
+
+/*
+ * Simulation parameters of one job.  Field names are the reference's config
+ * keys (same meaning, same units: A, kcal/mol, tau_H).  sopb_default_params()
+ * fills the reference defaults; mandatory keys without a default are zero.
+ */
+typedef struct sopb_params {
+    /* Integrators/langevin.h:12-23 */
+    float timestep;            /* h (mandatory)                               */
+    float zeta;                /* 50                                           */
+    float temperature;         /* 0.6                                          */
+    int32_t minimization;      /* 0: no random force when 1                    */
+    int32_t heating;           /* TemperatureUpdater on/off                    */
+    float initialT;
+    float deltaT;
+    int32_t tempFreq;
+    /* Potentials/covalent.h:12-14 */
+    float kspring_cov;         /* 20                                           */
+    float R_limit;             /* 2                                            */
+    /* Potentials/pairs.h:12-15 */
+    float a;                   /* 3.8                                          */
+    float el;                  /* 1                                            */
+    float pairs_cutoff;        /* 20: force cutoff                             */
+    /* Updaters/pairlist.h:12-14, Updaters/possiblepairlist.h:12-13 */
+    float pairlist_cutoff;     /* 20: Verlet list cutoff                       */
+    int32_t pairs_freq;        /* 1000                                         */
+    float pairs_threshold;     /* 200: possible-pairs cutoff                   */
+    int32_t possiblepairs_freq;/* 100000                                       */
+    int32_t max_pairs;         /* capacity of a bead's Verlet row (512)        */
+    int32_t max_possiblePairs; /* capacity of a bead's possible-pairs row      */
+    /* loop: gsop.h:34, gsop.cu:117-122 */
+    int32_t nav;               /* 1000                                         */
+    int32_t stride;            /* updater period; 0 = min(nav, frequencies)    */
+    /* Potentials/pulling.h:15-26 */
+    int32_t pulling;
+    float deltax;              /* cantilever speed per pullFreq steps          */
+    float k_trans;             /* 0.05                                         */
+    float fconst;              /* force-clamp magnitude                        */
+    int32_t pullFreq;          /* defaults to nav                              */
+    int32_t pull_direction;    /* SOPB_PULL_*                                  */
+    float pullVector[3];
+    int32_t fixedEnd;
+    int32_t pulledEnd;
+    /* Potentials/indentation.h:12-38 (continuous surface) */
+    int32_t indentation;
+    float indentationChip[3];
+    float indentationTip[3];
+    float indentationDirection[3];
+    float indentationSurfaceR0[3];
+    float indentationSurfaceN[3];
+    float indentationTipR;
+    float indentationKs;
+    float indentationDeltaX;
+    int32_t indentationMoveSurface;
+    int32_t indentationFixTrans;
+    float indentationTipSigma, indentationTipEl, indentationTipA, indentationTipB;
+    float indentationSurfSigma, indentationSurfEl, indentationSurfA, indentationSurfB;
+    float indentationTipZeta;  /* 5000                                         */
+    int64_t indentationRetractionStep; /* -1                                   */
+    /* Integrators/bdhitea.h:15-21 */
+    int32_t hi_on;
+    int32_t hi_exact;
+    float hi_a;                /* 1.8                                          */
+    int32_t hi_epsilon_freq;
+    int32_t hi_capricious;     /* 1                                            */
+    int32_t hi_unlisted;       /* 1                                            */
+    float hi_epsmax;           /* 999                                          */
+    /* keys added by this library (do not change the meaning of old ones) */
+    int32_t hi_b_mode;         /* SOPB_HI_B_*; default SOPB_HI_B_CHOLESKY      */
+    int32_t hi_refresh;        /* refactor D every k steps (reference: 1)      */
+    int32_t lanes_per_bead;    /* 0 = autotuned                                */
+    int32_t reserved[7];
+} sopb_params;
+
+/*
+ * One job: a single SOP chain system (one "trajectory" of the reference).
+ * Indices are 0-based bead numbers local to the job, as in the .top file.
+ */
+typedef struct sopb_job_desc {
+    int32_t n;                         /* beads                               */
+    const float* xyz;                  /* [3n] coordinates, A                 */
+    int32_t nbonds;
+    const int32_t* bonds;              /* [2*nbonds] (i, j) in .top order     */
+    const float* bonds_r0;             /* [nbonds]                            */
+    int32_t nnatives;
+    const int32_t* natives;            /* [2*nnatives] (i, j)                 */
+    const float* natives_r0;           /* [nnatives]                          */
+    const float* natives_eh;           /* [nnatives]                          */
+    int32_t nfixed;
+    const int32_t* fixed;              /* pulling 'fixed' bead list           */
+    int32_t npulled;
+    const int32_t* pulled;             /* pulling 'pulled' bead list          */
+    const uint32_t* seeds;             /* [4n] Hybrid Taus states, or NULL    */
+    int32_t seed;                      /* used when seeds == NULL             */
+    int32_t reserved;
+    sopb_params params;
+} sopb_job_desc;
+
+typedef struct sopb_context sopb_context;
+typedef struct sopb_job sopb_job;
+
+/* Quantities readable from / writable to a job (sopb_job_read/_write). */
+enum {
+    SOPB_COORDS = 0,   /* float[4n]  x y z w, w = 0 (gsop.d_coord)           */
+    SOPB_SEEDS = 1,    /* uint32[4n] Hybrid Taus states (ht.d_seeds)         */
+    SOPB_TEMP = 2,     /* float[n]   kinetic temperature accumulator (d_T)    */
+    SOPB_FORCES = 3,   /* float[4n]  potential forces at the current coords,  */
+                       /*            computed on demand (read only)           */
+    SOPB_TIPFORCES = 4,/* float[4n]  per-bead tip force accumulator           */
+    SOPB_PULLSTATE = 5,/* float[12]  extForce[3] cant[3] cant0[3] vec[3]      */
+    SOPB_TIPSTATE = 6  /* float[16]  tip[3] chip[3] micaR[3] V dx fav[4] pad  */
+};
+
+/* ---- host utilities ---------------------------------------------------- */
+
+/* ABI version (SOPB_ABI_VERSION). */
+int sopb_version(void);
+
+/* Human-readable text for a status code. */
+const char* sopb_status_string(int status);
+
+/* Fills *p with the reference defaults: the PARAMETER() defaults of the
+ * integrator, potential and updater headers under src/ (langevin.h,
+ * covalent.h, pairs.h, pairlist.h, possiblepairlist.h, pulling.h,
+ * indentation.h, bdhitea.h). */
+void sopb_default_params(sopb_params* p);
+
+/* Hybrid Taus seeding: replaces initRand/generateSeeds
+ * (src/Integrators/ht.cu:29-56) with ran2 (src/Integrators/ran2.cpp:51-89) as
+ * seen by a fresh process.  Writes count uint4 states (4*count uint32) drawn
+ * from one ran2 stream started at `seed` (the reference passes seed+firstrun
+ * and draws all Ntr*N states of a multi-run job from that one stream). */
+int sopb_generate_seeds(int32_t seed, int64_t count, uint32_t* out4);
+
+/* ---- device context ------------------------------------------------------ */
+
+/* Opens a context on `device`; work is ordered on `stream` (a cudaStream_t,
+ * NULL = a new non-blocking stream owned by the context).  Replaces
+ * initGPU() (src/gsop.cu:45-64). */
+int sopb_context_create(int32_t device, void* stream, sopb_context** out);
+int sopb_context_destroy(sopb_context* ctx);
+/* Blocks until the context's stream drains; returns the first job error. */
+int sopb_context_sync(sopb_context* ctx);
+
+/* Device bytes a job needs (admission by HBM footprint). */
+int sopb_job_footprint(const sopb_job_desc* desc, size_t* bytes);
+
+/* Builds a job's device state: coordinates, covalent and native maps,
+ * list storage, RNG states, pulling flags.  Replaces the constructors of
+ * CovalentPotential, NativePotential, PairsPotential, PairList,
+ * PossiblepairList, PullingPotential, IndentationPotential, LangevinIntegrator
+ * and TeaIntegrator (src/gsop.cu:66-106). */
+int sopb_job_create(sopb_context* ctx, const sopb_job_desc* desc, sopb_job** out);
+int sopb_job_destroy(sopb_job* job);
+
+/* Advances every job in `jobs` by `nsteps` Langevin steps.  For each job and
+ * each step it does what one pass of runGPU's inner loop does
+ * (src/gsop.cu:129-148): at step % stride == 0 the updaters run in the
+ * reference order (indentation tip, pulling, possible pairs, temperature
+ * reset, pairlist, heating, TEA), then all potentials are summed and the
+ * integrator moves the beads.  Asynchronous on the context stream. */
+int sopb_run(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, int64_t nsteps);
+
+/* Device-reported status of a job (after sopb_context_sync). */
+int sopb_job_status(sopb_job* job);
+/* Current step counter of a job. */
+int sopb_job_step(sopb_job* job, int64_t* step);
+/* Bead count of a job. */
+int sopb_job_size(sopb_job* job, int32_t* n);
+
+/* Launch shape of a job's resident kernel: lanes cooperating on one bead
+ * and the CTA size class.  A function of the job alone (not of the batch
+ * it runs in); a job's launch class groups it with same-class jobs.  No
+ * reference counterpart (the reference fixes one thread per bead,
+ * src/gsop.cuh:13). */
+int sopb_job_shape(sopb_job* job, int32_t* lanes_per_bead, int32_t* block);
+
+/* Copies a quantity of one job to / from host memory (synchronous). */
+int sopb_job_read(sopb_job* job, int32_t what, void* host_out);
+int sopb_job_write(sopb_job* job, int32_t what, const void* host_in);
+
+/* Reads the current Verlet pairlist (or possible-pairs list when
+ * possible != 0) in the reference layout: counts[n] and a row of `cap`
+ * entries per bead, -1 padded (d_pairs / d_pairsCount,
+ * src/Updaters/pairlist_kernel.cu:33-76). */
+int sopb_job_pairlist(sopb_job* job, int32_t possible, int32_t* counts, int32_t* rows, int32_t cap);
+
+/* Rebuilds the possible-pairs list and/or the pairlist of a job now
+ * (PossiblepairList::update / PairList::update without the step gate). */
+int sopb_job_rebuild_lists(sopb_job* job, int32_t possible, int32_t verlet);
+
+/* Bulk transfer of the coordinates of many jobs with one copy each way:
+ * host_xyzw holds sum(n_j) float4 in the order of `jobs`. */
+int sopb_jobs_upload_coords(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, const float* host_xyzw);
+int sopb_jobs_download_coords(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, float* host_xyzw);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOPB_H */

@@ -1,0 +1,801 @@
+// sopb_api.cu — the C ABI: device context, job construction and the batched
+// launch of the resident Langevin step kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "../../include/sopb.h"
+#include "sopb_device.cuh"
+#include "sopb_resident.cuh"
+
+using namespace sopb;
+
+namespace {
+
+constexpr int kJobSlots = 16384;
+constexpr int kSideStreams = 4;
+constexpr int64_t kDefaultBeadCapacity = int64_t(1) << 22;
+
+// First-fit allocator over index ranges [0, cap).
+struct RangeAlloc {
+    std::map<int64_t, int64_t> free_;  // start -> length
+    void init(int64_t cap) { free_.clear(); free_[0] = cap; }
+    bool alloc(int64_t n, int64_t* out) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                *out = it->first;
+                const int64_t rest = it->second - n, start = it->first + n;
+                free_.erase(it);
+                if (rest) free_[start] = rest;
+                return true;
+            }
+        }
+        return false;
+    }
+    void release(int64_t start, int64_t n) {
+        auto it = free_.emplace(start, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace
+
+struct sopb_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 0;
+    int64_t bead_cap = 0;
+    float4* x = nullptr;
+    float4* xalt = nullptr;
+    uint4* seeds = nullptr;
+    float* T = nullptr;
+    float4* tipF = nullptr;
+    uint8_t* flags = nullptr;
+    RangeAlloc beads;
+    JobDev* d_jobs = nullptr;
+    int32_t* d_ids = nullptr;
+    int64_t ids_cap = 0;
+    float4* d_scratch4 = nullptr;
+    int64_t scratch4_cap = 0;
+    std::vector<sopb_job*> slots;
+    std::vector<int> free_slots;
+    cudaStream_t side[kSideStreams] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[kSideStreams] = {};
+    int32_t last_error = SOPB_OK;
+};
+
+struct sopb_job {
+    sopb_context* ctx = nullptr;
+    int slot = -1;
+    int64_t b0 = 0;
+    int32_t n = 0;
+    JobDev h{};
+    void* dmem = nullptr;
+    size_t dbytes = 0;
+};
+
+#define CUDA_TRY(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            std::fprintf(stderr, "sopb: %s failed: %s (%s:%d)\n", #call, cudaGetErrorString(e_), \
+                         __FILE__, __LINE__);                                                  \
+            return e_ == cudaErrorMemoryAllocation ? SOPB_ERR_NOMEM : SOPB_ERR_CUDA;           \
+        }                                                                                      \
+    } while (0)
+
+namespace {
+
+template <int B>
+int set_smem_attr() {
+    const int maxsm = 227 * 1024;
+    CUDA_TRY(cudaFuncSetAttribute(k_resident_steps<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+    return SOPB_OK;
+}
+
+// Lanes per bead and CTA size for a job of n beads.  Depends only on the job
+// (never on the batch it runs in), so a job's arithmetic is identical alone
+// and in any mix.
+void launch_shape(int32_t n, int32_t lpb_req, int32_t* lpb, int32_t* block) {
+    int32_t l = lpb_req;
+    if (l <= 0) l = 4;
+    int32_t p2 = 1;
+    while (p2 < l && p2 < 32) p2 <<= 1;
+    l = p2;
+    int32_t want = n * l;
+    int32_t b = 128;
+    while (b < want && b < 1024) b <<= 1;
+    *lpb = l;
+    *block = b;
+}
+
+int launch_resident(int block, int grid, size_t smem, cudaStream_t st, JobDev* jobs, const int32_t* ids, int64_t nsteps) {
+    switch (block) {
+    case 128: k_resident_steps<128><<<grid, 128, smem, st>>>(jobs, ids, nsteps); break;
+    case 256: k_resident_steps<256><<<grid, 256, smem, st>>>(jobs, ids, nsteps); break;
+    case 512: k_resident_steps<512><<<grid, 512, smem, st>>>(jobs, ids, nsteps); break;
+    case 1024: k_resident_steps<1024><<<grid, 1024, smem, st>>>(jobs, ids, nsteps); break;
+    default: return SOPB_ERR_INVALID;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
+}
+
+int launch_forces(int block, int grid, cudaStream_t st, const JobDev* jobs, const int32_t* ids, float4* out) {
+    switch (block) {
+    case 128: k_forces_only<128><<<grid, 128, 0, st>>>(jobs, ids, out); break;
+    case 256: k_forces_only<256><<<grid, 256, 0, st>>>(jobs, ids, out); break;
+    case 512: k_forces_only<512><<<grid, 512, 0, st>>>(jobs, ids, out); break;
+    case 1024: k_forces_only<1024><<<grid, 1024, 0, st>>>(jobs, ids, out); break;
+    default: return SOPB_ERR_INVALID;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
+}
+
+int launch_rebuild(int block, int grid, cudaStream_t st, JobDev* jobs, const int32_t* ids, int possible, int verlet) {
+    switch (block) {
+    case 128: k_rebuild_lists<128><<<grid, 128, 0, st>>>(jobs, ids, possible, verlet); break;
+    case 256: k_rebuild_lists<256><<<grid, 256, 0, st>>>(jobs, ids, possible, verlet); break;
+    case 512: k_rebuild_lists<512><<<grid, 512, 0, st>>>(jobs, ids, possible, verlet); break;
+    case 1024: k_rebuild_lists<1024><<<grid, 1024, 0, st>>>(jobs, ids, possible, verlet); break;
+    default: return SOPB_ERR_INVALID;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
+}
+
+int ensure_ids(sopb_context* c, int64_t need) {
+    if (need <= c->ids_cap) return SOPB_OK;
+    if (c->d_ids) cudaFreeAsync(c->d_ids, c->stream);
+    int64_t cap = std::max<int64_t>(need, 1024);
+    CUDA_TRY(cudaMallocAsync((void**)&c->d_ids, cap * sizeof(int32_t), c->stream));
+    c->ids_cap = cap;
+    return SOPB_OK;
+}
+
+int read_slot(sopb_job* j) {
+    CUDA_TRY(cudaStreamSynchronize(j->ctx->stream));
+    CUDA_TRY(cudaMemcpy(&j->h, &j->ctx->d_jobs[j->slot], sizeof(JobDev), cudaMemcpyDeviceToHost));
+    return SOPB_OK;
+}
+
+float f3norm(const float* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+// Updater period: the minimum over nav and the frequencies of the updaters
+// that exist for this job (src/gsop.cu:117-122).  Output updaters are not
+// part of the library; a caller that mirrors the reference's outputtiming
+// and dcdfreq passes the full minimum in params.stride.
+int32_t compute_stride(const sopb_params& p) {
+    if (p.stride > 0) return p.stride;
+    int32_t s = p.nav;
+    auto mn = [&](int32_t v) { if (v > 0 && v < s) s = v; };
+    mn(p.pairs_freq);
+    mn(p.possiblepairs_freq);
+    if (p.pulling && p.deltax != 0.0f) mn(p.pullFreq > 0 ? p.pullFreq : p.nav);
+    if (p.heating) mn(p.tempFreq);
+    if (p.hi_on && !p.hi_exact) mn(p.hi_epsilon_freq);
+    return s;
+}
+
+}  // namespace
+
+extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** out) {
+    if (!out) return SOPB_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SOPB_ERR_NODEVICE;
+    }
+    if (device < 0 || device >= ndev) return SOPB_ERR_INVALID;
+    CUDA_TRY(cudaSetDevice(device));
+    sopb_context* c = new (std::nothrow) sopb_context();
+    if (!c) return SOPB_ERR_NOMEM;
+    c->device = device;
+    CUDA_TRY(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    const char* env = std::getenv("SOPB_BEAD_CAPACITY");
+    c->bead_cap = env ? std::atoll(env) : kDefaultBeadCapacity;
+    if (c->bead_cap < 1024) c->bead_cap = 1024;
+    const int64_t B = c->bead_cap;
+    CUDA_TRY(cudaMalloc((void**)&c->x, B * sizeof(float4)));
+    CUDA_TRY(cudaMalloc((void**)&c->xalt, B * sizeof(float4)));
+    CUDA_TRY(cudaMalloc((void**)&c->seeds, B * sizeof(uint4)));
+    CUDA_TRY(cudaMalloc((void**)&c->T, B * sizeof(float)));
+    CUDA_TRY(cudaMalloc((void**)&c->tipF, B * sizeof(float4)));
+    CUDA_TRY(cudaMalloc((void**)&c->flags, B));
+    CUDA_TRY(cudaMalloc((void**)&c->d_jobs, kJobSlots * sizeof(JobDev)));
+    CUDA_TRY(cudaMemset(c->d_jobs, 0, kJobSlots * sizeof(JobDev)));
+    c->beads.init(B);
+    c->slots.assign(kJobSlots, nullptr);
+    for (int s = kJobSlots - 1; s >= 0; --s) c->free_slots.push_back(s);
+    for (int k = 0; k < kSideStreams; ++k) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    int rc;
+    if ((rc = set_smem_attr<128>()) || (rc = set_smem_attr<256>()) || (rc = set_smem_attr<512>()) ||
+        (rc = set_smem_attr<1024>()))
+        return rc;
+    *out = c;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_context_destroy(sopb_context* c) {
+    if (!c) return SOPB_ERR_INVALID;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (sopb_job* j : c->slots)
+        if (j) {
+            cudaFree(j->dmem);
+            delete j;
+        }
+    cudaFree(c->x);
+    cudaFree(c->xalt);
+    cudaFree(c->seeds);
+    cudaFree(c->T);
+    cudaFree(c->tipF);
+    cudaFree(c->flags);
+    cudaFree(c->d_jobs);
+    if (c->d_ids) cudaFree(c->d_ids);
+    if (c->d_scratch4) cudaFree(c->d_scratch4);
+    for (int k = 0; k < kSideStreams; ++k) {
+        cudaStreamDestroy(c->side[k]);
+        cudaEventDestroy(c->ev_join[k]);
+    }
+    cudaEventDestroy(c->ev_fork);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_context_sync(sopb_context* c) {
+    if (!c) return SOPB_ERR_INVALID;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return SOPB_OK;
+}
+
+namespace {
+
+struct HostMaps {
+    std::vector<int32_t> cov_off, cov_j, nat_off, nat_j;
+    std::vector<float> cov_r0;
+    std::vector<float2> nat_par;
+};
+
+int validate_desc(const sopb_job_desc* d) {
+    if (!d || d->n <= 0 || !d->xyz) return SOPB_ERR_INVALID;
+    const int32_t n = d->n;
+    const sopb_params& p = d->params;
+    if (p.timestep <= 0.0f || p.zeta <= 0.0f) return SOPB_ERR_INVALID;
+    if (p.nav <= 0 || p.pairs_freq <= 0 || p.possiblepairs_freq <= 0) return SOPB_ERR_INVALID;
+    if (p.heating && p.tempFreq <= 0) return SOPB_ERR_INVALID;
+    if (d->nbonds < 0 || d->nnatives < 0 || d->nfixed < 0 || d->npulled < 0) return SOPB_ERR_INVALID;
+    if ((d->nbonds && (!d->bonds || !d->bonds_r0)) || (d->nnatives && (!d->natives || !d->natives_r0 || !d->natives_eh)))
+        return SOPB_ERR_INVALID;
+    for (int32_t k = 0; k < 2 * d->nbonds; ++k)
+        if (d->bonds[k] < 0 || d->bonds[k] >= n) return SOPB_ERR_INVALID;
+    for (int32_t k = 0; k < 2 * d->nnatives; ++k)
+        if (d->natives[k] < 0 || d->natives[k] >= n) return SOPB_ERR_INVALID;
+    if (p.pulling) {
+        // PullingPotential ctor checks (src/Potentials/pulling.cu:54-56, 101-123)
+        if (p.deltax == 0.0f && p.fconst == 0.0f) return SOPB_ERR_INVALID;
+        if (p.fixedEnd < 0 || p.fixedEnd >= n || p.pulledEnd < 0 || p.pulledEnd >= n) return SOPB_ERR_INVALID;
+        for (int32_t k = 0; k < d->nfixed; ++k)
+            if (d->fixed[k] < 0 || d->fixed[k] >= n) return SOPB_ERR_INVALID;
+        for (int32_t k = 0; k < d->npulled; ++k)
+            if (d->pulled[k] < 0 || d->pulled[k] >= n) return SOPB_ERR_INVALID;
+    }
+    if (p.indentation) {
+        if (p.indentationTipZeta == 0.0f) return SOPB_ERR_INVALID;
+        if (f3norm(p.indentationDirection) == 0.0f || f3norm(p.indentationSurfaceN) == 0.0f) return SOPB_ERR_INVALID;
+    }
+    if (p.hi_on) return SOPB_ERR_UNSUPPORTED;  // HI jobs use the HI path (not in this entry point yet)
+    if (n > kMaxResidentBeads) return SOPB_ERR_UNSUPPORTED;
+    return SOPB_OK;
+}
+
+// covalent.cu:126-157 and native.cu:112-146: per-bead rows in .top order.
+void build_maps(const sopb_job_desc* d, HostMaps& m) {
+    const int32_t n = d->n;
+    std::vector<int32_t> cnt(n + 1, 0);
+    for (int32_t k = 0; k < d->nbonds; ++k) { cnt[d->bonds[2 * k]]++; cnt[d->bonds[2 * k + 1]]++; }
+    m.cov_off.assign(n + 1, 0);
+    for (int32_t i = 0; i < n; ++i) m.cov_off[i + 1] = m.cov_off[i] + cnt[i];
+    m.cov_j.assign(m.cov_off[n], 0);
+    m.cov_r0.assign(m.cov_off[n], 0.0f);
+    std::vector<int32_t> fill(m.cov_off.begin(), m.cov_off.end() - 1);
+    for (int32_t k = 0; k < d->nbonds; ++k) {
+        const int32_t a = d->bonds[2 * k], b = d->bonds[2 * k + 1];
+        m.cov_j[fill[a]] = b; m.cov_r0[fill[a]++] = d->bonds_r0[k];
+        m.cov_j[fill[b]] = a; m.cov_r0[fill[b]++] = d->bonds_r0[k];
+    }
+    std::fill(cnt.begin(), cnt.end(), 0);
+    for (int32_t k = 0; k < d->nnatives; ++k) { cnt[d->natives[2 * k]]++; cnt[d->natives[2 * k + 1]]++; }
+    m.nat_off.assign(n + 1, 0);
+    for (int32_t i = 0; i < n; ++i) m.nat_off[i + 1] = m.nat_off[i] + cnt[i];
+    m.nat_j.assign(m.nat_off[n], 0);
+    m.nat_par.assign(m.nat_off[n], make_float2(0.f, 0.f));
+    fill.assign(m.nat_off.begin(), m.nat_off.end() - 1);
+    for (int32_t k = 0; k < d->nnatives; ++k) {
+        const int32_t a = d->natives[2 * k], b = d->natives[2 * k + 1];
+        const float r0 = d->natives_r0[k], eh = d->natives_eh[k];
+        const float2 par = make_float2(r0 * r0, (float)(-12.0 * (double)eh / (double)(r0 * r0)));
+        m.nat_j[fill[a]] = b; m.nat_par[fill[a]++] = par;
+        m.nat_j[fill[b]] = a; m.nat_par[fill[b]++] = par;
+    }
+}
+
+}  // namespace
+
+extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
+    if (!d || !bytes || d->n <= 0) return SOPB_ERR_INVALID;
+    const int64_t n = d->n;
+    const int64_t cap_pp = std::max<int64_t>(1, std::min<int64_t>(d->params.max_possiblePairs > 0 ? d->params.max_possiblePairs : 4096, n - 1));
+    const int64_t cap_pl = std::max<int64_t>(1, std::min<int64_t>(d->params.max_pairs > 0 ? d->params.max_pairs : 512, n - 1));
+    size_t b = 0;
+    b += align256((n + 1) * 4) * 2;                 // offsets
+    b += align256(2 * (size_t)d->nbonds * 8);       // cov_j + r0
+    b += align256(2 * (size_t)d->nnatives * 12);    // nat_j + par
+    b += align256(n * 4) * 2;                       // counts
+    b += align256(n * cap_pp * 4) + align256(n * cap_pl * 4);
+    b += n * (16 + 16 + 16 + 4 + 16 + 1);           // bead pools
+    *bytes = b;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job** out) {
+    if (!c || !out) return SOPB_ERR_INVALID;
+    *out = nullptr;
+    int rc = validate_desc(d);
+    if (rc) return rc;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int32_t n = d->n;
+    const sopb_params& p = d->params;
+    if (c->free_slots.empty()) return SOPB_ERR_NOMEM;
+    int64_t b0;
+    if (!c->beads.alloc(n, &b0)) return SOPB_ERR_NOMEM;
+
+    HostMaps m;
+    build_maps(d, m);
+    JobDev h;
+    std::memset(&h, 0, sizeof(h));
+    h.n = n;
+    launch_shape(n, p.lanes_per_bead, &h.lpb, &h.block);
+    h.cap_pp = (int32_t)std::max<int64_t>(1, std::min<int64_t>(p.max_possiblePairs > 0 ? p.max_possiblePairs : 4096, n - 1));
+    h.cap_pl = (int32_t)std::max<int64_t>(1, std::min<int64_t>(p.max_pairs > 0 ? p.max_pairs : 512, n - 1));
+    h.stride = compute_stride(p);
+    h.nav = p.nav;
+    h.pairs_freq = p.pairs_freq;
+    h.pp_freq = p.possiblepairs_freq;
+    h.pull_freq = p.pullFreq > 0 ? p.pullFreq : p.nav;
+    h.temp_freq = p.heating ? p.tempFreq : 1;
+    h.eps_freq = p.hi_epsilon_freq > 0 ? p.hi_epsilon_freq : 1;
+    h.step = 0;
+    h.retraction_step = p.indentationRetractionStep;
+    // force field constants as the reference hosts compute them
+    h.ks = p.kspring_cov;
+    h.R2 = p.R_limit * p.R_limit;
+    h.a2 = p.a * p.a;
+    h.m6 = -6.0f * p.el / h.a2;
+    h.cut2 = p.pairs_cutoff * p.pairs_cutoff;
+    h.pl_cut = p.pairlist_cutoff;
+    h.pp_thr = p.pairs_threshold;
+    h.h = p.timestep;
+    h.zeta = p.zeta;
+    h.hOverZeta = p.timestep / p.zeta;
+    h.tempNorm = (float)(p.zeta / (6.0 * p.timestep));
+    const float T0 = p.heating ? p.initialT : p.temperature;
+    h.var = std::sqrt(2.0f * T0 * p.zeta / p.timestep);
+    h.minimization = p.minimization ? 1 : 0;
+    h.heating = p.heating ? 1 : 0;
+    h.initialT = p.initialT;
+    h.deltaT = p.deltaT;
+
+    std::vector<float4> x(n);
+    for (int32_t i = 0; i < n; ++i) x[i] = make_float4(d->xyz[3 * i], d->xyz[3 * i + 1], d->xyz[3 * i + 2], 0.0f);
+    std::vector<uint8_t> flags(n, FLAG_FREE);
+    if (p.pulling) {
+        // PullingPotential ctor (src/Potentials/pulling.cu:36-146)
+        h.pulling = 1;
+        h.ramp = p.deltax != 0.0f ? 1 : 0;
+        h.deltax = p.deltax;
+        h.k_trans = p.k_trans;
+        h.pulledEnd = p.pulledEnd;
+        const float4 xe = x[p.pulledEnd], xf = x[p.fixedEnd];
+        if (p.pull_direction == SOPB_PULL_VECTOR) {
+            for (int c2 = 0; c2 < 3; ++c2) h.pullvec[c2] = p.pullVector[c2];
+        } else {
+            float v[3] = {xe.x - xf.x, xe.y - xf.y, xe.z - xf.z};
+            const float len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            for (int c2 = 0; c2 < 3; ++c2) h.pullvec[c2] = v[c2] / len;
+        }
+        const float xe3[3] = {xe.x, xe.y, xe.z};
+        for (int c2 = 0; c2 < 3; ++c2) {
+            h.cant0[c2] = h.cant[c2] = xe3[c2];
+            h.pullF[c2] = h.pullvec[c2] * p.fconst;
+        }
+        for (int32_t k = 0; k < d->npulled; ++k) flags[d->pulled[k]] = FLAG_PULLED;
+        for (int32_t k = 0; k < d->nfixed; ++k) flags[d->fixed[k]] = FLAG_FIXED;
+        // the force-ramp updater re-marks pulled beads at step 0 (pulling.cu:159-163)
+        if (h.ramp)
+            for (int32_t k = 0; k < d->npulled; ++k) flags[d->pulled[k]] = FLAG_PULLED;
+    }
+    if (p.indentation) {
+        // IndentationPotential ctor (src/Potentials/indentation.cu:75-137)
+        h.indent = 1;
+        h.moveSurface = p.indentationMoveSurface ? 1 : 0;
+        h.fixTrans = p.indentationFixTrans ? 1 : 0;
+        for (int c2 = 0; c2 < 3; ++c2) {
+            h.chip[c2] = h.chip0[c2] = p.indentationChip[c2];
+            h.tip[c2] = p.indentationTip[c2];
+            h.dir[c2] = p.indentationDirection[c2];
+            h.micaR[c2] = h.micaR0[c2] = p.indentationSurfaceR0[c2];
+            h.micaN[c2] = p.indentationSurfaceN[c2];
+        }
+        h.tipR = p.indentationTipR;
+        h.cantKs = p.indentationKs;
+        h.V = p.indentationDeltaX;
+        h.dx = 0.0f;
+        h.tipZeta = p.indentationTipZeta;
+        h.tipAp = 12.0f * p.indentationTipEl * std::pow(p.indentationTipSigma, 12.0f) * p.indentationTipA;
+        h.tipBp = 6.0f * p.indentationTipEl * std::pow(p.indentationTipSigma, 6.0f) * p.indentationTipB;
+        h.surfAp = 12.0f * p.indentationSurfEl * std::pow(p.indentationSurfSigma, 12.0f) * p.indentationSurfA;
+        h.surfBp = 6.0f * p.indentationSurfEl * std::pow(p.indentationSurfSigma, 6.0f) * p.indentationSurfB;
+        float nd = f3norm(h.dir);
+        for (int c2 = 0; c2 < 3; ++c2) h.dir[c2] /= nd;
+        nd = f3norm(h.micaN);
+        for (int c2 = 0; c2 < 3; ++c2) h.micaN[c2] /= nd;
+    }
+    std::vector<uint32_t> seeds(4 * (size_t)n);
+    if (d->seeds) std::memcpy(seeds.data(), d->seeds, seeds.size() * 4);
+    else sopb_generate_seeds(d->seed, n, seeds.data());
+
+    // device block for the maps and lists
+    const size_t o_covoff = 0;
+    const size_t o_covj = o_covoff + align256((n + 1) * 4);
+    const size_t o_covr0 = o_covj + align256(m.cov_j.size() * 4 + 4);
+    const size_t o_natoff = o_covr0 + align256(m.cov_r0.size() * 4 + 4);
+    const size_t o_natj = o_natoff + align256((n + 1) * 4);
+    const size_t o_natpar = o_natj + align256(m.nat_j.size() * 4 + 4);
+    const size_t o_ppcnt = o_natpar + align256(m.nat_par.size() * 8 + 8);
+    const size_t o_plcnt = o_ppcnt + align256((size_t)n * 4);
+    const size_t o_ppj = o_plcnt + align256((size_t)n * 4);
+    const size_t o_plj = o_ppj + align256((size_t)n * h.cap_pp * 4);
+    const size_t total = o_plj + align256((size_t)n * h.cap_pl * 4);
+    sopb_job* j = new (std::nothrow) sopb_job();
+    if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
+    cudaError_t e = cudaMalloc(&j->dmem, total);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c->beads.release(b0, n);
+        delete j;
+        return SOPB_ERR_NOMEM;
+    }
+    char* base = (char*)j->dmem;
+    h.cov_off = (int32_t*)(base + o_covoff);
+    h.cov_j = (int32_t*)(base + o_covj);
+    h.cov_r0 = (float*)(base + o_covr0);
+    h.nat_off = (int32_t*)(base + o_natoff);
+    h.nat_j = (int32_t*)(base + o_natj);
+    h.nat_par = (float2*)(base + o_natpar);
+    h.pp_cnt = (int32_t*)(base + o_ppcnt);
+    h.pl_cnt = (int32_t*)(base + o_plcnt);
+    h.pp_j = (int32_t*)(base + o_ppj);
+    h.pl_j = (int32_t*)(base + o_plj);
+    h.x = c->x + b0;
+    h.xalt = c->xalt + b0;
+    h.seeds = c->seeds + b0;
+    h.T = c->T + b0;
+    h.tipF = c->tipF + b0;
+    h.flags = c->flags + b0;
+    cudaStream_t st = c->stream;
+    CUDA_TRY(cudaMemsetAsync(base + o_ppcnt, 0, (size_t)n * 8 + 512, st));
+    CUDA_TRY(cudaMemcpyAsync(h.cov_off, m.cov_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
+    if (!m.cov_j.empty()) {
+        CUDA_TRY(cudaMemcpyAsync(h.cov_j, m.cov_j.data(), m.cov_j.size() * 4, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(h.cov_r0, m.cov_r0.data(), m.cov_r0.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(h.nat_off, m.nat_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
+    if (!m.nat_j.empty()) {
+        CUDA_TRY(cudaMemcpyAsync(h.nat_j, m.nat_j.data(), m.nat_j.size() * 4, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(h.nat_par, m.nat_par.data(), m.nat_par.size() * 8, cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(h.x, x.data(), (size_t)n * 16, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(h.seeds, seeds.data(), (size_t)n * 16, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(h.flags, flags.data(), (size_t)n, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(h.T, 0, (size_t)n * 4, st));
+    CUDA_TRY(cudaMemsetAsync(h.tipF, 0, (size_t)n * 16, st));
+    const int slot = c->free_slots.back();
+    c->free_slots.pop_back();
+    CUDA_TRY(cudaMemcpyAsync(&c->d_jobs[slot], &h, sizeof(JobDev), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));   // host staging vectors go out of scope
+    j->ctx = c;
+    j->slot = slot;
+    j->b0 = b0;
+    j->n = n;
+    j->h = h;
+    j->dbytes = total;
+    c->slots[slot] = j;
+    *out = j;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_destroy(sopb_job* j) {
+    if (!j) return SOPB_ERR_INVALID;
+    sopb_context* c = j->ctx;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(j->dmem);
+    c->beads.release(j->b0, j->n);
+    c->slots[j->slot] = nullptr;
+    c->free_slots.push_back(j->slot);
+    delete j;
+    return SOPB_OK;
+}
+
+namespace {
+// Groups jobs by CTA size class; returns (block, ids) per class, largest
+// jobs' class first so the longest CTAs start first.
+struct LaunchClass {
+    int block;
+    int32_t max_n;
+    std::vector<int32_t> ids;
+};
+void group_jobs(sopb_job* const* jobs, int32_t njobs, std::vector<LaunchClass>& out) {
+    std::map<int, LaunchClass> cls;
+    std::vector<int32_t> order(njobs);
+    for (int32_t k = 0; k < njobs; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return jobs[a]->n > jobs[b]->n; });
+    for (int32_t k : order) {
+        LaunchClass& L = cls[jobs[k]->h.block];
+        L.block = jobs[k]->h.block;
+        L.max_n = std::max(L.max_n, jobs[k]->n);
+        L.ids.push_back(jobs[k]->slot);
+    }
+    out.clear();
+    for (auto& kv : cls) out.push_back(kv.second);
+    std::sort(out.begin(), out.end(), [](const LaunchClass& a, const LaunchClass& b) { return a.max_n > b.max_n; });
+}
+}  // namespace
+
+extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, int64_t nsteps) {
+    if (!c || (njobs > 0 && !jobs) || njobs < 0 || nsteps < 0) return SOPB_ERR_INVALID;
+    if (njobs == 0 || nsteps == 0) return SOPB_OK;
+    for (int32_t k = 0; k < njobs; ++k)
+        if (!jobs[k] || jobs[k]->ctx != c) return SOPB_ERR_INVALID;
+    CUDA_TRY(cudaSetDevice(c->device));
+    std::vector<LaunchClass> cls;
+    group_jobs(jobs, njobs, cls);
+    std::vector<int32_t> ids;
+    std::vector<size_t> off;
+    for (auto& L : cls) {
+        off.push_back(ids.size());
+        ids.insert(ids.end(), L.ids.begin(), L.ids.end());
+    }
+    int rc = ensure_ids(c, (int64_t)ids.size());
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(c->d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    if (cls.size() == 1) {
+        const LaunchClass& L = cls[0];
+        return launch_resident(L.block, (int)L.ids.size(), (size_t)L.max_n * kResidentSmemPerBead, c->stream, c->d_jobs,
+                               c->d_ids, nsteps);
+    }
+    CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
+    for (size_t k = 0; k < cls.size(); ++k) {
+        cudaStream_t s = c->side[k % kSideStreams];
+        CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
+        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), (size_t)cls[k].max_n * kResidentSmemPerBead, s,
+                             c->d_jobs, c->d_ids + off[k], nsteps);
+        if (rc) return rc;
+    }
+    for (int k = 0; k < kSideStreams && k < (int)cls.size(); ++k) {
+        CUDA_TRY(cudaEventRecord(c->ev_join[k], c->side[k]));
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_join[k], 0));
+    }
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_status(sopb_job* j) {
+    if (!j) return SOPB_ERR_INVALID;
+    int rc = read_slot(j);
+    if (rc) return rc;
+    return j->h.status;
+}
+
+extern "C" int sopb_job_step(sopb_job* j, int64_t* step) {
+    if (!j || !step) return SOPB_ERR_INVALID;
+    int rc = read_slot(j);
+    if (rc) return rc;
+    *step = j->h.step;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_size(sopb_job* j, int32_t* n) {
+    if (!j || !n) return SOPB_ERR_INVALID;
+    *n = j->n;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_shape(sopb_job* j, int32_t* lpb, int32_t* block) {
+    if (!j || !lpb || !block) return SOPB_ERR_INVALID;
+    *lpb = j->h.lpb;
+    *block = j->h.block;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
+    if (!j || !out) return SOPB_ERR_INVALID;
+    sopb_context* c = j->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t n = j->n;
+    switch (what) {
+    case SOPB_COORDS:
+        CUDA_TRY(cudaMemcpyAsync(out, c->x + j->b0, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        break;
+    case SOPB_SEEDS:
+        CUDA_TRY(cudaMemcpyAsync(out, c->seeds + j->b0, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        break;
+    case SOPB_TEMP:
+        CUDA_TRY(cudaMemcpyAsync(out, c->T + j->b0, n * 4, cudaMemcpyDeviceToHost, c->stream));
+        break;
+    case SOPB_TIPFORCES:
+        CUDA_TRY(cudaMemcpyAsync(out, c->tipF + j->b0, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        break;
+    case SOPB_FORCES: {
+        if ((int64_t)n > c->scratch4_cap) {
+            if (c->d_scratch4) cudaFreeAsync(c->d_scratch4, c->stream);
+            CUDA_TRY(cudaMallocAsync((void**)&c->d_scratch4, n * 16, c->stream));
+            c->scratch4_cap = (int64_t)n;
+        }
+        int rc = ensure_ids(c, 1);
+        if (rc) return rc;
+        const int32_t id = j->slot;
+        CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
+        rc = launch_forces(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, c->d_scratch4);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(out, c->d_scratch4, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        break;
+    }
+    case SOPB_PULLSTATE: {
+        int rc = read_slot(j);
+        if (rc) return rc;
+        float* o = (float*)out;
+        std::memcpy(o, j->h.pullF, 12);
+        std::memcpy(o + 3, j->h.cant, 12);
+        std::memcpy(o + 6, j->h.cant0, 12);
+        std::memcpy(o + 9, j->h.pullvec, 12);
+        return SOPB_OK;
+    }
+    case SOPB_TIPSTATE: {
+        int rc = read_slot(j);
+        if (rc) return rc;
+        float* o = (float*)out;
+        std::memset(o, 0, 64);
+        std::memcpy(o, j->h.tip, 12);
+        std::memcpy(o + 3, j->h.chip, 12);
+        std::memcpy(o + 6, j->h.micaR, 12);
+        o[9] = j->h.V;
+        o[10] = j->h.dx;
+        std::memcpy(o + 11, j->h.fav, 16);
+        return SOPB_OK;
+    }
+    default: return SOPB_ERR_INVALID;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_write(sopb_job* j, int32_t what, const void* in) {
+    if (!j || !in) return SOPB_ERR_INVALID;
+    sopb_context* c = j->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t n = j->n;
+    switch (what) {
+    case SOPB_COORDS: CUDA_TRY(cudaMemcpyAsync(c->x + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->stream)); break;
+    case SOPB_SEEDS: CUDA_TRY(cudaMemcpyAsync(c->seeds + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->stream)); break;
+    case SOPB_TEMP: CUDA_TRY(cudaMemcpyAsync(c->T + j->b0, in, n * 4, cudaMemcpyHostToDevice, c->stream)); break;
+    case SOPB_TIPFORCES: CUDA_TRY(cudaMemcpyAsync(c->tipF + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->stream)); break;
+    default: return SOPB_ERR_INVALID;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_pairlist(sopb_job* j, int32_t possible, int32_t* counts, int32_t* rows, int32_t cap) {
+    if (!j || !counts || !rows || cap <= 0) return SOPB_ERR_INVALID;
+    sopb_context* c = j->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int32_t n = j->n;
+    const int32_t lcap = possible ? j->h.cap_pp : j->h.cap_pl;
+    std::vector<int32_t> cnt(n), lst((size_t)n * lcap);
+    CUDA_TRY(cudaMemcpyAsync(cnt.data(), possible ? j->h.pp_cnt : j->h.pl_cnt, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(lst.data(), possible ? j->h.pp_j : j->h.pl_j, lst.size() * 4, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int32_t i = 0; i < n; ++i) {
+        counts[i] = cnt[i];
+        for (int32_t k = 0; k < cap; ++k) rows[(size_t)i * cap + k] = (k < cnt[i] && k < lcap) ? lst[(size_t)i * lcap + k] : -1;
+    }
+    return SOPB_OK;
+}
+
+extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t verlet) {
+    if (!j) return SOPB_ERR_INVALID;
+    sopb_context* c = j->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = ensure_ids(c, 1);
+    if (rc) return rc;
+    const int32_t id = j->slot;
+    CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
+    rc = launch_rebuild(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, possible, verlet);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return SOPB_OK;
+}
+
+namespace {
+// One copy when the jobs' bead ranges are contiguous and in order, else one
+// copy per job.
+int bulk_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, void* host, bool up) {
+    if (!c || (njobs && !jobs) || !host) return SOPB_ERR_INVALID;
+    CUDA_TRY(cudaSetDevice(c->device));
+    bool contiguous = true;
+    for (int32_t k = 1; k < njobs; ++k)
+        if (jobs[k]->b0 != jobs[k - 1]->b0 + jobs[k - 1]->n) contiguous = false;
+    if (contiguous && njobs) {
+        int64_t total = 0;
+        for (int32_t k = 0; k < njobs; ++k) total += jobs[k]->n;
+        if (up) CUDA_TRY(cudaMemcpyAsync(c->x + jobs[0]->b0, host, total * 16, cudaMemcpyHostToDevice, c->stream));
+        else CUDA_TRY(cudaMemcpyAsync(host, c->x + jobs[0]->b0, total * 16, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        char* h = (char*)host;
+        for (int32_t k = 0; k < njobs; ++k) {
+            const size_t b = (size_t)jobs[k]->n * 16;
+            if (up) CUDA_TRY(cudaMemcpyAsync(c->x + jobs[k]->b0, h, b, cudaMemcpyHostToDevice, c->stream));
+            else CUDA_TRY(cudaMemcpyAsync(h, c->x + jobs[k]->b0, b, cudaMemcpyDeviceToHost, c->stream));
+            h += b;
+        }
+    }
+    return SOPB_OK;
+}
+}  // namespace
+
+extern "C" int sopb_jobs_upload_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, const float* host_xyzw) {
+    return bulk_coords(c, jobs, njobs, (void*)host_xyzw, true);
+}
+
+extern "C" int sopb_jobs_download_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, float* host_xyzw) {
+    int rc = bulk_coords(c, jobs, njobs, host_xyzw, false);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return SOPB_OK;
+}

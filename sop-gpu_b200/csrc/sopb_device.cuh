@@ -1,0 +1,183 @@
+// sopb_device.cuh — device-side job descriptor and per-bead math of the SOP
+// Langevin step for sm_100a.
+//
+// One JobDev describes one independent SOP system (a "trajectory" of the
+// reference).  Per-bead state lives in context-wide bead pools (coordinates,
+// RNG states, temperature accumulator, flags) so a batch's coordinates move
+// with one copy; the neighbour maps of a job are CSR (covalent, native) or
+// fixed-capacity rows (possible pairs, Verlet pairs).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sopb {
+
+enum : int { FLAG_FREE = 0, FLAG_FIXED = 1, FLAG_PULLED = 2 };
+
+struct JobDev {
+    // ---- sizes and schedule ------------------------------------------------
+    int32_t n;            // beads
+    int32_t lpb;          // lanes cooperating on one bead's lists
+    int32_t block;        // CTA size class of the resident kernel
+    int32_t cap_pp;       // possible-pairs row capacity
+    int32_t cap_pl;       // Verlet row capacity
+    int32_t stride;       // updater period (gsop.cu:117-122)
+    int32_t nav;
+    int32_t pairs_freq;
+    int32_t pp_freq;
+    int32_t pull_freq;
+    int32_t temp_freq;
+    int32_t eps_freq;
+    int64_t step;
+    int64_t retraction_step;
+    // ---- per-bead state (views into the context pools) ----------------------
+    float4* x;            // coordinates, w = 0
+    uint4* seeds;         // Hybrid Taus states
+    float* T;             // kinetic temperature accumulator
+    float4* tipF;         // per-bead tip force accumulator (indentation)
+    uint8_t* flags;       // FLAG_*
+    float4* xalt;         // second coordinate buffer (grid path ping-pong)
+    // ---- maps ----------------------------------------------------------------
+    int32_t* cov_off;     // [n+1]
+    int32_t* cov_j;
+    float* cov_r0;
+    int32_t* nat_off;     // [n+1]
+    int32_t* nat_j;
+    float2* nat_par;      // (r0^2, -12 eh / r0^2)  (native.cu:112-146)
+    int32_t* pp_cnt;      // [n]
+    int32_t* pp_j;        // [n * cap_pp]
+    int32_t* pl_cnt;      // [n]
+    int32_t* pl_j;        // [n * cap_pl]
+    // ---- force field ---------------------------------------------------------
+    float ks, R2;         // FENE: kspring_cov, R_limit^2
+    float a2, m6, cut2;   // repulsive: a^2, -6 el / a^2, pairs_cutoff^2
+    float pl_cut;         // pairlist_cutoff
+    float pp_thr;         // pairs_threshold
+    // ---- integrator ------------------------------------------------------------
+    float hOverZeta, tempNorm, var, zeta, h;
+    int32_t minimization, heating;
+    float initialT, deltaT;
+    // ---- pulling ---------------------------------------------------------------
+    int32_t pulling, ramp, pulledEnd, pad0;
+    float deltax, k_trans;
+    float pullvec[3], cant0[3], cant[3], pullF[3];
+    // ---- indentation (continuous surface) ------------------------------------
+    int32_t indent, moveSurface, fixTrans, pad1;
+    float tip[3], chip[3], chip0[3], dir[3], micaR[3], micaR0[3], micaN[3];
+    float tipR, tipAp, tipBp, surfAp, surfBp, cantKs, V, dx, tipZeta;
+    float fav[4];
+    // ---- status ---------------------------------------------------------------
+    int32_t status;
+    int32_t pad2[3];
+};
+
+// ---------------------------------------------------------------------------
+// Hybrid Taus generator (L'Ecuyer's combined Tausworthe steps + an LCG,
+// "GPU Gems 3" ch. 37), as used by the reference (src/Integrators/ht.cu:61-106).
+// The integer stream is bit-exact; the Gaussians use the fast-math intrinsics
+// the reference build uses (-use_fast_math, src/Makefile:14).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t taus_step(uint32_t& z, int s1, int s2, int s3, uint32_t m) {
+    uint32_t b = (((z << s1) ^ z) >> s2);
+    z = (((z & m) << s3) ^ b);
+    return z;
+}
+__device__ __forceinline__ uint32_t hybrid_taus(uint4& s) {
+    uint32_t a = taus_step(s.x, 13, 19, 12, 4294967294u);
+    uint32_t b = taus_step(s.y, 2, 25, 4, 4294967288u);
+    uint32_t c = taus_step(s.z, 3, 11, 17, 4294967280u);
+    s.w = 1664525u * s.w + 1013904223u;
+    return a ^ b ^ c ^ s.w;
+}
+// Mantissa fill to [1,2) minus one; exact zero maps to 1e-8 (ht.cu:61-69).
+__device__ __forceinline__ float uint_to_unit(uint32_t u) {
+    float f = __uint_as_float(0x3f800000u | (0x007fffffu & u)) - 1.0f;
+    return f == 0.0f ? 1.0e-8f : f;
+}
+// Box-Muller on four draws.  The angle is 2*pi*u formed in double precision
+// and rounded to float, as the reference's `2.0f*M_PI*u` is.
+__device__ __forceinline__ float4 gaussian4(uint4& s) {
+    float4 g;
+    float r = sqrtf(-2.0f * __logf(uint_to_unit(hybrid_taus(s))));
+    float th = __double2float_rn(6.283185307179586 * (double)uint_to_unit(hybrid_taus(s)));
+    g.x = r * __sinf(th);
+    g.y = r * __cosf(th);
+    r = sqrtf(-2.0f * __logf(uint_to_unit(hybrid_taus(s))));
+    th = __double2float_rn(6.283185307179586 * (double)uint_to_unit(hybrid_taus(s)));
+    g.z = r * __sinf(th);
+    g.w = r * __cosf(th);
+    return g;
+}
+
+// Distance test used by both list builders, in IEEE round-to-nearest with no
+// contraction: sqrt(dx*dx + dy*dy + dz*dz) < cut, the reference's test
+// (possiblepairlist_kernel.cu:45-46, pairlist_kernel.cu:57-63) evaluated
+// exactly as the CPU oracle evaluates it, so list membership is bit-exact.
+__device__ __forceinline__ bool within_cutoff(float4 xi, float4 xj, float cut) {
+    float dx = __fsub_rn(xj.x, xi.x), dy = __fsub_rn(xj.y, xi.y), dz = __fsub_rn(xj.z, xi.z);
+    float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    return __fsqrt_rn(r2) < cut;
+}
+
+// FENE term (covalent_kernel.cu:28-51): Ks*(r-r0)/(r*(1-(r-r0)^2/R0^2)).
+__device__ __forceinline__ void fene_term(float4 xi, float4 xj, float r0, float ks, float R2, float3& f) {
+    float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    float w = sqrtf(dx * dx + dy * dy + dz * dz) - r0;
+    w = ks * w / ((w + r0) * (1.0f - w * w / R2));
+    f.x += w * dx;
+    f.y += w * dy;
+    f.z += w * dz;
+}
+// Native LJ 12-6 term (native_kernel.cu:27-52).
+__device__ __forceinline__ void native_term(float4 xi, float4 xj, float2 par, float3& f) {
+    float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    float w = par.x / (dx * dx + dy * dy + dz * dz);
+    float p6 = w * w * w;
+    w = w * (p6 * p6 - p6) * par.y;
+    f.x += dx * w;
+    f.y += dy * w;
+    f.z += dz * w;
+}
+// Repulsive r^-6 term with the force cutoff (pairs_kernel.cu:33-59).
+__device__ __forceinline__ void pair_term(float4 xi, float4 xj, float a2, float m6, float cut2, float3& f) {
+    float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    float w = dx * dx + dy * dy + dz * dz;
+    if (w < cut2) {
+        w = a2 / w;
+        w = w * w;
+        w = m6 * w * w;
+        f.x += dx * w;
+        f.y += dy * w;
+        f.z += dz * w;
+    }
+}
+
+// Tip and continuous-surface terms (indentation_kernel.cu:71-128).  Returns
+// the tip's share in tipf (accumulated per bead by the caller).
+struct IndentGeom {
+    float tip[3], micaR[3], micaN[3];
+    float tipR, tipAp, tipBp, surfAp, surfBp;
+};
+__device__ __forceinline__ void indentation_term(float4 xi, const IndentGeom& g, float3& f, float3& tipf) {
+    float dx = xi.x - g.tip[0], dy = xi.y - g.tip[1], dz = xi.z - g.tip[2];
+    float dw = sqrtf(dx * dx + dy * dy + dz * dz);
+    float r2 = 1.0f / (dw - g.tipR);
+    r2 = r2 * r2;
+    float r6 = r2 * r2 * r2;
+    float w = g.tipAp * r6 + g.tipBp;
+    w = w * r6 / (dw * (dw - g.tipR));
+    float3 df = make_float3(dx * w, dy * w, dz * w);
+    tipf = df;
+    float d = (xi.x - g.micaR[0]) * g.micaN[0] + (xi.y - g.micaR[1]) * g.micaN[1] + (xi.z - g.micaR[2]) * g.micaN[2];
+    d = 1.0f / d;
+    d = d * d;
+    r6 = d * d * d;
+    w = g.surfAp * r6 + g.surfBp;
+    w = w * r6 * d;
+    f.x += g.micaN[0] * w + df.x;
+    f.y += g.micaN[1] * w + df.y;
+    f.z += g.micaN[2] * w + df.z;
+}
+
+}  // namespace sopb

@@ -1,0 +1,403 @@
+// sopb_resident.cuh — the replica-resident Langevin step kernel.
+//
+// One CTA owns one job for a whole launch of `nsteps` steps.  Coordinates
+// (ping-pong), Hybrid Taus states and the temperature accumulator sit in
+// shared memory; every updater of the reference loop (indentation tip,
+// force-ramp cantilever, possible pairs, temperature reset, Verlet pairlist,
+// heating) runs inside the kernel at its step, so there is no host round
+// trip and no launch per step (the reference launches 4-6 kernels per step
+// and copies all coordinates to the host every `stride` steps for pulling,
+// src/Potentials/pulling.cu:152-165).
+//
+// Work split: `lpb` lanes (a power of two <= 32, aligned inside a warp)
+// cooperate on one bead: they stride over its covalent, native and Verlet
+// lists and combine their partial forces with xor-shuffles; lane 0 then draws
+// the bead's noise and integrates.  All loops that contain warp collectives
+// have CTA-uniform trip counts.
+#pragma once
+
+#include "sopb_device.cuh"
+
+namespace sopb {
+
+constexpr int kMaxResidentBeads = 4096;     // 52 B of shared memory per bead
+constexpr int kResidentSmemPerBead = 52;
+
+struct StepScalars {
+    float var;
+    float pullF[3];
+    float cant[3];
+    IndentGeom ig;
+    float chip[3];
+    float V, dx;
+    float fav[4];
+    int32_t err;
+};
+
+// Cooperative copy of a job descriptor into shared memory (read by every
+// thread as a broadcast instead of per-thread register copies).
+template <int BLOCK>
+__device__ __forceinline__ void load_job(JobDev& dst, const JobDev* src) {
+    static_assert(sizeof(JobDev) % 4 == 0, "JobDev must be word sized");
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int w = threadIdx.x; w < (int)(sizeof(JobDev) / 4); w += BLOCK) d[w] = s[w];
+}
+
+__device__ __forceinline__ unsigned group_mask(int lpb) {
+    return lpb == 32 ? 0xffffffffu : ((1u << lpb) - 1u);
+}
+
+// Partial force of lane `l` of the group working on bead i: covalent, then
+// native, then Verlet pairs, each list strided by lpb (the reference sums
+// the three kernels' contributions in this order, gsop.cu:80-85).
+__device__ __forceinline__ float3 bead_force_partial(const JobDev& J, const float4* __restrict__ xs, int i, float4 xi,
+                                                     int l, int lpb) {
+    float3 f = make_float3(0.f, 0.f, 0.f);
+    const int c0 = J.cov_off[i], c1 = J.cov_off[i + 1];
+    for (int k = c0 + l; k < c1; k += lpb) fene_term(xi, xs[J.cov_j[k]], J.cov_r0[k], J.ks, J.R2, f);
+    const int n0 = J.nat_off[i], n1 = J.nat_off[i + 1];
+    for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[J.nat_j[k]], J.nat_par[k], f);
+    const int np = J.pl_cnt[i];
+    const int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
+    for (int k = l; k < np; k += lpb) pair_term(xi, xs[row[k]], J.a2, J.m6, J.cut2, f);
+    return f;
+}
+
+__device__ __forceinline__ float3 group_reduce(float3 f, int lpb) {
+    for (int o = lpb >> 1; o > 0; o >>= 1) {
+        f.x += __shfl_xor_sync(0xffffffffu, f.x, o);
+        f.y += __shfl_xor_sync(0xffffffffu, f.y, o);
+        f.z += __shfl_xor_sync(0xffffffffu, f.z, o);
+    }
+    return f;
+}
+
+__device__ __forceinline__ bool excluded(const JobDev& J, int i, int q) {
+    for (int k = J.cov_off[i]; k < J.cov_off[i + 1]; ++k)
+        if (J.cov_j[k] == q) return true;
+    for (int k = J.nat_off[i]; k < J.nat_off[i + 1]; ++k)
+        if (J.nat_j[k] == q) return true;
+    return false;
+}
+
+// generate_possiblepairs (src/Updaters/possiblepairlist_kernel.cu:18-71):
+// every q != i of the job with |r| < pairs_threshold that is neither a
+// covalent nor a native partner, appended in increasing q.  Ballot
+// compaction inside the group keeps the order.  Overflow sets err.
+template <int BLOCK>
+__device__ void build_possible(const JobDev& J, const float4* __restrict__ xs, int& err) {
+    const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
+    const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
+    const int gbase = (tid & 31) & ~(lpb - 1);
+    const unsigned gm = group_mask(lpb);
+    for (int base = 0; base < n; base += ng) {
+        const int i = base + g;
+        const bool act = i < n;
+        const float4 xi = xs[act ? i : 0];
+        int32_t* row = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
+        int cnt = 0;
+        for (int qb = 0; qb < n; qb += lpb) {
+            const int q = qb + l;
+            bool ok = act && q < n && q != i && within_cutoff(xi, xs[q < n ? q : 0], J.pp_thr);
+            if (ok) ok = !excluded(J, i, q);
+            const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
+            if (ok) {
+                const int pos = cnt + __popc(m & ((1u << l) - 1u));
+                if (pos < J.cap_pp) row[pos] = q;
+                else err = 2;
+            }
+            cnt += __popc(m);
+        }
+        if (act && l == 0) J.pp_cnt[i] = cnt < J.cap_pp ? cnt : J.cap_pp;
+    }
+}
+
+// generate_pairs (src/Updaters/pairlist_kernel.cu:33-76): the possible pairs
+// with |r| < pairlist_cutoff, order kept.  The reference pads rows with -1
+// every rebuild; rows here are read only up to their count.
+template <int BLOCK>
+__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int& err) {
+    const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
+    const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
+    const int gbase = (tid & 31) & ~(lpb - 1);
+    const unsigned gm = group_mask(lpb);
+    for (int base = 0; base < n; base += ng) {
+        const int i = base + g;
+        const bool act = i < n;
+        const float4 xi = xs[act ? i : 0];
+        const int npp = act ? J.pp_cnt[i] : 0;
+        const int32_t* prow = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
+        int32_t* row = J.pl_j + (size_t)(act ? i : 0) * J.cap_pl;
+        const int kmax = __reduce_max_sync(0xffffffffu, npp);
+        int cnt = 0;
+        for (int kb = 0; kb < kmax; kb += lpb) {
+            const int k = kb + l;
+            int q = 0;
+            bool ok = k < npp;
+            if (ok) {
+                q = prow[k];
+                ok = within_cutoff(xi, xs[q], J.pl_cut);
+            }
+            const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
+            if (ok) {
+                const int pos = cnt + __popc(m & ((1u << l) - 1u));
+                if (pos < J.cap_pl) row[pos] = q;
+                else err = 2;
+            }
+            cnt += __popc(m);
+        }
+        if (act && l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
+    }
+}
+
+// Deterministic CTA sum of a float3 (fixed tree for a given BLOCK).
+template <int BLOCK>
+__device__ float3 block_sum3(float3 v, float (*red)[4]) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+    }
+    __syncthreads();
+    if (lane == 0) { red[w][0] = v.x; red[w][1] = v.y; red[w][2] = v.z; }
+    __syncthreads();
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int q = 0; q < BLOCK / 32; ++q) { s.x += red[q][0]; s.y += red[q][1]; s.z += red[q][2]; }
+    return s;
+}
+
+// IndentationTipUpdater::update (src/Potentials/indentation.cu:414-550) for
+// the continuous surface, run by thread 0 after the CTA summed the tip force.
+// Host-side arithmetic of the reference is IEEE without contraction, hence
+// the explicit _rn intrinsics.
+__device__ void tip_update(const JobDev& J, StepScalars& sc, float3 fsum, int64_t step) {
+    const float inv = (float)J.nav;
+    float f[3] = {__fdiv_rn(fsum.x, inv), __fdiv_rn(fsum.y, inv), __fdiv_rn(fsum.z, inv)};
+    sc.dx = __fmul_rn((float)(step / J.nav), sc.V);
+    if (J.moveSurface) {
+        for (int c = 0; c < 3; ++c) sc.ig.micaR[c] = __fadd_rn(J.micaR0[c], __fmul_rn(J.dir[c], sc.dx));
+    } else {
+        for (int c = 0; c < 3; ++c) sc.chip[c] = __fadd_rn(J.chip0[c], __fmul_rn(J.dir[c], sc.dx));
+    }
+    float df[3];
+    for (int c = 0; c < 3; ++c) df[c] = __fadd_rn(-f[c], __fmul_rn(__fsub_rn(sc.chip[c], sc.ig.tip[c]), J.cantKs));
+    const float mult = __fdiv_rn(__fmul_rn(J.h, (float)J.nav), J.tipZeta);
+    if (J.fixTrans) {
+        float ct = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(mult, df[0]), J.dir[0]), __fmul_rn(__fmul_rn(mult, df[1]), J.dir[1])),
+                             __fmul_rn(__fmul_rn(mult, df[2]), J.dir[2]));
+        for (int c = 0; c < 3; ++c) sc.ig.tip[c] = __fadd_rn(sc.ig.tip[c], __fmul_rn(ct, J.dir[c]));
+    } else {
+        for (int c = 0; c < 3; ++c) sc.ig.tip[c] = __fadd_rn(sc.ig.tip[c], __fmul_rn(mult, df[c]));
+    }
+    sc.fav[0] = f[0];
+    sc.fav[1] = f[1];
+    sc.fav[2] = f[2];
+    sc.fav[3] = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], f[0]), __fmul_rn(f[1], f[1])), __fmul_rn(f[2], f[2])));
+}
+
+// The updaters of one `stride` boundary in the reference order
+// (creation order in src/gsop.cu:80-101; loop in src/gsop.cu:129-133).
+template <int BLOCK>
+__device__ void run_updaters(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, float* Ts, float (*red)[4],
+                             int64_t step, int& err) {
+    const int tid = threadIdx.x, n = J.n;
+    if (J.indent) {
+        if (tid == 0 && step == J.retraction_step) sc.V = -sc.V;
+        if (step % J.nav == 0) {
+            float3 p = make_float3(0.f, 0.f, 0.f);
+            for (int i = tid; i < n; i += BLOCK) {
+                float4 t = J.tipF[i];
+                p.x += t.x; p.y += t.y; p.z += t.z;
+                J.tipF[i] = make_float4(0.f, 0.f, 0.f, t.w);
+            }
+            const float3 s = block_sum3<BLOCK>(p, red);
+            if (tid == 0) tip_update(J, sc, s, step);
+        }
+    }
+    if (J.pulling && J.ramp && tid == 0) {
+        // PullingUpdater::update runs every stride (src/Potentials/pulling.cu:198-204)
+        const float xt = __fmul_rn(J.deltax, (float)(step / J.pull_freq));
+        const float4 xe = xs[J.pulledEnd];
+        const float xe3[3] = {xe.x, xe.y, xe.z};
+        for (int c = 0; c < 3; ++c) sc.pullF[c] = __fmul_rn(J.k_trans, __fsub_rn(sc.cant[c], xe3[c]));
+        for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
+    }
+    const bool pp = step % J.pp_freq == 0;
+    if (pp) build_possible<BLOCK>(J, xs, err);
+    if (step % J.nav == 0)
+        for (int i = tid; i < n; i += BLOCK) Ts[i] = 0.0f;   // output_manager.cu:125-127
+    if (step % J.pairs_freq == 0) {
+        if (pp) __syncthreads();
+        build_verlet<BLOCK>(J, xs, err);
+    }
+    if (J.heating && tid == 0 && step % J.temp_freq == 0) {
+        // TemperatureUpdater (src/Integrators/langevin.cu:129-135, 44-48)
+        const float temp = __fadd_rn(J.initialT, __fmul_rn((float)(step / J.temp_freq), J.deltaT));
+        sc.var = __fsqrt_rn(__fdiv_rn(__fmul_rn(__fmul_rn(2.0f, temp), J.zeta), J.h));
+    }
+    __syncthreads();
+}
+
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1)
+k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int64_t nsteps) {
+    JobDev* Jp = &jobs[ids[blockIdx.x]];
+    __shared__ JobDev Js;
+    load_job<BLOCK>(Js, Jp);
+    __syncthreads();
+    const JobDev& J = Js;
+    if (J.status != 0) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ StepScalars sc;
+    __shared__ float red[BLOCK / 32][4];
+    const int n = J.n, tid = threadIdx.x;
+    float4* xa = reinterpret_cast<float4*>(smem);
+    float4* xb = xa + n;
+    uint4* sd = reinterpret_cast<uint4*>(xb + n);
+    float* Ts = reinterpret_cast<float*>(sd + n);
+    for (int i = tid; i < n; i += BLOCK) {
+        xa[i] = J.x[i];
+        sd[i] = J.seeds[i];
+        Ts[i] = J.T[i];
+    }
+    if (tid == 0) {
+        sc.var = J.var;
+        for (int c = 0; c < 3; ++c) {
+            sc.pullF[c] = J.pullF[c];
+            sc.cant[c] = J.cant[c];
+            sc.ig.tip[c] = J.tip[c];
+            sc.ig.micaR[c] = J.micaR[c];
+            sc.ig.micaN[c] = J.micaN[c];
+            sc.chip[c] = J.chip[c];
+        }
+        sc.ig.tipR = J.tipR; sc.ig.tipAp = J.tipAp; sc.ig.tipBp = J.tipBp;
+        sc.ig.surfAp = J.surfAp; sc.ig.surfBp = J.surfBp;
+        sc.V = J.V; sc.dx = J.dx;
+        for (int c = 0; c < 4; ++c) sc.fav[c] = J.fav[c];
+        sc.err = 0;
+    }
+    __syncthreads();
+
+    const int lpb = J.lpb, g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
+    int err = 0;
+    int64_t step = J.step;
+    float4* xc = xa;
+    float4* xn = xb;
+    for (int64_t s = 0; s < nsteps; ++s, ++step) {
+        if (step % J.stride == 0) run_updaters<BLOCK>(J, sc, xc, Ts, red, step, err);
+        const float var = sc.var;
+        for (int base = 0; base < n; base += ng) {
+            const int i = base + g;
+            const bool act = i < n;
+            const float4 xi = xc[act ? i : 0];
+            float3 f = act ? bead_force_partial(J, xc, i, xi, l, lpb) : make_float3(0.f, 0.f, 0.f);
+            f = group_reduce(f, lpb);
+            if (act && l == 0) {
+                if (J.indent) {
+                    float3 tf;
+                    indentation_term(xi, sc.ig, f, tf);
+                    float4 t = J.tipF[i];
+                    t.x += tf.x; t.y += tf.y; t.z += tf.z;
+                    J.tipF[i] = t;
+                }
+                // integrateLangevin_kernel (src/Integrators/langevin_kernel.cu:17-58)
+                if (!J.minimization) {
+                    uint4 st = sd[i];
+                    const float4 gg = gaussian4(st);
+                    sd[i] = st;
+                    f.x += gg.x * var;
+                    f.y += gg.y * var;
+                    f.z += gg.z * var;
+                }
+                if (J.pulling) {
+                    const uint8_t fl = J.flags[i];
+                    if (fl == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
+                    if (fl == FLAG_PULLED) { f.x += sc.pullF[0]; f.y += sc.pullF[1]; f.z += sc.pullF[2]; }
+                }
+                const float dx = J.hOverZeta * f.x, dy = J.hOverZeta * f.y, dz = J.hOverZeta * f.z;
+                xn[i] = make_float4(xi.x + dx, xi.y + dy, xi.z + dz, xi.w);
+                Ts[i] += J.tempNorm * (dx * dx + dy * dy + dz * dz);
+            }
+        }
+        __syncthreads();
+        float4* t = xc; xc = xn; xn = t;
+    }
+    for (int i = tid; i < n; i += BLOCK) {
+        const float4 v = xc[i];
+        if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) err = 3;
+        J.x[i] = v;
+        J.seeds[i] = sd[i];
+        J.T[i] = Ts[i];
+    }
+    if (err) atomicMax(&sc.err, err);
+    __syncthreads();
+    if (tid == 0) {
+        Jp->step = step;
+        Jp->var = sc.var;
+        for (int c = 0; c < 3; ++c) {
+            Jp->pullF[c] = sc.pullF[c];
+            Jp->cant[c] = sc.cant[c];
+            Jp->tip[c] = sc.ig.tip[c];
+            Jp->micaR[c] = sc.ig.micaR[c];
+            Jp->chip[c] = sc.chip[c];
+        }
+        Jp->V = sc.V;
+        Jp->dx = sc.dx;
+        for (int c = 0; c < 4; ++c) Jp->fav[c] = sc.fav[c];
+        if (sc.err) Jp->status = sc.err;
+    }
+}
+
+// Potential forces only (SOPPotential::compute of every potential, no
+// integrator) at the job's current coordinates; for parity checks and
+// energy-free observables.  Does not touch the tip-force accumulator.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1)
+k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, float4* __restrict__ out) {
+    __shared__ JobDev Js;
+    load_job<BLOCK>(Js, &jobs[ids[blockIdx.x]]);
+    __syncthreads();
+    const JobDev& J = Js;
+    const int n = J.n, tid = threadIdx.x, lpb = J.lpb, g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
+    IndentGeom ig;
+    for (int c = 0; c < 3; ++c) { ig.tip[c] = J.tip[c]; ig.micaR[c] = J.micaR[c]; ig.micaN[c] = J.micaN[c]; }
+    ig.tipR = J.tipR; ig.tipAp = J.tipAp; ig.tipBp = J.tipBp; ig.surfAp = J.surfAp; ig.surfBp = J.surfBp;
+    for (int base = 0; base < n; base += ng) {
+        const int i = base + g;
+        const bool act = i < n;
+        const float4 xi = J.x[act ? i : 0];
+        float3 f = act ? bead_force_partial(J, J.x, i, xi, l, lpb) : make_float3(0.f, 0.f, 0.f);
+        f = group_reduce(f, lpb);
+        if (act && l == 0) {
+            if (J.indent) {
+                float3 tf;
+                indentation_term(xi, ig, f, tf);
+            }
+            out[i] = make_float4(f.x, f.y, f.z, 0.f);
+        }
+    }
+}
+
+// Rebuilds the possible-pairs and/or Verlet lists now, without the step gate.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1)
+k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int possible, int verlet) {
+    JobDev* Jp = &jobs[ids[blockIdx.x]];
+    __shared__ JobDev Js;
+    load_job<BLOCK>(Js, Jp);
+    const JobDev& J = Js;
+    __shared__ int errs;
+    if (threadIdx.x == 0) errs = 0;
+    __syncthreads();
+    int err = 0;
+    if (possible) build_possible<BLOCK>(J, J.x, err);
+    __syncthreads();
+    if (verlet) build_verlet<BLOCK>(J, J.x, err);
+    if (err) atomicMax(&errs, err);
+    __syncthreads();
+    if (threadIdx.x == 0 && errs) Jp->status = errs;
+}
+
+}  // namespace sopb

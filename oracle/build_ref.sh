@@ -18,3 +18,26 @@ mkdir -p "$OUT"
     "$REF/src/IO/topio.cpp" "$REF/src/IO/pdbio.cpp" \
     "$REF/src/Util/wrapper.cpp" "$REF/src/Util/mystl.cpp"
 echo "built $OUT/ref_host"
+
+# The reference's CUDA path for sm_100a (golden harness ref_gpu).  As
+# shipped it targets sm_30 with texture references, both gone from CUDA 12:
+# -DNOTEXTURE selects its plain-load path and ref_texture_shim.h covers the
+# TEA integrator's three texture references.  Flags otherwise follow the
+# reference Makefile (-O3, -use_fast_math).
+NVCC=/usr/local/cuda/bin/nvcc
+if [ -x "$NVCC" ]; then
+    OBJ="$OUT/obj"
+    mkdir -p "$OBJ"
+    "$NVCC" -O3 -gencode arch=compute_100a,code=sm_100a -use_fast_math -w -DNOTEXTURE \
+        -ccbin /usr/bin/g++ -include "$HERE/ref_texture_shim.h" -I"$REF/src" \
+        -c "$REF/src/gsop.cu" -o "$OBJ/gsop.o"
+    for f in Integrators/ran2.cpp IO/dcdio.cpp IO/pdbio.cpp IO/topio.cpp IO/configreader.cpp \
+             Util/wrapper.cpp Util/mystl.cpp Util/parameters.cpp Updaters/dcd_manager.cpp; do
+        /usr/bin/g++ -O3 -w -DNOTEXTURE -I"$REF/src" -I/usr/local/cuda/include -c "$REF/src/$f" \
+            -o "$OBJ/$(basename "$f" .cpp).o"
+    done
+    /usr/bin/g++ -O2 -w -DNOTEXTURE -I"$REF/src" -I/usr/local/cuda/include -c "$HERE/ref_gpu_harness.cpp" \
+        -o "$OBJ/ref_gpu_harness.o"
+    /usr/bin/g++ -o "$OUT/ref_gpu" "$OBJ"/*.o -L/usr/local/cuda/lib64 -lcudart -lrt -lm -ldl -lpthread
+    echo "built $OUT/ref_gpu"
+fi

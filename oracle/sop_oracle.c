@@ -458,8 +458,11 @@ void orc_job_forces(orc_job* j, float* out4, double* out4d, double* abs4d) {
                 double d[3] = {(double)xj[0] - xi[0], (double)xj[1] - xi[1], (double)xj[2] - xi[2]};
                 double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
                 double dl = r - j->cov_r0[s];
-                double w = (double)j->ks * dl / (r * (1.0 - dl * dl / ((double)j->p.R_limit * j->p.R_limit)));
-                for (int c = 0; c < 3; c++) { fd[c] += w * d[c]; fa[c] += fabs(w * d[c]); }
+                double R2 = (double)j->p.R_limit * j->p.R_limit, q = 1.0 - dl * dl / R2;
+                double w = (double)j->ks * dl / (r * q);
+                /* rounding scale: r - r0 cancels (|r| + |r0|) and so does q */
+                double sc = fabs((double)j->ks * (r + j->cov_r0[s]) / (r * q)) + fabs(w) * (1.0 + dl * dl / R2) / fabs(q);
+                for (int c = 0; c < 3; c++) { fd[c] += w * d[c]; fa[c] += sc * fabs(d[c]); }
             }
             for (int32_t k = 0; k < j->nat_cnt[i]; k++) {
                 int32_t s = i * j->cap_nat + k;
@@ -468,8 +471,11 @@ void orc_job_forces(orc_job* j, float* out4, double* out4d, double* abs4d) {
                 double r0 = j->nat_r0d[s];
                 double q = r0 * r0 / (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
                 double p6 = q * q * q;
-                double w = q * (p6 * p6 - p6) * (-12.0 * j->nat_ehd[s] / (r0 * r0));
-                for (int c = 0; c < 3; c++) { fd[c] += w * d[c]; fa[c] += fabs(w * d[c]); }
+                double m12 = -12.0 * j->nat_ehd[s] / (r0 * r0);
+                double w = q * (p6 * p6 - p6) * m12;
+                /* p6^2 - p6 cancels at r = r0: scale by |p6^2| + |p6| */
+                double sc = q * (p6 * p6 + p6) * fabs(m12);
+                for (int c = 0; c < 3; c++) { fd[c] += w * d[c]; fa[c] += sc * fabs(d[c]); }
             }
             for (int32_t k = 0; k < j->pl_cnt[i]; k++) {
                 const float* xj = F4(j->x, j->pl_j[(size_t)i * j->cap_pl + k]);
@@ -490,10 +496,16 @@ void orc_job_forces(orc_job* j, float* out4, double* out4d, double* abs4d) {
                 double dd = m[0] * j->micaN[0] + m[1] * j->micaN[1] + m[2] * j->micaN[2];
                 double s6 = 1.0 / (dd * dd * dd * dd * dd * dd);
                 double ws = ((double)j->surfAp * s6 + j->surfBp) * s6 / (dd * dd);
+                /* r - R_tip and the surface distance cancel: scale by the
+                 * magnitudes that are subtracted */
+                double stip = fabs(w) * 7.0 * (r + j->tipR) / fabs(rho);
+                double mabs = fabs((double)xi[0] * j->micaN[0]) + fabs((double)xi[1] * j->micaN[1]) + fabs((double)xi[2] * j->micaN[2])
+                            + fabs((double)j->micaR[0] * j->micaN[0]) + fabs((double)j->micaR[1] * j->micaN[1]) + fabs((double)j->micaR[2] * j->micaN[2]);
+                double ssurf = fabs(ws) * 8.0 * mabs / fabs(dd);
                 for (int c = 0; c < 3; c++) {
                     double t = w * d[c] + ws * j->micaN[c];
                     fd[c] += t;
-                    fa[c] += fabs(w * d[c]) + fabs(ws * j->micaN[c]);
+                    fa[c] += stip * fabs(d[c]) + ssurf * fabs(j->micaN[c]);
                 }
             }
             if (out4d) { for (int c = 0; c < 3; c++) out4d[4 * i + c] = fd[c]; out4d[4 * i + 3] = 0; }

@@ -42,8 +42,9 @@ int orc_job_advance(orc_job* job, int64_t nsteps);
 /* Advances many jobs on `nthreads` OpenMP threads (one job per thread). */
 int orc_jobs_advance(orc_job** jobs, int32_t njobs, int64_t nsteps, int32_t nthreads);
 /* Potential forces at the current coordinates, FP32 (out4) and FP64 (out4d),
- * plus the sum of the absolute values of every term (abs4d) for a
- * condition-aware error bound.  Any output may be NULL. */
+ * plus per component the FP32 rounding scale (abs4d): the magnitudes of the
+ * quantities each term subtracts, for a condition-aware relative error.
+ * Any output may be NULL. */
 void orc_job_forces(orc_job* job, float* out4, double* out4d, double* abs4d);
 void orc_job_read(const orc_job* job, int32_t what, void* out);
 void orc_job_write(orc_job* job, int32_t what, const void* in);

@@ -84,6 +84,7 @@ struct sopb_context {
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[kSideStreams] = {};
     int32_t last_error = SOPB_OK;
+    int smem_dyn_max = 1 << 30;   // dynamic shared memory available to the resident kernel
 };
 
 struct sopb_job {
@@ -108,10 +109,18 @@ struct sopb_job {
 
 namespace {
 
-template <int B>
-int set_smem_attr() {
-    const int maxsm = 227 * 1024;
-    CUDA_TRY(cudaFuncSetAttribute(k_resident_steps<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
+// Opt the resident kernel in to the largest dynamic shared memory the device
+// allows next to the kernel's static shared memory.
+template <int B, bool M>
+int set_smem_attr(int device, int* dyn_out) {
+    int optin = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    cudaFuncAttributes fa;
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k_resident_steps<B, M>));
+    const int dyn = optin - (int)fa.sharedSizeBytes;
+    if (dyn < kMaxResidentBeads * kResidentSmemPerBead) return SOPB_ERR_UNSUPPORTED;
+    CUDA_TRY(cudaFuncSetAttribute(k_resident_steps<B, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    if (dyn < *dyn_out) *dyn_out = dyn;
     return SOPB_OK;
 }
 
@@ -131,38 +140,37 @@ void launch_shape(int32_t n, int32_t lpb_req, int32_t* lpb, int32_t* block) {
     *block = b;
 }
 
-int launch_resident(int block, int grid, size_t smem, cudaStream_t st, JobDev* jobs, const int32_t* ids, int64_t nsteps) {
-    switch (block) {
-    case 128: k_resident_steps<128><<<grid, 128, smem, st>>>(jobs, ids, nsteps); break;
-    case 256: k_resident_steps<256><<<grid, 256, smem, st>>>(jobs, ids, nsteps); break;
-    case 512: k_resident_steps<512><<<grid, 512, smem, st>>>(jobs, ids, nsteps); break;
-    case 1024: k_resident_steps<1024><<<grid, 1024, smem, st>>>(jobs, ids, nsteps); break;
-    default: return SOPB_ERR_INVALID;
+#define SOPB_BLOCK_SWITCH(block, MASK, LAUNCH)             \
+    switch (block) {                                     \
+    case 128: LAUNCH(128, MASK); break;                  \
+    case 256: LAUNCH(256, MASK); break;                  \
+    case 512: LAUNCH(512, MASK); break;                  \
+    case 1024: LAUNCH(1024, MASK); break;                \
+    default: return SOPB_ERR_INVALID;                    \
     }
+
+int launch_resident(int block, bool mask, int grid, size_t smem, cudaStream_t st, JobDev* jobs, const int32_t* ids,
+                    int64_t nsteps) {
+#define L_RES(B, M) k_resident_steps<B, M><<<grid, B, smem, st>>>(jobs, ids, nsteps)
+    if (mask) { SOPB_BLOCK_SWITCH(block, true, L_RES) } else { SOPB_BLOCK_SWITCH(block, false, L_RES) }
+#undef L_RES
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
 
-int launch_forces(int block, int grid, cudaStream_t st, const JobDev* jobs, const int32_t* ids, float4* out) {
-    switch (block) {
-    case 128: k_forces_only<128><<<grid, 128, 0, st>>>(jobs, ids, out); break;
-    case 256: k_forces_only<256><<<grid, 256, 0, st>>>(jobs, ids, out); break;
-    case 512: k_forces_only<512><<<grid, 512, 0, st>>>(jobs, ids, out); break;
-    case 1024: k_forces_only<1024><<<grid, 1024, 0, st>>>(jobs, ids, out); break;
-    default: return SOPB_ERR_INVALID;
-    }
+int launch_forces(int block, bool mask, int grid, cudaStream_t st, const JobDev* jobs, const int32_t* ids, float4* out) {
+#define L_FRC(B, M) k_forces_only<B, M><<<grid, B, 0, st>>>(jobs, ids, out)
+    if (mask) { SOPB_BLOCK_SWITCH(block, true, L_FRC) } else { SOPB_BLOCK_SWITCH(block, false, L_FRC) }
+#undef L_FRC
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
 
-int launch_rebuild(int block, int grid, cudaStream_t st, JobDev* jobs, const int32_t* ids, int possible, int verlet) {
-    switch (block) {
-    case 128: k_rebuild_lists<128><<<grid, 128, 0, st>>>(jobs, ids, possible, verlet); break;
-    case 256: k_rebuild_lists<256><<<grid, 256, 0, st>>>(jobs, ids, possible, verlet); break;
-    case 512: k_rebuild_lists<512><<<grid, 512, 0, st>>>(jobs, ids, possible, verlet); break;
-    case 1024: k_rebuild_lists<1024><<<grid, 1024, 0, st>>>(jobs, ids, possible, verlet); break;
-    default: return SOPB_ERR_INVALID;
-    }
+int launch_rebuild(int block, bool mask, int grid, cudaStream_t st, JobDev* jobs, const int32_t* ids, int possible,
+                   int verlet) {
+#define L_REB(B, M) k_rebuild_lists<B, M><<<grid, B, 0, st>>>(jobs, ids, possible, verlet)
+    if (mask) { SOPB_BLOCK_SWITCH(block, true, L_REB) } else { SOPB_BLOCK_SWITCH(block, false, L_REB) }
+#undef L_REB
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
@@ -243,8 +251,11 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
     }
     CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     int rc;
-    if ((rc = set_smem_attr<128>()) || (rc = set_smem_attr<256>()) || (rc = set_smem_attr<512>()) ||
-        (rc = set_smem_attr<1024>()))
+    int* dm = &c->smem_dyn_max;
+    if ((rc = set_smem_attr<128, false>(device, dm)) || (rc = set_smem_attr<256, false>(device, dm)) ||
+        (rc = set_smem_attr<512, false>(device, dm)) || (rc = set_smem_attr<1024, false>(device, dm)) ||
+        (rc = set_smem_attr<128, true>(device, dm)) || (rc = set_smem_attr<256, true>(device, dm)) ||
+        (rc = set_smem_attr<512, true>(device, dm)) || (rc = set_smem_attr<1024, true>(device, dm)))
         return rc;
     *out = c;
     return SOPB_OK;
@@ -480,18 +491,37 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     if (d->seeds) std::memcpy(seeds.data(), d->seeds, seeds.size() * 4);
     else sopb_generate_seeds(d->seed, n, seeds.data());
 
+    // list representation: bitmasks when the Verlet masks fit in shared memory
+    h.W = (n + 31) / 32;
+    h.mask = resident_smem_bytes(n, h.W, true) <= (size_t)c->smem_dyn_max ? 1 : 0;
+    h.max_pp = p.max_possiblePairs > 0 ? p.max_possiblePairs : 4096;
+    h.max_pl = p.max_pairs > 0 ? p.max_pairs : 512;
+    // exclusion mask: self, covalent and native partners (the linear scans of
+    // possiblepairlist_kernel.cu:47-59, precomputed)
+    std::vector<uint32_t> ex((size_t)n * h.W, 0u);
+    auto excl = [&](int32_t i, int32_t q) { ex[(size_t)i * h.W + (q >> 5)] |= 1u << (q & 31); };
+    for (int32_t i = 0; i < n; ++i) excl(i, i);
+    for (int32_t i = 0; i < n; ++i) {
+        for (int32_t k = m.cov_off[i]; k < m.cov_off[i + 1]; ++k) excl(i, m.cov_j[k]);
+        for (int32_t k = m.nat_off[i]; k < m.nat_off[i + 1]; ++k) excl(i, m.nat_j[k]);
+    }
+
     // device block for the maps and lists
+    const size_t mask_bytes = (size_t)n * h.W * 4;
     const size_t o_covoff = 0;
     const size_t o_covj = o_covoff + align256((n + 1) * 4);
     const size_t o_covr0 = o_covj + align256(m.cov_j.size() * 4 + 4);
     const size_t o_natoff = o_covr0 + align256(m.cov_r0.size() * 4 + 4);
     const size_t o_natj = o_natoff + align256((n + 1) * 4);
     const size_t o_natpar = o_natj + align256(m.nat_j.size() * 4 + 4);
-    const size_t o_ppcnt = o_natpar + align256(m.nat_par.size() * 8 + 8);
+    const size_t o_ex = o_natpar + align256(m.nat_par.size() * 8 + 8);
+    const size_t o_ppm = o_ex + align256(mask_bytes);
+    const size_t o_plm = o_ppm + (h.mask ? align256(mask_bytes) : 0);
+    const size_t o_ppcnt = o_plm + (h.mask ? align256(mask_bytes) : 0);
     const size_t o_plcnt = o_ppcnt + align256((size_t)n * 4);
     const size_t o_ppj = o_plcnt + align256((size_t)n * 4);
-    const size_t o_plj = o_ppj + align256((size_t)n * h.cap_pp * 4);
-    const size_t total = o_plj + align256((size_t)n * h.cap_pl * 4);
+    const size_t o_plj = o_ppj + (h.mask ? 0 : align256((size_t)n * h.cap_pp * 4));
+    const size_t total = o_plj + (h.mask ? 0 : align256((size_t)n * h.cap_pl * 4));
     sopb_job* j = new (std::nothrow) sopb_job();
     if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
     cudaError_t e = cudaMalloc(&j->dmem, total);
@@ -508,10 +538,13 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.nat_off = (int32_t*)(base + o_natoff);
     h.nat_j = (int32_t*)(base + o_natj);
     h.nat_par = (float2*)(base + o_natpar);
+    h.ex_mask = (uint32_t*)(base + o_ex);
+    h.pp_mask = h.mask ? (uint32_t*)(base + o_ppm) : nullptr;
+    h.pl_mask = h.mask ? (uint32_t*)(base + o_plm) : nullptr;
     h.pp_cnt = (int32_t*)(base + o_ppcnt);
     h.pl_cnt = (int32_t*)(base + o_plcnt);
-    h.pp_j = (int32_t*)(base + o_ppj);
-    h.pl_j = (int32_t*)(base + o_plj);
+    h.pp_j = h.mask ? nullptr : (int32_t*)(base + o_ppj);
+    h.pl_j = h.mask ? nullptr : (int32_t*)(base + o_plj);
     h.x = c->x + b0;
     h.xalt = c->xalt + b0;
     h.seeds = c->seeds + b0;
@@ -519,7 +552,8 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.tipF = c->tipF + b0;
     h.flags = c->flags + b0;
     cudaStream_t st = c->stream;
-    CUDA_TRY(cudaMemsetAsync(base + o_ppcnt, 0, (size_t)n * 8 + 512, st));
+    CUDA_TRY(cudaMemsetAsync(base + o_ppm, 0, o_ppj - o_ppm, st));   // masks and counts
+    CUDA_TRY(cudaMemcpyAsync(h.ex_mask, ex.data(), mask_bytes, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(h.cov_off, m.cov_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
     if (!m.cov_j.empty()) {
         CUDA_TRY(cudaMemcpyAsync(h.cov_j, m.cov_j.data(), m.cov_j.size() * 4, cudaMemcpyHostToDevice, st));
@@ -567,19 +601,24 @@ namespace {
 // Groups jobs by CTA size class; returns (block, ids) per class, largest
 // jobs' class first so the longest CTAs start first.
 struct LaunchClass {
-    int block;
-    int32_t max_n;
+    int block = 0;
+    bool mask = false;
+    int32_t max_n = 0;
+    size_t smem = 0;
     std::vector<int32_t> ids;
 };
 void group_jobs(sopb_job* const* jobs, int32_t njobs, std::vector<LaunchClass>& out) {
-    std::map<int, LaunchClass> cls;
+    std::map<int, LaunchClass> cls;   // key: block * 2 + mask
     std::vector<int32_t> order(njobs);
     for (int32_t k = 0; k < njobs; ++k) order[k] = k;
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return jobs[a]->n > jobs[b]->n; });
     for (int32_t k : order) {
-        LaunchClass& L = cls[jobs[k]->h.block];
-        L.block = jobs[k]->h.block;
+        const JobDev& h = jobs[k]->h;
+        LaunchClass& L = cls[h.block * 2 + h.mask];
+        L.block = h.block;
+        L.mask = h.mask != 0;
         L.max_n = std::max(L.max_n, jobs[k]->n);
+        L.smem = std::max(L.smem, resident_smem_bytes(jobs[k]->n, h.W, L.mask));
         L.ids.push_back(jobs[k]->slot);
     }
     out.clear();
@@ -607,15 +646,14 @@ extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, i
     CUDA_TRY(cudaMemcpyAsync(c->d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->stream));
     if (cls.size() == 1) {
         const LaunchClass& L = cls[0];
-        return launch_resident(L.block, (int)L.ids.size(), (size_t)L.max_n * kResidentSmemPerBead, c->stream, c->d_jobs,
-                               c->d_ids, nsteps);
+        return launch_resident(L.block, L.mask, (int)L.ids.size(), L.smem, c->stream, c->d_jobs, c->d_ids, nsteps);
     }
     CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
     for (size_t k = 0; k < cls.size(); ++k) {
         cudaStream_t s = c->side[k % kSideStreams];
         CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
-        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), (size_t)cls[k].max_n * kResidentSmemPerBead, s,
-                             c->d_jobs, c->d_ids + off[k], nsteps);
+        rc = launch_resident(cls[k].block, cls[k].mask, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs,
+                             c->d_ids + off[k], nsteps);
         if (rc) return rc;
     }
     for (int k = 0; k < kSideStreams && k < (int)cls.size(); ++k) {
@@ -681,7 +719,7 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         if (rc) return rc;
         const int32_t id = j->slot;
         CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
-        rc = launch_forces(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, c->d_scratch4);
+        rc = launch_forces(j->h.block, j->h.mask != 0, 1, c->stream, c->d_jobs, c->d_ids, c->d_scratch4);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(out, c->d_scratch4, n * 16, cudaMemcpyDeviceToHost, c->stream));
         break;
@@ -736,6 +774,24 @@ extern "C" int sopb_job_pairlist(sopb_job* j, int32_t possible, int32_t* counts,
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
     const int32_t n = j->n;
+    if (j->h.mask) {
+        const int32_t W = j->h.W;
+        std::vector<uint32_t> msk((size_t)n * W);
+        CUDA_TRY(cudaMemcpyAsync(msk.data(), possible ? j->h.pp_mask : j->h.pl_mask, msk.size() * 4,
+                                 cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (int32_t i = 0; i < n; ++i) {
+            int32_t k = 0;
+            for (int32_t q = 0; q < n; ++q)
+                if ((msk[(size_t)i * W + (q >> 5)] >> (q & 31)) & 1u) {
+                    if (k < cap) rows[(size_t)i * cap + k] = q;
+                    ++k;
+                }
+            counts[i] = k;
+            for (int32_t r = k; r < cap; ++r) rows[(size_t)i * cap + r] = -1;
+        }
+        return SOPB_OK;
+    }
     const int32_t lcap = possible ? j->h.cap_pp : j->h.cap_pl;
     std::vector<int32_t> cnt(n), lst((size_t)n * lcap);
     CUDA_TRY(cudaMemcpyAsync(cnt.data(), possible ? j->h.pp_cnt : j->h.pl_cnt, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -756,7 +812,7 @@ extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t ver
     if (rc) return rc;
     const int32_t id = j->slot;
     CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
-    rc = launch_rebuild(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, possible, verlet);
+    rc = launch_rebuild(j->h.block, j->h.mask != 0, 1, c->stream, c->d_jobs, c->d_ids, possible, verlet);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return SOPB_OK;

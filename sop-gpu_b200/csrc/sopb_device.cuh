@@ -5,15 +5,20 @@
 // reference).  Per-bead state lives in context-wide bead pools (coordinates,
 // RNG states, temperature accumulator, flags) so a batch's coordinates move
 // with one copy; the neighbour maps of a job are CSR (covalent, native) or
-// fixed-capacity rows (possible pairs, Verlet pairs).
+// either bitmasks over the job's beads or fixed-capacity index rows
+// (possible pairs, Verlet pairs).
 #pragma once
 
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "../../include/sopb.h"
+
 namespace sopb {
 
 enum : int { FLAG_FREE = 0, FLAG_FIXED = 1, FLAG_PULLED = 2 };
+constexpr int SOPB_STATUS_CAPACITY = SOPB_ERR_CAPACITY;
+constexpr int SOPB_STATUS_NONFINITE = SOPB_ERR_NONFINITE;
 
 struct JobDev {
     // ---- sizes and schedule ------------------------------------------------
@@ -22,6 +27,10 @@ struct JobDev {
     int32_t block;        // CTA size class of the resident kernel
     int32_t cap_pp;       // possible-pairs row capacity
     int32_t cap_pl;       // Verlet row capacity
+    int32_t mask;         // 1: bitmask lists (shared-memory Verlet masks)
+    int32_t W;            // words per bitmask row, ceil(n/32)
+    int32_t max_pp;       // configured max_possiblePairs (overflow -> error)
+    int32_t max_pl;       // configured max_pairs
     int32_t stride;       // updater period (gsop.cu:117-122)
     int32_t nav;
     int32_t pairs_freq;
@@ -49,6 +58,9 @@ struct JobDev {
     int32_t* pp_j;        // [n * cap_pp]
     int32_t* pl_cnt;      // [n]
     int32_t* pl_j;        // [n * cap_pl]
+    uint32_t* ex_mask;    // [n * W] bonded + native partners and self
+    uint32_t* pp_mask;    // [n * W] possible pairs (MASK mode)
+    uint32_t* pl_mask;    // [n * W] Verlet pairs (MASK mode, between launches)
     // ---- force field ---------------------------------------------------------
     float ks, R2;         // FENE: kspring_cov, R_limit^2
     float a2, m6, cut2;   // repulsive: a^2, -6 el / a^2, pairs_cutoff^2
@@ -121,10 +133,13 @@ __device__ __forceinline__ bool within_cutoff(float4 xi, float4 xj, float cut) {
 }
 
 // FENE term (covalent_kernel.cu:28-51): Ks*(r-r0)/(r*(1-(r-r0)^2/R0^2)).
+// r - r0 cancels for a near-relaxed bond, so r is formed with a correctly
+// rounded square root (the reference's fast-math build uses the approximate
+// one and loses ~1e-4 of the bond force there).
 __device__ __forceinline__ void fene_term(float4 xi, float4 xj, float r0, float ks, float R2, float3& f) {
     float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    float w = sqrtf(dx * dx + dy * dy + dz * dz) - r0;
-    w = ks * w / ((w + r0) * (1.0f - w * w / R2));
+    float w = __fsqrt_rn(dx * dx + dy * dy + dz * dz) - r0;
+    w = __fdiv_rn(ks * w, (w + r0) * (1.0f - __fdiv_rn(w * w, R2)));
     f.x += w * dx;
     f.y += w * dy;
     f.z += w * dz;
@@ -161,8 +176,8 @@ struct IndentGeom {
 };
 __device__ __forceinline__ void indentation_term(float4 xi, const IndentGeom& g, float3& f, float3& tipf) {
     float dx = xi.x - g.tip[0], dy = xi.y - g.tip[1], dz = xi.z - g.tip[2];
-    float dw = sqrtf(dx * dx + dy * dy + dz * dz);
-    float r2 = 1.0f / (dw - g.tipR);
+    float dw = __fsqrt_rn(dx * dx + dy * dy + dz * dz);
+    float r2 = __frcp_rn(dw - g.tipR);
     r2 = r2 * r2;
     float r6 = r2 * r2 * r2;
     float w = g.tipAp * r6 + g.tipBp;

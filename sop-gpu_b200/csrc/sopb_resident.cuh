@@ -9,18 +9,27 @@
 // and copies all coordinates to the host every `stride` steps for pulling,
 // src/Potentials/pulling.cu:152-165).
 //
+// Neighbour lists, two representations chosen per job:
+//   MASK  (jobs whose bitmasks fit in shared memory, n <= ~1100): the Verlet
+//         list of bead i is a bitmask over the job's beads held in shared
+//         memory (n*ceil(n/32) words), the possible-pairs list a bitmask in
+//         global memory, bonded/native exclusions a precomputed bitmask.
+//         Set bits are visited in increasing j, the reference's list order.
+//   ROWS  (larger jobs): fixed-capacity index rows in global memory, the
+//         reference's layout transposed to bead-major.
+//
 // Work split: `lpb` lanes (a power of two <= 32, aligned inside a warp)
 // cooperate on one bead: they stride over its covalent, native and Verlet
-// lists and combine their partial forces with xor-shuffles; lane 0 then draws
-// the bead's noise and integrates.  All loops that contain warp collectives
-// have CTA-uniform trip counts.
+// entries (mask words) and combine partial forces with xor-shuffles; lane 0
+// then draws the bead's noise and integrates.  Loops containing warp
+// collectives have CTA-uniform trip counts.
 #pragma once
 
 #include "sopb_device.cuh"
 
 namespace sopb {
 
-constexpr int kMaxResidentBeads = 4096;     // 52 B of shared memory per bead
+constexpr int kMaxResidentBeads = 4096;     // ROWS mode: 52 B of shared memory per bead
 constexpr int kResidentSmemPerBead = 52;
 
 struct StepScalars {
@@ -48,22 +57,6 @@ __device__ __forceinline__ unsigned group_mask(int lpb) {
     return lpb == 32 ? 0xffffffffu : ((1u << lpb) - 1u);
 }
 
-// Partial force of lane `l` of the group working on bead i: covalent, then
-// native, then Verlet pairs, each list strided by lpb (the reference sums
-// the three kernels' contributions in this order, gsop.cu:80-85).
-__device__ __forceinline__ float3 bead_force_partial(const JobDev& J, const float4* __restrict__ xs, int i, float4 xi,
-                                                     int l, int lpb) {
-    float3 f = make_float3(0.f, 0.f, 0.f);
-    const int c0 = J.cov_off[i], c1 = J.cov_off[i + 1];
-    for (int k = c0 + l; k < c1; k += lpb) fene_term(xi, xs[J.cov_j[k]], J.cov_r0[k], J.ks, J.R2, f);
-    const int n0 = J.nat_off[i], n1 = J.nat_off[i + 1];
-    for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[J.nat_j[k]], J.nat_par[k], f);
-    const int np = J.pl_cnt[i];
-    const int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
-    for (int k = l; k < np; k += lpb) pair_term(xi, xs[row[k]], J.a2, J.m6, J.cut2, f);
-    return f;
-}
-
 __device__ __forceinline__ float3 group_reduce(float3 f, int lpb) {
     for (int o = lpb >> 1; o > 0; o >>= 1) {
         f.x += __shfl_xor_sync(0xffffffffu, f.x, o);
@@ -73,81 +66,146 @@ __device__ __forceinline__ float3 group_reduce(float3 f, int lpb) {
     return f;
 }
 
-__device__ __forceinline__ bool excluded(const JobDev& J, int i, int q) {
-    for (int k = J.cov_off[i]; k < J.cov_off[i + 1]; ++k)
-        if (J.cov_j[k] == q) return true;
-    for (int k = J.nat_off[i]; k < J.nat_off[i + 1]; ++k)
-        if (J.nat_j[k] == q) return true;
-    return false;
+__device__ __forceinline__ int group_sum(int v, int lpb) {
+    for (int o = lpb >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Covalent then native terms of bead i, strided over the group's lanes
+// (the reference sums its kernels' contributions in this order,
+// src/gsop.cu:80-85).  The maps are read-only for a launch.
+__device__ __forceinline__ void bonded_partial(const JobDev& J, const float4* __restrict__ xs, int i, float4 xi, int l,
+                                               int lpb, float3& f) {
+    const int c0 = __ldg(&J.cov_off[i]), c1 = __ldg(&J.cov_off[i + 1]);
+    for (int k = c0 + l; k < c1; k += lpb) fene_term(xi, xs[__ldg(&J.cov_j[k])], __ldg(&J.cov_r0[k]), J.ks, J.R2, f);
+    const int n0 = __ldg(&J.nat_off[i]), n1 = __ldg(&J.nat_off[i + 1]);
+    for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[__ldg(&J.nat_j[k])], __ldg(&J.nat_par[k]), f);
+}
+
+// Verlet-pair terms: ROWS mode walks the bead's index row; MASK mode walks
+// the set bits of its mask words (lane l takes words l, l+lpb, ...).
+template <bool MASK>
+__device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const uint32_t* vm, int i,
+                                              float4 xi, int l, int lpb, float3& f) {
+    if (MASK) {
+        const uint32_t* row = vm + (size_t)i * J.W;
+        for (int w = l; w < J.W; w += lpb) {
+            uint32_t m = row[w];
+            const float4* xw = xs + 32 * w;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                pair_term(xi, xw[b], J.a2, J.m6, J.cut2, f);
+            }
+        }
+    } else {
+        const int np = J.pl_cnt[i];
+        const int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
+        for (int k = l; k < np; k += lpb) pair_term(xi, xs[row[k]], J.a2, J.m6, J.cut2, f);
+    }
 }
 
 // generate_possiblepairs (src/Updaters/possiblepairlist_kernel.cu:18-71):
-// every q != i of the job with |r| < pairs_threshold that is neither a
-// covalent nor a native partner, appended in increasing q.  Ballot
-// compaction inside the group keeps the order.  Overflow sets err.
-template <int BLOCK>
+// every q of the job with |r| < pairs_threshold that is neither i nor a
+// covalent or native partner.  More than max_possiblePairs sets err (the
+// reference writes past its rows there).
+template <int BLOCK, bool MASK>
 __device__ void build_possible(const JobDev& J, const float4* __restrict__ xs, int& err) {
     const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
     const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
-    const int gbase = (tid & 31) & ~(lpb - 1);
-    const unsigned gm = group_mask(lpb);
     for (int base = 0; base < n; base += ng) {
         const int i = base + g;
         const bool act = i < n;
         const float4 xi = xs[act ? i : 0];
-        int32_t* row = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
         int cnt = 0;
-        for (int qb = 0; qb < n; qb += lpb) {
-            const int q = qb + l;
-            bool ok = act && q < n && q != i && within_cutoff(xi, xs[q < n ? q : 0], J.pp_thr);
-            if (ok) ok = !excluded(J, i, q);
-            const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
-            if (ok) {
-                const int pos = cnt + __popc(m & ((1u << l) - 1u));
-                if (pos < J.cap_pp) row[pos] = q;
-                else err = 2;
+        if (MASK) {
+            if (act) {
+                for (int w = l; w < J.W; w += lpb) {
+                    uint32_t bits = 0;
+                    const int q0 = 32 * w;
+                    const int qn = min(32, n - q0);
+                    for (int b = 0; b < qn; ++b)
+                        if (within_cutoff(xi, xs[q0 + b], J.pp_thr)) bits |= 1u << b;
+                    bits &= ~__ldg(&J.ex_mask[(size_t)i * J.W + w]);
+                    J.pp_mask[(size_t)i * J.W + w] = bits;
+                    cnt += __popc(bits);
+                }
             }
-            cnt += __popc(m);
+            cnt = group_sum(cnt, lpb);
+            if (act && l == 0 && cnt > J.max_pp) err = SOPB_STATUS_CAPACITY;
+        } else {
+            const int gbase = (tid & 31) & ~(lpb - 1);
+            const unsigned gm = group_mask(lpb);
+            int32_t* row = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
+            const uint32_t* ex = J.ex_mask ? J.ex_mask + (size_t)(act ? i : 0) * J.W : nullptr;
+            for (int qb = 0; qb < n; qb += lpb) {
+                const int q = qb + l;
+                bool ok = act && q < n && within_cutoff(xi, xs[q < n ? q : 0], J.pp_thr);
+                if (ok) ok = !((__ldg(&ex[q >> 5]) >> (q & 31)) & 1u);
+                const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
+                if (ok) {
+                    const int pos = cnt + __popc(m & ((1u << l) - 1u));
+                    if (pos < J.cap_pp) row[pos] = q;
+                    else err = SOPB_STATUS_CAPACITY;
+                }
+                cnt += __popc(m);
+            }
+            if (act && l == 0) J.pp_cnt[i] = cnt < J.cap_pp ? cnt : J.cap_pp;
         }
-        if (act && l == 0) J.pp_cnt[i] = cnt < J.cap_pp ? cnt : J.cap_pp;
     }
 }
 
 // generate_pairs (src/Updaters/pairlist_kernel.cu:33-76): the possible pairs
-// with |r| < pairlist_cutoff, order kept.  The reference pads rows with -1
-// every rebuild; rows here are read only up to their count.
-template <int BLOCK>
-__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int& err) {
+// with |r| < pairlist_cutoff, order kept.  More than max_pairs sets err.
+template <int BLOCK, bool MASK>
+__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, uint32_t* vm, int& err) {
     const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
     const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
-    const int gbase = (tid & 31) & ~(lpb - 1);
-    const unsigned gm = group_mask(lpb);
     for (int base = 0; base < n; base += ng) {
         const int i = base + g;
         const bool act = i < n;
         const float4 xi = xs[act ? i : 0];
-        const int npp = act ? J.pp_cnt[i] : 0;
-        const int32_t* prow = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
-        int32_t* row = J.pl_j + (size_t)(act ? i : 0) * J.cap_pl;
-        const int kmax = __reduce_max_sync(0xffffffffu, npp);
         int cnt = 0;
-        for (int kb = 0; kb < kmax; kb += lpb) {
-            const int k = kb + l;
-            int q = 0;
-            bool ok = k < npp;
-            if (ok) {
-                q = prow[k];
-                ok = within_cutoff(xi, xs[q], J.pl_cut);
+        if (MASK) {
+            if (act) {
+                for (int w = l; w < J.W; w += lpb) {
+                    uint32_t m = J.pp_mask[(size_t)i * J.W + w], out = 0;
+                    while (m) {
+                        const int b = __ffs(m) - 1;
+                        m &= m - 1;
+                        if (within_cutoff(xi, xs[32 * w + b], J.pl_cut)) out |= 1u << b;
+                    }
+                    vm[(size_t)i * J.W + w] = out;
+                    cnt += __popc(out);
+                }
             }
-            const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
-            if (ok) {
-                const int pos = cnt + __popc(m & ((1u << l) - 1u));
-                if (pos < J.cap_pl) row[pos] = q;
-                else err = 2;
+            cnt = group_sum(cnt, lpb);
+            if (act && l == 0 && cnt > J.max_pl) err = SOPB_STATUS_CAPACITY;
+        } else {
+            const int gbase = (tid & 31) & ~(lpb - 1);
+            const unsigned gm = group_mask(lpb);
+            const int npp = act ? J.pp_cnt[i] : 0;
+            const int32_t* prow = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
+            int32_t* row = J.pl_j + (size_t)(act ? i : 0) * J.cap_pl;
+            const int kmax = __reduce_max_sync(0xffffffffu, npp);
+            for (int kb = 0; kb < kmax; kb += lpb) {
+                const int k = kb + l;
+                int q = 0;
+                bool ok = k < npp;
+                if (ok) {
+                    q = prow[k];
+                    ok = within_cutoff(xi, xs[q], J.pl_cut);
+                }
+                const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
+                if (ok) {
+                    const int pos = cnt + __popc(m & ((1u << l) - 1u));
+                    if (pos < J.cap_pl) row[pos] = q;
+                    else err = SOPB_STATUS_CAPACITY;
+                }
+                cnt += __popc(m);
             }
-            cnt += __popc(m);
+            if (act && l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
         }
-        if (act && l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
     }
 }
 
@@ -172,7 +230,7 @@ __device__ float3 block_sum3(float3 v, float (*red)[4]) {
 // the continuous surface, run by thread 0 after the CTA summed the tip force.
 // Host-side arithmetic of the reference is IEEE without contraction, hence
 // the explicit _rn intrinsics.
-__device__ void tip_update(const JobDev& J, StepScalars& sc, float3 fsum, int64_t step) {
+__device__ __noinline__ void tip_update(const JobDev& J, StepScalars& sc, float3 fsum, int64_t step) {
     const float inv = (float)J.nav;
     float f[3] = {__fdiv_rn(fsum.x, inv), __fdiv_rn(fsum.y, inv), __fdiv_rn(fsum.z, inv)};
     sc.dx = __fmul_rn((float)(step / J.nav), sc.V);
@@ -199,9 +257,9 @@ __device__ void tip_update(const JobDev& J, StepScalars& sc, float3 fsum, int64_
 
 // The updaters of one `stride` boundary in the reference order
 // (creation order in src/gsop.cu:80-101; loop in src/gsop.cu:129-133).
-template <int BLOCK>
-__device__ void run_updaters(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, float* Ts, float (*red)[4],
-                             int64_t step, int& err) {
+template <int BLOCK, bool MASK>
+__device__ __noinline__ void run_updaters(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, float* Ts, uint32_t* vm,
+                             float (*red)[4], int64_t step, int& err) {
     const int tid = threadIdx.x, n = J.n;
     if (J.indent) {
         if (tid == 0 && step == J.retraction_step) sc.V = -sc.V;
@@ -225,12 +283,12 @@ __device__ void run_updaters(const JobDev& J, StepScalars& sc, const float4* __r
         for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
     }
     const bool pp = step % J.pp_freq == 0;
-    if (pp) build_possible<BLOCK>(J, xs, err);
+    if (pp) build_possible<BLOCK, MASK>(J, xs, err);
     if (step % J.nav == 0)
         for (int i = tid; i < n; i += BLOCK) Ts[i] = 0.0f;   // output_manager.cu:125-127
     if (step % J.pairs_freq == 0) {
         if (pp) __syncthreads();
-        build_verlet<BLOCK>(J, xs, err);
+        build_verlet<BLOCK, MASK>(J, xs, vm, err);
     }
     if (J.heating && tid == 0 && step % J.temp_freq == 0) {
         // TemperatureUpdater (src/Integrators/langevin.cu:129-135, 44-48)
@@ -240,7 +298,12 @@ __device__ void run_updaters(const JobDev& J, StepScalars& sc, const float4* __r
     __syncthreads();
 }
 
-template <int BLOCK>
+// Shared-memory bytes of a job's resident launch.
+__host__ __device__ inline size_t resident_smem_bytes(int n, int W, bool mask) {
+    return (size_t)n * kResidentSmemPerBead + (mask ? (size_t)n * W * 4 : 0);
+}
+
+template <int BLOCK, bool MASK>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int64_t nsteps) {
     JobDev* Jp = &jobs[ids[blockIdx.x]];
@@ -257,11 +320,14 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     float4* xb = xa + n;
     uint4* sd = reinterpret_cast<uint4*>(xb + n);
     float* Ts = reinterpret_cast<float*>(sd + n);
+    uint32_t* vm = reinterpret_cast<uint32_t*>(Ts + n);   // MASK mode Verlet masks
     for (int i = tid; i < n; i += BLOCK) {
         xa[i] = J.x[i];
         sd[i] = J.seeds[i];
         Ts[i] = J.T[i];
     }
+    if (MASK)
+        for (int w = tid; w < n * J.W; w += BLOCK) vm[w] = J.pl_mask[w];
     if (tid == 0) {
         sc.var = J.var;
         for (int c = 0; c < 3; ++c) {
@@ -283,16 +349,22 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     const int lpb = J.lpb, g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
     int err = 0;
     int64_t step = J.step;
+    int phase = (int)(step % J.stride);       // steps since the last updater pass
     float4* xc = xa;
     float4* xn = xb;
     for (int64_t s = 0; s < nsteps; ++s, ++step) {
-        if (step % J.stride == 0) run_updaters<BLOCK>(J, sc, xc, Ts, red, step, err);
+        if (phase == 0) run_updaters<BLOCK, MASK>(J, sc, xc, Ts, vm, red, step, err);
+        if (++phase == J.stride) phase = 0;
         const float var = sc.var;
         for (int base = 0; base < n; base += ng) {
             const int i = base + g;
             const bool act = i < n;
             const float4 xi = xc[act ? i : 0];
-            float3 f = act ? bead_force_partial(J, xc, i, xi, l, lpb) : make_float3(0.f, 0.f, 0.f);
+            float3 f = make_float3(0.f, 0.f, 0.f);
+            if (act) {
+                bonded_partial(J, xc, i, xi, l, lpb, f);
+                pairs_partial<MASK>(J, xc, vm, i, xi, l, lpb, f);
+            }
             f = group_reduce(f, lpb);
             if (act && l == 0) {
                 if (J.indent) {
@@ -326,11 +398,13 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     }
     for (int i = tid; i < n; i += BLOCK) {
         const float4 v = xc[i];
-        if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) err = 3;
+        if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) err = SOPB_STATUS_NONFINITE;
         J.x[i] = v;
         J.seeds[i] = sd[i];
         J.T[i] = Ts[i];
     }
+    if (MASK)
+        for (int w = tid; w < n * J.W; w += BLOCK) J.pl_mask[w] = vm[w];
     if (err) atomicMax(&sc.err, err);
     __syncthreads();
     if (tid == 0) {
@@ -351,9 +425,9 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
 }
 
 // Potential forces only (SOPPotential::compute of every potential, no
-// integrator) at the job's current coordinates; for parity checks and
-// energy-free observables.  Does not touch the tip-force accumulator.
-template <int BLOCK>
+// integrator) at the job's current coordinates, reading the Verlet list the
+// last launch left in global memory; does not touch the tip accumulator.
+template <int BLOCK, bool MASK>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, float4* __restrict__ out) {
     __shared__ JobDev Js;
@@ -368,7 +442,11 @@ k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, 
         const int i = base + g;
         const bool act = i < n;
         const float4 xi = J.x[act ? i : 0];
-        float3 f = act ? bead_force_partial(J, J.x, i, xi, l, lpb) : make_float3(0.f, 0.f, 0.f);
+        float3 f = make_float3(0.f, 0.f, 0.f);
+        if (act) {
+            bonded_partial(J, J.x, i, xi, l, lpb, f);
+            pairs_partial<MASK>(J, J.x, J.pl_mask, i, xi, l, lpb, f);
+        }
         f = group_reduce(f, lpb);
         if (act && l == 0) {
             if (J.indent) {
@@ -381,7 +459,7 @@ k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, 
 }
 
 // Rebuilds the possible-pairs and/or Verlet lists now, without the step gate.
-template <int BLOCK>
+template <int BLOCK, bool MASK>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int possible, int verlet) {
     JobDev* Jp = &jobs[ids[blockIdx.x]];
@@ -392,9 +470,9 @@ k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int 
     if (threadIdx.x == 0) errs = 0;
     __syncthreads();
     int err = 0;
-    if (possible) build_possible<BLOCK>(J, J.x, err);
+    if (possible) build_possible<BLOCK, MASK>(J, J.x, err);
     __syncthreads();
-    if (verlet) build_verlet<BLOCK>(J, J.x, err);
+    if (verlet) build_verlet<BLOCK, MASK>(J, J.x, J.pl_mask, err);
     if (err) atomicMax(&errs, err);
     __syncthreads();
     if (threadIdx.x == 0 && errs) Jp->status = errs;

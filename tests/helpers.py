@@ -6,8 +6,9 @@ import numpy as np
 import sopb
 import sopb_synth as S
 
-# Force parity bound: |F_gpu - F_ref| <= FORCE_RTOL * sum_k |term_k| per
-# component (the scale of the FP32 summation), i.e. 1e-5 relative.
+# Force parity bound, per component: |F_gpu - F_fp64| <= FORCE_RTOL * S where
+# S is the FP32 rounding scale of the sum (for every term the magnitudes of
+# the quantities it subtracts; oracle orc_job_forces), i.e. 1e-5 relative.
 FORCE_RTOL = 1e-5
 
 
@@ -52,6 +53,6 @@ def spec(n: int, seed: int, mode: str = "ramp", rng_seed: int = 1119727, **kw) -
 
 
 def force_error(f, f64, abs64) -> float:
-    """max over components of |f - f64| / (sum |terms| + tiny)."""
+    """max over components of |f - f64| / (rounding scale + tiny)."""
     f = np.asarray(f, np.float64)[:, :3]
     return float(np.max(np.abs(f - f64[:, :3]) / (abs64[:, :3] + 1e-30)))

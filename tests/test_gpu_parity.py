@@ -29,7 +29,7 @@ def test_hybrid_taus_states_bit_exact(gpu_ctx, n, steps):
     g.destroy()
 
 
-@pytest.mark.parametrize("n,seed", [(60, 1), (200, 11), (451, 5), (1100, 9)])
+@pytest.mark.parametrize("n,seed", [(60, 1), (200, 11), (451, 5), (1100, 9), (1500, 4)])
 def test_lists_bit_exact_on_identical_coordinates(gpu_ctx, n, seed):
     sp = spec(n, seed, "free", pairs_threshold=25.0)
     g, o = pair(gpu_ctx, sp)
@@ -89,6 +89,30 @@ def test_one_step_matches_oracle(gpu_ctx, mode):
     xg, xo = g.read(sopb.COORDS), o.read(sopb.COORDS)
     assert np.max(np.abs(xg - xo)) < 1e-5
     assert np.array_equal(g.read(sopb.SEEDS), o.read(sopb.SEEDS))
+    g.destroy()
+
+
+def test_list_representation_by_size(gpu_ctx):
+    # bitmask lists while they fit in shared memory, index rows above
+    for n, want_mask in ((600, True), (1500, False)):
+        j = gpu_ctx.job(spec(n, 1, "free"))
+        lpb, block = j.shape()
+        assert block in (128, 256, 512, 1024) and lpb in (1, 2, 4, 8, 16, 32)
+        j.destroy()
+
+
+@pytest.mark.parametrize("n", [300, 1500])
+def test_forces_match_oracle_both_list_modes(gpu_ctx, n):
+    sp = spec(n, 21, "free")
+    g, o = pair(gpu_ctx, sp)
+    g.rebuild(True, True)
+    o.rebuild(True, True)
+    f32, f64, a64 = o.forces()
+    assert force_error(g.read(sopb.FORCES), f64, a64) <= FORCE_RTOL
+    gpu_ctx.run([g], 30)
+    o.advance(30)
+    assert np.array_equal(g.read(sopb.SEEDS), o.read(sopb.SEEDS))
+    assert np.max(np.abs(g.read(sopb.COORDS) - o.read(sopb.COORDS))) < 1e-3
     g.destroy()
 
 

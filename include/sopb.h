@@ -127,7 +127,9 @@ typedef struct sopb_params {
     int32_t hi_b_mode;         /* SOPB_HI_B_*; default SOPB_HI_B_CHOLESKY      */
     int32_t hi_refresh;        /* refactor D every k steps (reference: 1)      */
     int32_t lanes_per_bead;    /* 0 = autotuned                                */
-    int32_t reserved[7];
+    int32_t cell_list;         /* possible pairs by cell list: 0 auto, 1 on, 2 off */
+    int32_t grid_path;         /* 0 auto (resident kernel when it fits), 1 grid */
+    int32_t reserved[5];
 } sopb_params;
 
 /*

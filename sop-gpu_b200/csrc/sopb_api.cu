@@ -14,6 +14,7 @@
 #include "../../include/sopb.h"
 #include "sopb_device.cuh"
 #include "sopb_resident.cuh"
+#include "sopb_grid.cuh"
 
 using namespace sopb;
 
@@ -95,6 +96,12 @@ struct sopb_job {
     JobDev h{};
     void* dmem = nullptr;
     size_t dbytes = 0;
+    // grid path
+    GridAux aux{};
+    void* amem = nullptr;
+    int64_t host_step = 0;             // the device step counter, tracked on the host
+    cudaGraphExec_t chunk = nullptr;   // one stride chunk: updaters + stride steps
+    int bead_blocks = 1;               // CTAs of the per-bead grid kernels
 };
 
 #define CUDA_TRY(call)                                                                         \
@@ -331,7 +338,6 @@ int validate_desc(const sopb_job_desc* d) {
         if (f3norm(p.indentationDirection) == 0.0f || f3norm(p.indentationSurfaceN) == 0.0f) return SOPB_ERR_INVALID;
     }
     if (p.hi_on) return SOPB_ERR_UNSUPPORTED;  // HI jobs use the HI path (not in this entry point yet)
-    if (n > kMaxResidentBeads) return SOPB_ERR_UNSUPPORTED;
     return SOPB_OK;
 }
 
@@ -364,6 +370,134 @@ void build_maps(const sopb_job_desc* d, HostMaps& m) {
         m.nat_j[fill[a]] = b; m.nat_par[fill[a]++] = par;
         m.nat_j[fill[b]] = a; m.nat_par[fill[b]++] = par;
     }
+}
+
+}  // namespace
+
+namespace {
+
+// Buffers of the grid path: force buffer (the context's second coordinate
+// pool), reduction partials and, for large jobs, the cell list.
+int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
+    GridAux& a = j->aux;
+    j->bead_blocks = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)c->sm_count * 8);
+    a.npart = j->bead_blocks;
+    a.use_cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
+    size_t off = 0;
+    const size_t o_part = off; off += align256(2 * (size_t)a.npart * sizeof(float4));
+    const size_t o_geo = off; off += align256(8 * sizeof(float));
+    size_t o_cc = 0, o_cs = 0, o_cb = 0, o_bc = 0;
+    if (a.use_cells) {
+        o_cc = off; off += align256(((size_t)kCellMax + 1) * 4);
+        o_cs = off; off += align256(((size_t)kCellMax + 1) * 4);
+        o_cb = off; off += align256((size_t)n * 4);
+        o_bc = off; off += align256((size_t)n * 4);
+    }
+    if (cudaMalloc(&j->amem, off) != cudaSuccess) {
+        cudaGetLastError();
+        return SOPB_ERR_NOMEM;
+    }
+    char* b = (char*)j->amem;
+    a.F = c->xalt + j->b0;
+    a.part = (float4*)(b + o_part);
+    a.cell_geo = (float*)(b + o_geo);
+    if (a.use_cells) {
+        a.cell_count = (int32_t*)(b + o_cc);
+        a.cell_start = (int32_t*)(b + o_cs);
+        a.cell_beads = (int32_t*)(b + o_cb);
+        a.bead_cell = (int32_t*)(b + o_bc);
+    }
+    CUDA_TRY(cudaMemsetAsync(j->amem, 0, off, c->stream));
+    return SOPB_OK;
+}
+
+// Possible pairs of a grid job: brute force, or cell list + row sort.
+int grid_possible(sopb_job* j, JobDev* Jp, cudaStream_t st, int force) {
+    GridAux& a = j->aux;
+    const int nb = j->bead_blocks;
+    const int warps_blocks = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)j->ctx->sm_count * 16);
+    if (!a.use_cells) {
+        k_g_possible_brute<<<warps_blocks, kGridBlock, 0, st>>>(Jp, force);
+        CUDA_TRY(cudaGetLastError());
+        return SOPB_OK;
+    }
+    // cell_count is zeroed by the scan's consumer (k_cl_fill turns counts
+    // into cursors); clear it for this rebuild first
+    k_cl_bounds<<<nb, kGridBlock, 0, st>>>(Jp, a, force);
+    k_cl_geometry<<<1, 32, 0, st>>>(Jp, a, nb, force);
+    CUDA_TRY(cudaMemsetAsync(a.cell_count, 0, ((size_t)kCellMax + 1) * 4, st));
+    k_cl_count<<<nb, kGridBlock, 0, st>>>(Jp, a, force);
+    k_cl_scan<<<1, 1024, 0, st>>>(Jp, a, force);
+    k_cl_fill<<<nb, kGridBlock, 0, st>>>(Jp, a, force);
+    k_cl_possible<<<warps_blocks, kGridBlock, 0, st>>>(Jp, a, force);
+    const int sort_blocks = (int)std::min<int64_t>((j->n + 3) / 4, (int64_t)j->ctx->sm_count * 16);
+    k_cl_sort_rows<<<sort_blocks, 128, 4 * kSortCap * sizeof(int32_t), st>>>(Jp, force);
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
+}
+
+// Updaters of a stride boundary (each gated on the device step), then
+// `steps` Langevin steps, then the step counter moves by `steps`.
+int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps) {
+    sopb_context* c = j->ctx;
+    JobDev* Jp = &c->d_jobs[j->slot];
+    GridAux& a = j->aux;
+    const int nb = j->bead_blocks;
+    if (updaters) {
+        k_g_tip_partial<<<nb, kGridBlock, 0, st>>>(Jp, a);
+        k_g_scalar_updaters<<<1, 32, 0, st>>>(Jp, a);
+        k_g_treset<<<nb, kGridBlock, 0, st>>>(Jp);
+        int rc = grid_possible(j, Jp, st, 0);
+        if (rc) return rc;
+        const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
+        k_g_verlet<<<wb, kGridBlock, 0, st>>>(Jp, 0);
+    }
+    const int fb = (int)std::min<int64_t>((j->n + (kGridBlock / kGridLpb) - 1) / (kGridBlock / kGridLpb), (int64_t)c->sm_count * 8);
+    for (int s = 0; s < steps; ++s) {
+        k_g_forces<<<fb, kGridBlock, 0, st>>>(Jp, a);
+        k_g_langevin<<<nb, kGridBlock, 0, st>>>(Jp, a);
+    }
+    k_g_advance<<<1, 32, 0, st>>>(Jp, steps);
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
+}
+
+// Advances a grid job: whole stride chunks by graph replay, the rest by
+// direct launches.
+int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
+    const int32_t stride = j->h.stride;
+    int64_t left = nsteps;
+    int rc;
+    while (left > 0 && (j->host_step % stride) != 0) {   // finish a partial chunk
+        if ((rc = grid_launch(j, st, false, 1))) return rc;
+        j->host_step++;
+        left--;
+    }
+    const int64_t chunks = left / stride;
+    if (chunks > 0) {
+        if (!j->chunk) {
+            cudaGraph_t g;
+            cudaStream_t cap = j->ctx->side[kSideStreams - 1];
+            CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+            rc = grid_launch(j, cap, true, stride);
+            cudaError_t e = cudaStreamEndCapture(cap, &g);
+            if (rc) return rc;
+            CUDA_TRY(e);
+            CUDA_TRY(cudaGraphInstantiate(&j->chunk, g, 0));
+            cudaGraphDestroy(g);
+        }
+        for (int64_t k = 0; k < chunks; ++k) CUDA_TRY(cudaGraphLaunch(j->chunk, st));
+        j->host_step += chunks * stride;
+        left -= chunks * stride;
+    }
+    while (left > 0) {
+        if ((rc = grid_launch(j, st, j->host_step % stride == 0, 1))) return rc;
+        j->host_step++;
+        left--;
+    }
+    k_g_check_finite<<<j->bead_blocks, kGridBlock, 0, st>>>(&j->ctx->d_jobs[j->slot]);
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
 }
 
 }  // namespace
@@ -491,23 +625,33 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     if (d->seeds) std::memcpy(seeds.data(), d->seeds, seeds.size() * 4);
     else sopb_generate_seeds(d->seed, n, seeds.data());
 
-    // list representation: bitmasks when the Verlet masks fit in shared memory
+    // path: the resident kernel while a job fits one CTA, else per-step
+    // grid kernels; list representation: bitmasks when the Verlet masks fit
+    // in shared memory
+    h.grid = (p.grid_path == 1 || n > kMaxResidentBeads) ? 1 : 0;
     h.W = (n + 31) / 32;
-    h.mask = resident_smem_bytes(n, h.W, true) <= (size_t)c->smem_dyn_max ? 1 : 0;
+    h.mask = (!h.grid && resident_smem_bytes(n, h.W, true) <= (size_t)c->smem_dyn_max) ? 1 : 0;
+    if (h.grid) {
+        h.lpb = kGridLpb;
+        h.block = 1024;
+    }
     h.max_pp = p.max_possiblePairs > 0 ? p.max_possiblePairs : 4096;
     h.max_pl = p.max_pairs > 0 ? p.max_pairs : 512;
     // exclusion mask: self, covalent and native partners (the linear scans of
     // possiblepairlist_kernel.cu:47-59, precomputed)
-    std::vector<uint32_t> ex((size_t)n * h.W, 0u);
+    // (grid jobs scan their partners' rows instead: n^2 bits would not fit)
+    std::vector<uint32_t> ex(h.grid ? 0 : (size_t)n * h.W, 0u);
     auto excl = [&](int32_t i, int32_t q) { ex[(size_t)i * h.W + (q >> 5)] |= 1u << (q & 31); };
-    for (int32_t i = 0; i < n; ++i) excl(i, i);
-    for (int32_t i = 0; i < n; ++i) {
-        for (int32_t k = m.cov_off[i]; k < m.cov_off[i + 1]; ++k) excl(i, m.cov_j[k]);
-        for (int32_t k = m.nat_off[i]; k < m.nat_off[i + 1]; ++k) excl(i, m.nat_j[k]);
+    if (!h.grid) {
+        for (int32_t i = 0; i < n; ++i) excl(i, i);
+        for (int32_t i = 0; i < n; ++i) {
+            for (int32_t k = m.cov_off[i]; k < m.cov_off[i + 1]; ++k) excl(i, m.cov_j[k]);
+            for (int32_t k = m.nat_off[i]; k < m.nat_off[i + 1]; ++k) excl(i, m.nat_j[k]);
+        }
     }
 
     // device block for the maps and lists
-    const size_t mask_bytes = (size_t)n * h.W * 4;
+    const size_t mask_bytes = h.grid ? 0 : (size_t)n * h.W * 4;
     const size_t o_covoff = 0;
     const size_t o_covj = o_covoff + align256((n + 1) * 4);
     const size_t o_covr0 = o_covj + align256(m.cov_j.size() * 4 + 4);
@@ -538,7 +682,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.nat_off = (int32_t*)(base + o_natoff);
     h.nat_j = (int32_t*)(base + o_natj);
     h.nat_par = (float2*)(base + o_natpar);
-    h.ex_mask = (uint32_t*)(base + o_ex);
+    h.ex_mask = h.grid ? nullptr : (uint32_t*)(base + o_ex);
     h.pp_mask = h.mask ? (uint32_t*)(base + o_ppm) : nullptr;
     h.pl_mask = h.mask ? (uint32_t*)(base + o_plm) : nullptr;
     h.pp_cnt = (int32_t*)(base + o_ppcnt);
@@ -553,7 +697,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.flags = c->flags + b0;
     cudaStream_t st = c->stream;
     CUDA_TRY(cudaMemsetAsync(base + o_ppm, 0, o_ppj - o_ppm, st));   // masks and counts
-    CUDA_TRY(cudaMemcpyAsync(h.ex_mask, ex.data(), mask_bytes, cudaMemcpyHostToDevice, st));
+    if (!h.grid) CUDA_TRY(cudaMemcpyAsync(h.ex_mask, ex.data(), mask_bytes, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(h.cov_off, m.cov_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
     if (!m.cov_j.empty()) {
         CUDA_TRY(cudaMemcpyAsync(h.cov_j, m.cov_j.data(), m.cov_j.size() * 4, cudaMemcpyHostToDevice, st));
@@ -569,6 +713,15 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     CUDA_TRY(cudaMemcpyAsync(h.flags, flags.data(), (size_t)n, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemsetAsync(h.T, 0, (size_t)n * 4, st));
     CUDA_TRY(cudaMemsetAsync(h.tipF, 0, (size_t)n * 16, st));
+    if (h.grid) {
+        int rc2 = grid_alloc(c, j, p, n);
+        if (rc2) {
+            cudaFree(j->dmem);
+            c->beads.release(b0, n);
+            delete j;
+            return rc2;
+        }
+    }
     const int slot = c->free_slots.back();
     c->free_slots.pop_back();
     CUDA_TRY(cudaMemcpyAsync(&c->d_jobs[slot], &h, sizeof(JobDev), cudaMemcpyHostToDevice, st));
@@ -589,6 +742,8 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     sopb_context* c = j->ctx;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    if (j->chunk) cudaGraphExecDestroy(j->chunk);
+    if (j->amem) cudaFree(j->amem);
     cudaFree(j->dmem);
     c->beads.release(j->b0, j->n);
     c->slots[j->slot] = nullptr;
@@ -633,6 +788,25 @@ extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, i
     for (int32_t k = 0; k < njobs; ++k)
         if (!jobs[k] || jobs[k]->ctx != c) return SOPB_ERR_INVALID;
     CUDA_TRY(cudaSetDevice(c->device));
+    std::vector<sopb_job*> resident, grid;
+    for (int32_t k = 0; k < njobs; ++k) (jobs[k]->h.grid ? grid : resident).push_back(jobs[k]);
+    if (resident.empty()) {
+        for (sopb_job* j : grid) {
+            int rc = grid_run(j, c->stream, nsteps);
+            if (rc) return rc;
+        }
+        return SOPB_OK;
+    }
+    if (!grid.empty()) {
+        // grid jobs on the context stream, resident classes beside them
+        int rc = sopb_run(c, resident.data(), (int32_t)resident.size(), nsteps);
+        if (rc) return rc;
+        for (sopb_job* j : grid) {
+            rc = grid_run(j, c->stream, nsteps);
+            if (rc) return rc;
+        }
+        return SOPB_OK;
+    }
     std::vector<LaunchClass> cls;
     group_jobs(jobs, njobs, cls);
     std::vector<int32_t> ids;
@@ -808,6 +982,19 @@ extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t ver
     if (!j) return SOPB_ERR_INVALID;
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
+    if (j->h.grid) {
+        JobDev* Jp = &c->d_jobs[j->slot];
+        int rc = SOPB_OK;
+        if (possible) rc = grid_possible(j, Jp, c->stream, 1);
+        if (rc) return rc;
+        if (verlet) {
+            const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
+            k_g_verlet<<<wb, kGridBlock, 0, c->stream>>>(Jp, 1);
+            CUDA_TRY(cudaGetLastError());
+        }
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return SOPB_OK;
+    }
     int rc = ensure_ids(c, 1);
     if (rc) return rc;
     const int32_t id = j->slot;

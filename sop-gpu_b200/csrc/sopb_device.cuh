@@ -31,6 +31,7 @@ struct JobDev {
     int32_t W;            // words per bitmask row, ceil(n/32)
     int32_t max_pp;       // configured max_possiblePairs (overflow -> error)
     int32_t max_pl;       // configured max_pairs
+    int32_t grid;         // 1: grid path (per-step kernels, CUDA graphs)
     int32_t stride;       // updater period (gsop.cu:117-122)
     int32_t nav;
     int32_t pairs_freq;

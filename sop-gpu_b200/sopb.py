@@ -51,7 +51,8 @@ class Params(C.Structure):
         ("hi_on", C.c_int32), ("hi_exact", C.c_int32), ("hi_a", C.c_float), ("hi_epsilon_freq", C.c_int32),
         ("hi_capricious", C.c_int32), ("hi_unlisted", C.c_int32), ("hi_epsmax", C.c_float),
         ("hi_b_mode", C.c_int32), ("hi_refresh", C.c_int32), ("lanes_per_bead", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("cell_list", C.c_int32), ("grid_path", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

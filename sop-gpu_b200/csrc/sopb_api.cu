@@ -133,22 +133,28 @@ int set_smem_attr(int device, int* dyn_out) {
 
 // Lanes per bead and CTA size for a job of n beads.  Depends only on the job
 // (never on the batch it runs in), so a job's arithmetic is identical alone
-// and in any mix.
+// and in any mix.  Threads are given in proportion to the expected work of a
+// step, n x (Verlet partners per bead, ~20 n^0.28 for a compact globule at a
+// 20 A cutoff), so the CTAs of a ragged batch finish their steps together.
+constexpr float kWorkPerThread = 80.0f;
 void launch_shape(int32_t n, int32_t lpb_req, int32_t* lpb, int32_t* block) {
     int32_t l = lpb_req;
     if (l <= 0) l = 4;
     int32_t p2 = 1;
     while (p2 < l && p2 < 32) p2 <<= 1;
     l = p2;
-    int32_t want = n * l;
-    int32_t b = 128;
-    while (b < want && b < 1024) b <<= 1;
+    const float work = (float)n * 20.0f * powf((float)n, 0.28f);
+    const float want = work / kWorkPerThread;
+    int32_t b = 64;
+    while (b < 1024 && (float)b * 1.41421356f < want) b <<= 1;   // nearest power of two
+    while (b < 1024 && b < l) b <<= 1;
     *lpb = l;
     *block = b;
 }
 
 #define SOPB_BLOCK_SWITCH(block, MASK, LAUNCH)             \
     switch (block) {                                     \
+    case 64: LAUNCH(64, MASK); break;                    \
     case 128: LAUNCH(128, MASK); break;                  \
     case 256: LAUNCH(256, MASK); break;                  \
     case 512: LAUNCH(512, MASK); break;                  \
@@ -259,7 +265,8 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
     CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     int rc;
     int* dm = &c->smem_dyn_max;
-    if ((rc = set_smem_attr<128, false>(device, dm)) || (rc = set_smem_attr<256, false>(device, dm)) ||
+    if ((rc = set_smem_attr<64, false>(device, dm)) || (rc = set_smem_attr<64, true>(device, dm)) ||
+        (rc = set_smem_attr<128, false>(device, dm)) || (rc = set_smem_attr<256, false>(device, dm)) ||
         (rc = set_smem_attr<512, false>(device, dm)) || (rc = set_smem_attr<1024, false>(device, dm)) ||
         (rc = set_smem_attr<128, true>(device, dm)) || (rc = set_smem_attr<256, true>(device, dm)) ||
         (rc = set_smem_attr<512, true>(device, dm)) || (rc = set_smem_attr<1024, true>(device, dm)))

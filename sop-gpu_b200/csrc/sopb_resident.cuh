@@ -303,8 +303,9 @@ __host__ __device__ inline size_t resident_smem_bytes(int n, int W, bool mask) {
     return (size_t)n * kResidentSmemPerBead + (mask ? (size_t)n * W * 4 : 0);
 }
 
+// Register cap of 64 per thread: 1024 threads of resident CTAs per SM.
 template <int BLOCK, bool MASK>
-__global__ void __launch_bounds__(BLOCK, 1)
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
 k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int64_t nsteps) {
     JobDev* Jp = &jobs[ids[blockIdx.x]];
     __shared__ JobDev Js;

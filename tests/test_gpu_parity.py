@@ -97,7 +97,7 @@ def test_list_representation_by_size(gpu_ctx):
     for n, want_mask in ((600, True), (1500, False)):
         j = gpu_ctx.job(spec(n, 1, "free"))
         lpb, block = j.shape()
-        assert block in (128, 256, 512, 1024) and lpb in (1, 2, 4, 8, 16, 32)
+        assert block in (64, 128, 256, 512, 1024) and lpb in (1, 2, 4, 8, 16, 32)
         j.destroy()
 
 

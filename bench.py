@@ -238,6 +238,12 @@ def run_gpu(args):
     t0 = time.perf_counter()
     specs = batch_specs(rank=rank)
     log("rank %d: generated %d systems in %.1fs" % (rank, len(specs), time.perf_counter() - t0))
+    tuned = None
+    if not args.no_autotune:
+        import sopb_autotune
+        t0 = time.perf_counter()
+        tuned = sopb_autotune.autotune(ctx, specs, steps=100, log=log if rank == 0 else None)
+        log("rank %d: autotuned shape policy %s in %.1fs" % (rank, tuned["policy"], time.perf_counter() - t0))
     jobs = [ctx.job(sp) for sp in specs]
     beads = sum(sp.n for sp in specs)
     chunk = args.chunk
@@ -348,6 +354,9 @@ def run_gpu(args):
                        "dt_tauH": 0.08, "parallelism": "replicas-dp%d" % world, "l2": "flushed between timed steps"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": beads * 16, "d2h_bytes_per_step": beads * 16},
             "gpu_launches": launches,
+            "shape_policy": None if tuned is None else {"lanes_per_bead": tuned["policy"][0],
+                                                        "work_per_thread": tuned["policy"][1],
+                                                        "max_block": tuned["policy"][2]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                          "alg_bytes_per_bead_step": bps, "lists": stats},
@@ -373,6 +382,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -15,6 +15,7 @@
 #include "sopb_device.cuh"
 #include "sopb_resident.cuh"
 #include "sopb_grid.cuh"
+#include "sopb_hi.cuh"
 
 using namespace sopb;
 
@@ -59,6 +60,13 @@ struct RangeAlloc {
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Shape policy of the resident kernel (see launch_shape).
+struct ShapePolicy {
+    int32_t lpb = 4;
+    float work_per_thread = 0.0f;
+    int32_t max_block = 1024;
+};
+
 }  // namespace
 
 struct sopb_context {
@@ -86,6 +94,7 @@ struct sopb_context {
     cudaEvent_t ev_join[kSideStreams] = {};
     int32_t last_error = SOPB_OK;
     int smem_dyn_max = 1 << 30;   // dynamic shared memory available to the resident kernel
+    ShapePolicy policy;
 };
 
 struct sopb_job {
@@ -102,6 +111,7 @@ struct sopb_job {
     int64_t host_step = 0;             // the device step counter, tracked on the host
     cudaGraphExec_t chunk = nullptr;   // one stride chunk: updaters + stride steps
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
+    int jsplit = 1;                    // j slices of the O(N^2) HI sums
 };
 
 #define CUDA_TRY(call)                                                                         \
@@ -131,22 +141,29 @@ int set_smem_attr(int device, int* dyn_out) {
     return SOPB_OK;
 }
 
-// Lanes per bead and CTA size for a job of n beads.  Depends only on the job
-// (never on the batch it runs in), so a job's arithmetic is identical alone
-// and in any mix.  Threads are given in proportion to the expected work of a
-// step, n x (Verlet partners per bead, ~20 n^0.28 for a compact globule at a
-// 20 A cutoff), so the CTAs of a ragged batch finish their steps together.
-constexpr float kWorkPerThread = 80.0f;
-void launch_shape(int32_t n, int32_t lpb_req, int32_t* lpb, int32_t* block) {
-    int32_t l = lpb_req;
-    if (l <= 0) l = 4;
+// Lanes per bead and CTA size of a job.  A function of the job and of the
+// context's shape policy only (never of the batch it runs in), so a job's
+// arithmetic is identical alone and in any mix.  Policy:
+//   work_per_thread <= 0: one bead per lane group (CTA = n * lanes, rounded up
+//                         to a power of two, at most max_block);
+//   work_per_thread  > 0: threads in proportion to the expected work of a
+//                         step, n x (Verlet partners per bead, ~20 n^0.28 for a
+//                         compact globule at a 20 A cutoff) / work_per_thread.
+// sopb_context_set_shape_policy sets it (the autotuner's knob).
+void launch_shape(const ShapePolicy& pol, int32_t n, int32_t lpb_req, int32_t* lpb, int32_t* block) {
+    int32_t l = lpb_req > 0 ? lpb_req : pol.lpb;
     int32_t p2 = 1;
     while (p2 < l && p2 < 32) p2 <<= 1;
     l = p2;
-    const float work = (float)n * 20.0f * powf((float)n, 0.28f);
-    const float want = work / kWorkPerThread;
+    const int32_t maxb = pol.max_block >= 64 && pol.max_block <= 1024 ? pol.max_block : 1024;
     int32_t b = 64;
-    while (b < 1024 && (float)b * 1.41421356f < want) b <<= 1;   // nearest power of two
+    if (pol.work_per_thread <= 0.0f) {
+        const int64_t want = (int64_t)n * l;
+        while (b < maxb && b < want) b <<= 1;
+    } else {
+        const float want = (float)n * 20.0f * powf((float)n, 0.28f) / pol.work_per_thread;
+        while (b < maxb && (float)b * 1.41421356f < want) b <<= 1;
+    }
     while (b < 1024 && b < l) b <<= 1;
     *lpb = l;
     *block = b;
@@ -303,6 +320,15 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     return SOPB_OK;
 }
 
+extern "C" int sopb_context_set_shape_policy(sopb_context* c, int32_t lanes_per_bead, float work_per_thread,
+                                             int32_t max_block) {
+    if (!c || lanes_per_bead < 1 || lanes_per_bead > 32 || max_block < 64 || max_block > 1024) return SOPB_ERR_INVALID;
+    c->policy.lpb = lanes_per_bead;
+    c->policy.work_per_thread = work_per_thread;
+    c->policy.max_block = max_block;
+    return SOPB_OK;
+}
+
 extern "C" int sopb_context_sync(sopb_context* c) {
     if (!c) return SOPB_ERR_INVALID;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -344,7 +370,13 @@ int validate_desc(const sopb_job_desc* d) {
         if (p.indentationTipZeta == 0.0f) return SOPB_ERR_INVALID;
         if (f3norm(p.indentationDirection) == 0.0f || f3norm(p.indentationSurfaceN) == 0.0f) return SOPB_ERR_INVALID;
     }
-    if (p.hi_on) return SOPB_ERR_UNSUPPORTED;  // HI jobs use the HI path (not in this entry point yet)
+    if (p.hi_on) {
+        // TeaIntegrator ctor (src/Integrators/bdhitea.cu:30-74)
+        if (p.minimization) return SOPB_ERR_INVALID;
+        if (p.hi_a <= 0.0f) return SOPB_ERR_INVALID;
+        if (!p.hi_exact && p.hi_epsilon_freq <= 0) return SOPB_ERR_INVALID;
+        if (p.hi_exact && n > 128) return SOPB_ERR_UNSUPPORTED;   // blocked factorisation: not in this build
+    }
     return SOPB_OK;
 }
 
@@ -390,8 +422,26 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
     j->bead_blocks = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)c->sm_count * 8);
     a.npart = j->bead_blocks;
     a.use_cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
+    const bool hi = p.hi_on != 0;
+    const int itiles = (n + kHiTile - 1) / kHiTile;
+    j->jsplit = 1;
+    if (hi && !p.hi_exact && p.hi_unlisted)
+        j->jsplit = std::max(1, std::min((4 * c->sm_count + itiles - 1) / itiles, itiles));
+    const size_t part_elems = std::max<size_t>(2 * (size_t)a.npart, hi ? (size_t)j->jsplit * n : 0);
     size_t off = 0;
-    const size_t o_part = off; off += align256(2 * (size_t)a.npart * sizeof(float4));
+    const size_t o_part = off; off += align256(part_elems * sizeof(float4));
+    size_t o_rf = 0, o_mf = 0, o_xc = 0, o_ci = 0, o_eps = 0, o_ten = 0;
+    if (hi) {
+        o_rf = off; off += align256((size_t)n * 16);
+        o_mf = off; off += align256((size_t)n * 16);
+        o_xc = off; off += align256((size_t)n * 16);
+        o_ci = off; off += align256((size_t)n * 16);
+        o_eps = off; off += align256((size_t)n * 4);
+        if (p.hi_exact) {
+            a.ld = 3 * n;
+            o_ten = off; off += align256((size_t)a.ld * a.ld * 4);
+        }
+    }
     const size_t o_geo = off; off += align256(8 * sizeof(float));
     size_t o_cc = 0, o_cs = 0, o_cb = 0, o_bc = 0;
     if (a.use_cells) {
@@ -407,6 +457,14 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
     char* b = (char*)j->amem;
     a.F = c->xalt + j->b0;
     a.part = (float4*)(b + o_part);
+    if (hi) {
+        a.rf = (float4*)(b + o_rf);
+        a.mf = (float4*)(b + o_mf);
+        a.xc = (float4*)(b + o_xc);
+        a.ci4 = (float4*)(b + o_ci);
+        a.eps = (float*)(b + o_eps);
+        if (p.hi_exact) a.tensor = (float*)(b + o_ten);
+    }
     a.cell_geo = (float*)(b + o_geo);
     if (a.use_cells) {
         a.cell_count = (int32_t*)(b + o_cc);
@@ -458,11 +516,30 @@ int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps) {
         if (rc) return rc;
         const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
         k_g_verlet<<<wb, kGridBlock, 0, st>>>(Jp, 0);
+        if (j->h.hi && !j->h.hi_exact) {
+            // TeaUpdater (src/Integrators/bdhitea.cu:133-176), last updater
+            const dim3 tg((j->n + kHiTile - 1) / kHiTile, j->jsplit);
+            k_tea_eps_partial<<<tg, kHiTile, 0, st>>>(Jp, a, j->jsplit, 0);
+            k_tea_eps_reduce<<<nb, kGridBlock, 0, st>>>(Jp, a, j->jsplit, 0);
+            k_tea_beta<<<1, 256, 0, st>>>(Jp, a, 0);
+        }
     }
     const int fb = (int)std::min<int64_t>((j->n + (kGridBlock / kGridLpb) - 1) / (kGridBlock / kGridLpb), (int64_t)c->sm_count * 8);
     for (int s = 0; s < steps; ++s) {
         k_g_forces<<<fb, kGridBlock, 0, st>>>(Jp, a);
-        k_g_langevin<<<nb, kGridBlock, 0, st>>>(Jp, a);
+        if (!j->h.hi) {
+            k_g_langevin<<<nb, kGridBlock, 0, st>>>(Jp, a);
+        } else if (!j->h.hi_exact) {
+            k_hi_prepare<<<nb, kGridBlock, 0, st>>>(Jp, a);
+            const dim3 tg((j->n + kHiTile - 1) / kHiTile, j->jsplit);
+            k_tea_force_partial<<<tg, kHiTile, 0, st>>>(Jp, a, j->jsplit);
+            k_tea_integrate<<<nb, kGridBlock, 0, st>>>(Jp, a, j->jsplit);
+        } else {
+            k_hi_prepare<<<nb, kGridBlock, 0, st>>>(Jp, a);
+            k_chol_D<<<nb, kGridBlock, 0, st>>>(Jp, a);
+            k_chol_factor_small<<<1, 384, 0, st>>>(Jp, a);
+            k_chol_apply<<<nb, kGridBlock, 0, st>>>(Jp, a);
+        }
     }
     k_g_advance<<<1, 32, 0, st>>>(Jp, steps);
     CUDA_TRY(cudaGetLastError());
@@ -542,7 +619,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     JobDev h;
     std::memset(&h, 0, sizeof(h));
     h.n = n;
-    launch_shape(n, p.lanes_per_bead, &h.lpb, &h.block);
+    launch_shape(c->policy, n, p.lanes_per_bead, &h.lpb, &h.block);
     h.cap_pp = (int32_t)std::max<int64_t>(1, std::min<int64_t>(p.max_possiblePairs > 0 ? p.max_possiblePairs : 4096, n - 1));
     h.cap_pl = (int32_t)std::max<int64_t>(1, std::min<int64_t>(p.max_pairs > 0 ? p.max_pairs : 512, n - 1));
     h.stride = compute_stride(p);
@@ -635,7 +712,18 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     // path: the resident kernel while a job fits one CTA, else per-step
     // grid kernels; list representation: bitmasks when the Verlet masks fit
     // in shared memory
-    h.grid = (p.grid_path == 1 || n > kMaxResidentBeads) ? 1 : 0;
+    h.grid = (p.grid_path == 1 || p.hi_on || n > kMaxResidentBeads) ? 1 : 0;
+    if (p.hi_on) {
+        h.hi = 1;
+        h.hi_exact = p.hi_exact ? 1 : 0;
+        h.hi_unlisted = p.hi_unlisted ? 1 : 0;
+        h.hi_capricious = p.hi_capricious ? 1 : 0;
+        h.hi_bmode = p.hi_b_mode;
+        h.hi_refresh = p.hi_refresh > 0 ? p.hi_refresh : 1;
+        h.hi_a = p.hi_a;
+        h.hi_epsmax = p.hi_epsmax;
+        h.beta = 0.5f;
+    }
     h.W = (n + 31) / 32;
     h.mask = (!h.grid && resident_smem_bytes(n, h.W, true) <= (size_t)c->smem_dyn_max) ? 1 : 0;
     if (h.grid) {

@@ -80,6 +80,11 @@ struct JobDev {
     float tip[3], chip[3], chip0[3], dir[3], micaR[3], micaR0[3], micaN[3];
     float tipR, tipAp, tipBp, surfAp, surfBp, cantKs, V, dx, tipZeta;
     float fav[4];
+    // ---- hydrodynamics (TEA / exact) ----------------------------------------------
+    int32_t hi, hi_exact, hi_unlisted, hi_capricious, hi_bmode, hi_refresh;
+    float hi_a, hi_epsmax;
+    float beta;           // TEA beta' of the job (bdhitea.cu:158-169)
+    float epsilon;        // last per-job epsilon (for output)
     // ---- status ---------------------------------------------------------------
     int32_t status;
     int32_t pad2[3];

@@ -275,15 +275,24 @@ __global__ void k_cl_geometry(JobDev* __restrict__ Jp, GridAux aux, int nparts, 
         mx[0] = fmaxf(mx[0], z.x); mx[1] = fmaxf(mx[1], z.y); mx[2] = fmaxf(mx[2], z.z);
     }
     float size = J.pp_thr * 1.0001f + 1e-3f;
-    int dims[3];
-    for (;;) {
-        double tot = 1.0;
-        for (int c = 0; c < 3; ++c) {
-            dims[c] = (int)floorf((mx[c] - mn[c]) / size) + 1;
-            tot *= dims[c];
+    int dims[3] = {1, 1, 1};
+    bool ok = true;
+    for (int c = 0; c < 3; ++c) ok = ok && isfinite(mn[c]) && isfinite(mx[c]) && mx[c] >= mn[c];
+    if (!ok) {   // non-finite coordinates: one cell; the job is flagged after the step
+        atomicMax(&Jp->status, SOPB_STATUS_NONFINITE);
+        for (int c = 0; c < 3; ++c) mn[c] = 0.f;
+    } else {
+        for (int it = 0; it < 200; ++it) {   // bounded: each round grows the cells by 25%
+            double tot = 1.0;
+            for (int c = 0; c < 3; ++c) {
+                dims[c] = (int)fminf(floorf((mx[c] - mn[c]) / size) + 1.0f, (float)kCellMax);
+                tot *= dims[c];
+            }
+            if (tot <= (double)kCellMax) break;
+            size *= 1.25f;
         }
-        if (tot <= (double)kCellMax) break;
-        size *= 1.25f;
+        double tot = (double)dims[0] * dims[1] * dims[2];
+        if (tot > (double)kCellMax) { dims[0] = dims[1] = dims[2] = 1; size = 3.0e38f; }
     }
     for (int c = 0; c < 3; ++c) aux.cell_geo[c] = mn[c];
     aux.cell_geo[3] = size;

@@ -57,11 +57,13 @@ __device__ __forceinline__ unsigned group_mask(int lpb) {
     return lpb == 32 ? 0xffffffffu : ((1u << lpb) - 1u);
 }
 
-__device__ __forceinline__ float3 group_reduce(float3 f, int lpb) {
+// Sum over a lane group; `mask` names the lanes taking part (the whole
+// warp, or just the group when groups of a warp run independently).
+__device__ __forceinline__ float3 group_reduce(float3 f, int lpb, unsigned mask = 0xffffffffu) {
     for (int o = lpb >> 1; o > 0; o >>= 1) {
-        f.x += __shfl_xor_sync(0xffffffffu, f.x, o);
-        f.y += __shfl_xor_sync(0xffffffffu, f.y, o);
-        f.z += __shfl_xor_sync(0xffffffffu, f.z, o);
+        f.x += __shfl_xor_sync(mask, f.x, o);
+        f.y += __shfl_xor_sync(mask, f.y, o);
+        f.z += __shfl_xor_sync(mask, f.z, o);
     }
     return f;
 }
@@ -88,14 +90,24 @@ template <bool MASK>
 __device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const uint32_t* vm, int i,
                                               float4 xi, int l, int lpb, float3& f) {
     if (MASK) {
+        // two set bits per round: two independent shared-memory gathers in
+        // flight (the summation order within a lane stays increasing j)
         const uint32_t* row = vm + (size_t)i * J.W;
         for (int w = l; w < J.W; w += lpb) {
             uint32_t m = row[w];
             const float4* xw = xs + 32 * w;
             while (m) {
-                const int b = __ffs(m) - 1;
+                const int b0 = __ffs(m) - 1;
                 m &= m - 1;
-                pair_term(xi, xw[b], J.a2, J.m6, J.cut2, f);
+                if (m) {
+                    const int b1 = __ffs(m) - 1;
+                    m &= m - 1;
+                    const float4 x0 = xw[b0], x1 = xw[b1];
+                    pair_term(xi, x0, J.a2, J.m6, J.cut2, f);
+                    pair_term(xi, x1, J.a2, J.m6, J.cut2, f);
+                } else {
+                    pair_term(xi, xw[b0], J.a2, J.m6, J.cut2, f);
+                }
             }
         }
     } else {
@@ -347,27 +359,35 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     }
     __syncthreads();
 
-    const int lpb = J.lpb, g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
+    const int lpb = J.lpb, l = tid % lpb;
+    const unsigned gmask = group_mask(lpb) << ((tid & 31) & ~(lpb - 1));
     int err = 0;
     int64_t step = J.step;
     int phase = (int)(step % J.stride);       // steps since the last updater pass
     float4* xc = xa;
     float4* xn = xb;
+    __shared__ int next_bead[2];              // per-step bead counters, double buffered
+    if (tid < 2) next_bead[tid] = 0;
+    __syncthreads();
     for (int64_t s = 0; s < nsteps; ++s, ++step) {
         if (phase == 0) run_updaters<BLOCK, MASK>(J, sc, xc, Ts, vm, red, step, err);
         if (++phase == J.stride) phase = 0;
         const float var = sc.var;
-        for (int base = 0; base < n; base += ng) {
-            const int i = base + g;
-            const bool act = i < n;
-            const float4 xi = xc[act ? i : 0];
+        int* counter = &next_bead[s & 1];
+        // lane groups take beads from a shared counter: the busiest groups
+        // stop taking work early instead of holding the CTA at the barrier;
+        // a bead's arithmetic does not depend on which group computes it
+        for (;;) {
+            int i = 0;
+            if (l == 0) i = atomicAdd(counter, 1);
+            i = __shfl_sync(gmask, i, 0, lpb);
+            if (i >= n) break;
+            const float4 xi = xc[i];
             float3 f = make_float3(0.f, 0.f, 0.f);
-            if (act) {
-                bonded_partial(J, xc, i, xi, l, lpb, f);
-                pairs_partial<MASK>(J, xc, vm, i, xi, l, lpb, f);
-            }
-            f = group_reduce(f, lpb);
-            if (act && l == 0) {
+            bonded_partial(J, xc, i, xi, l, lpb, f);
+            pairs_partial<MASK>(J, xc, vm, i, xi, l, lpb, f);
+            f = group_reduce(f, lpb, gmask);
+            if (l == 0) {
                 if (J.indent) {
                     float3 tf;
                     indentation_term(xi, sc.ig, f, tf);
@@ -395,6 +415,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
             }
         }
         __syncthreads();
+        if (tid == 0) *counter = 0;          // reused two steps from now, after a barrier
         float4* t = xc; xc = xn; xn = t;
     }
     for (int i = tid; i < n; i += BLOCK) {

@@ -86,6 +86,7 @@ def lib() -> C.CDLL:
             "sopb_context_create": ([i32, vp, vp], C.c_int),
             "sopb_context_destroy": ([vp], C.c_int),
             "sopb_context_sync": ([vp], C.c_int),
+            "sopb_context_set_shape_policy": ([vp, i32, C.c_float, i32], C.c_int),
             "sopb_job_footprint": ([vp, vp], C.c_int),
             "sopb_job_create": ([vp, vp, vp], C.c_int),
             "sopb_job_destroy": ([vp], C.c_int),
@@ -289,6 +290,11 @@ class Context:
 
     def sync(self) -> None:
         check(lib().sopb_context_sync(self.handle), "sync")
+
+    def set_shape_policy(self, lanes_per_bead: int = 4, work_per_thread: float = 0.0, max_block: int = 1024) -> None:
+        """Resident-kernel shape for jobs created from now on (autotuner knob)."""
+        check(lib().sopb_context_set_shape_policy(self.handle, int(lanes_per_bead), float(work_per_thread),
+                                                  int(max_block)), "set_shape_policy")
 
     def upload_coords(self, jobs: Sequence[Job], xyzw: np.ndarray) -> None:
         arr = self._handles(jobs)

@@ -123,7 +123,7 @@ def test_reference_verlet_list_rebuilt_bit_exact(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", [c for c in cases() if not ref_cases.CASES[c]["cfg"].get("hi_on")])
+@pytest.mark.parametrize("name", cases())
 def test_cuda_path_against_reference_cuda(gpu_ctx, name):
     g, jc, specs = load(name)
     c = ref_cases.CASES[name]

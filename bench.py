@@ -239,7 +239,11 @@ def run_gpu(args):
     specs = batch_specs(rank=rank)
     log("rank %d: generated %d systems in %.1fs" % (rank, len(specs), time.perf_counter() - t0))
     tuned = None
-    if not args.no_autotune:
+    if args.policy:
+        lpb, wpt, maxb = args.policy.split(",")
+        ctx.set_shape_policy(int(lpb), float(wpt), int(maxb))
+        tuned = {"policy": (int(lpb), float(wpt), int(maxb))}
+    elif not args.no_autotune:
         import sopb_autotune
         t0 = time.perf_counter()
         tuned = sopb_autotune.autotune(ctx, specs, steps=100, log=log if rank == 0 else None)
@@ -383,6 +387,7 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--policy", default="", help="lanes_per_bead,work_per_thread,max_block (skips the autotuner)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -377,6 +377,142 @@ def run_gpu(args):
     return 0
 
 
+def capsid_spec():
+    """The 198k-bead shell (180 copies of an 1100-bead chain, icosahedral
+    60 x 3 placement), nanoindented by a 10 nm tip on a ramped cantilever
+    against an attractive substrate; cell-list pairlist."""
+    import sopb
+    import sopb_synth as S
+    s, info = S.make_capsid()
+    x = s.xyz.astype(np.float64)
+    c = x.mean(axis=0)
+    tipR = 100.0
+    tip = [float(c[0]), float(x[:, 1].max() + tipR + 4.0), float(c[2])]
+    p = plain_params(pairs_threshold=40.0, max_possiblePairs=2048, max_pairs=512, possiblepairs_freq=100000,
+                     indentation=1, indentationTipR=tipR, indentationKs=0.07, indentationDeltaX=0.012,
+                     indentationTip=tip, indentationChip=tip, indentationDirection=[0.0, -1.0, 0.0],
+                     indentationSurfaceR0=[0.0, float(x[:, 1].min() - 10.0), 0.0],
+                     indentationSurfaceN=[0.0, 1.0, 0.0], indentationTipZeta=5000.0,
+                     indentationSurfA=1.0, indentationSurfB=-2.0, indentationSurfSigma=10.0, indentationSurfEl=0.2,
+                     indentationFixTrans=1, nav=100)
+    return sopb.JobSpec.from_system(s, p, seed=5032015), info
+
+
+def run_capsid(args):
+    """Large-assembly workload: one 198k-bead job on the grid path."""
+    import torch
+    import sopb
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = sopb.Context(dev, stream=stream.cuda_stream)
+    t0 = time.perf_counter()
+    spec, info = capsid_spec()
+    log("capsid: generated %d beads in %.1fs (%s)" % (spec.n, time.perf_counter() - t0, info))
+    job = ctx.job(spec)
+    chunk = args.chunk
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            ctx.run([job], chunk)
+    ctx.sync()
+    if job.status() != 0:
+        raise RuntimeError("capsid job failed in warm-up: status %d" % job.status())
+    stats = list_stats([job], [spec])
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                starts[k].record(stream)
+                ctx.run([job], chunk)
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    total_ms = sum(s_.elapsed_time(e) for s_, e in zip(starts, ends))
+    if job.status() != 0:
+        raise RuntimeError("capsid job failed: status %d" % job.status())
+    value = spec.n * chunk * args.steps / (total_ms / 1e3)
+    host = torch.empty((spec.n, 4), dtype=torch.float32, pin_memory=True).numpy()
+    ctx.download_coords([job], host)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        ctx.upload_coords([job], host)
+        ctx.run([job], chunk)
+        ctx.download_coords([job], host)
+    torch.cuda.synchronize()
+    e2e = spec.n * chunk * args.steps / (time.perf_counter() - t0)
+    peak, peak_kind = peaks()
+    bps = alg_bytes_per_bead_step(stats, 10)
+    achieved = bps * spec.n * chunk / ((total_ms / 1e3) / args.steps) / 1e9
+    out = {"metric": "bead-steps/s (198k-bead capsid indentation)", "value": value, "unit": UNIT, "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded shell of chain copies)",
+           "config": {"workload": "capsid198k_indentation", "beads": spec.n, "langevin_steps_per_step": chunk,
+                      "pairs_threshold_A": 40.0, "pairlist": "cell list, every 10 steps", "shell": info,
+                      "l2": "flushed between timed steps"},
+           "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": spec.n * 16, "d2h_bytes_per_step": spec.n * 16},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": None, "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats},
+           "tip": job.read(sopb.TIPSTATE)[:11].tolist(), "clocks": clk.summary()}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
+def run_serve(args):
+    """Serving workload: a seeded Poisson stream of pulling, clamp and
+    indentation jobs (sizes log-normal in [50, 5000], 30% with HI: exact for
+    n <= 128, TEA above), served by continuous batching; throughput and
+    p50/p99 completion latency, next to each sampled job's time alone."""
+    import torch
+    import sopb
+    import sopb_serve
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    from serve_mix import poisson_stream
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    ctx = sopb.Context(dev)
+    t0 = time.perf_counter()
+    reqs = poisson_stream(args.serve_jobs, args.serve_rate, 2024, steps_lo=int(1e4 * args.serve_step_scale),
+                          steps_hi=int(1e5 * args.serve_step_scale))
+    log("serve: generated %d requests in %.1fs" % (len(reqs), time.perf_counter() - t0))
+    # warm-up: one small job of each path
+    for r in reqs[:4]:
+        j = ctx.job(r.spec)
+        ctx.run([j], 20)
+        j.destroy()
+    ctx.sync()
+    srv = sopb_serve.Server(ctx, quantum=args.serve_quantum)
+    t0 = time.perf_counter()
+    res = srv.serve(reqs)
+    wall = time.perf_counter() - t0
+    summ = sopb_serve.summarize(res, wall)
+    # the same jobs alone (a sample): latency without the mix
+    alone = []
+    for r in reqs[:: max(1, len(reqs) // 16)]:
+        j = ctx.job(r.spec)
+        ctx.sync()
+        ta = time.perf_counter()
+        ctx.run([j], r.steps)
+        ctx.sync()
+        alone.append(time.perf_counter() - ta)
+        j.destroy()
+    out = {"metric": "bead-steps/s (served Poisson stream)", "value": summ["throughput"], "unit": UNIT,
+           "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
+           "config": {"workload": "serve_poisson", "jobs": len(reqs), "rate_per_s": args.serve_rate,
+                      "sizes": "lognormal [50, 5000]", "hi_fraction": 0.3,
+                      "steps": "log-uniform [%d, %d]" % (int(1e4 * args.serve_step_scale), int(1e5 * args.serve_step_scale)),
+                      "quantum": args.serve_quantum},
+           "serve": summ, "peak_inflight": srv.peak_inflight,
+           "alone_sample": {"jobs": len(alone), "p50_s": float(np.percentile(alone, 50)),
+                            "p99_s": float(np.percentile(alone, 99))}}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -387,10 +523,19 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--workload", default="batch512", choices=["batch512", "serve", "capsid"])
+    ap.add_argument("--serve-jobs", type=int, default=200)
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-quantum", type=int, default=1000)
+    ap.add_argument("--serve-step-scale", type=float, default=0.1)
     ap.add_argument("--policy", default="", help="lanes_per_bead,work_per_thread,max_block (skips the autotuner)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serve":
+        return run_serve(args)
+    if args.workload == "capsid":
+        return run_capsid(args)
     return run_gpu(args)
 
 

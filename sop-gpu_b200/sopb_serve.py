@@ -62,6 +62,8 @@ class Server:
         self.waiting: Deque[Request] = collections.deque()
         self.inflight: Dict[int, dict] = {}
         self.used = 0
+        self.peak_used = 0
+        self.peak_inflight = 0
         self.results: List[Result] = []
         self.t0 = time.perf_counter()
 
@@ -85,7 +87,9 @@ class Server:
                                            self.now(), e.code, None))
                 continue
             self.used += fp
+            self.peak_used = max(self.peak_used, self.used)
             self.inflight[req.rid] = dict(req=req, job=job, done=0, fp=fp, admitted=self.now())
+            self.peak_inflight = max(self.peak_inflight, len(self.inflight))
 
     def _retire(self, rid: int) -> None:
         st = self.inflight.pop(rid)
@@ -114,8 +118,7 @@ class Server:
         self.ctx.sync()
         finished = [rid for rid, st in self.inflight.items() if st["done"] >= st["req"].steps]
         for rid in finished:
-            self._retire(rid)
-        # failed jobs are evicted at once
+            self._retire(rid)       # a failed job stops advancing; its status is reported here
         return len(finished)
 
     def serve(self, arrivals: List[Request], until_idle: bool = True) -> List[Result]:

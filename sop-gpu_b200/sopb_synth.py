@@ -225,3 +225,114 @@ def save_system(prefix: str, sys_: System) -> None:
     os.makedirs(os.path.dirname(prefix) or ".", exist_ok=True)
     write_top(prefix + ".top", sys_)
     write_pdb(prefix + ".pdb", sys_.xyz)
+
+
+# ---------------------------------------------------------------------------
+# Large assembly: a capsid-like shell of chain copies on an icosahedral lattice
+# ---------------------------------------------------------------------------
+def icosahedral_rotations() -> np.ndarray:
+    """The 60 proper rotations of the icosahedron (closure of a 5-fold and a
+    3-fold generator)."""
+    phi = (1.0 + 5.0 ** 0.5) / 2.0
+
+    def rot(axis, ang):
+        a = np.asarray(axis, np.float64)
+        a /= np.linalg.norm(a)
+        K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+        return np.eye(3) + math.sin(ang) * K + (1 - math.cos(ang)) * K @ K
+
+    gens = [rot((0.0, 1.0, phi), 2 * math.pi / 5), rot((1.0, 1.0, 1.0), 2 * math.pi / 3)]
+    group = [np.eye(3)]
+    frontier = [np.eye(3)]
+    while frontier:
+        nxt = []
+        for g in frontier:
+            for h in gens:
+                m = h @ g
+                if not any(np.allclose(m, q, atol=1e-8) for q in group):
+                    group.append(m)
+                    nxt.append(m)
+        frontier = nxt
+    assert len(group) == 60
+    return np.array(group)
+
+
+def make_capsid(copies_per_unit: int = 3, chain_n: int = 1100, seed: int = 7, radius: float = 140.0,
+                slab: float = 22.0, native_cutoff: float = NATIVE_CUTOFF):
+    """A shell of 60 x copies_per_unit copies of an n-bead chain.
+
+    Each copy is a flattened globule (semi-axes a, a, `slab`) whose short axis
+    points along the radius; copies are placed by the icosahedral group from
+    `copies_per_unit` seed directions in one asymmetric unit.  The radius
+    starts at `radius` and grows by 3% until no two beads of different copies
+    are closer than 4 A (180 copies of 1100 beads need ~33 nm).  Natives:
+    |i-j| > 2 within 8 A inside a copy, and every inter-copy pair within 8 A.
+    Returns (System, info)."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    vol = chain_n * 210.0                              # A^3 per bead in a compact globule
+    a = math.sqrt(vol / (4.0 / 3.0 * math.pi * slab))
+    chains = []
+    for k in range(copies_per_unit):
+        x = random_walk(chain_n, seed * 101 + k, shape=(a, a, slab))
+        chains.append(x - x.mean(axis=0))
+    G = icosahedral_rotations()
+    # seed directions: the best-spread of 3000 random draws (largest minimum
+    # angle between any two of the 60 x k images)
+    best, best_sep = None, -1.0
+    for _ in range(3000):
+        d = rng.normal(size=(copies_per_unit, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        P = np.einsum("gij,kj->gki", G, d).reshape(-1, 3)
+        cosm = P @ P.T
+        np.fill_diagonal(cosm, -1.0)
+        sep = math.acos(min(1.0, float(cosm.max())))
+        if sep > best_sep:
+            best, best_sep = d, sep
+    seeds = list(best)
+    R = radius
+    while True:
+        blocks = []
+        for g in G:
+            for k, d in enumerate(seeds):
+                u = g @ d
+                # frame with z along u
+                e1 = np.cross(u, [0.0, 0.0, 1.0])
+                if np.linalg.norm(e1) < 1e-6:
+                    e1 = np.cross(u, [0.0, 1.0, 0.0])
+                e1 /= np.linalg.norm(e1)
+                e2 = np.cross(u, e1)
+                F = np.stack([e1, e2, u], axis=1)
+                blocks.append(chains[k] @ F.T + R * u)
+        X = np.concatenate(blocks)
+        tree = cKDTree(X)
+        copy_id = np.repeat(np.arange(len(blocks)), chain_n)
+        close = tree.query_pairs(4.0, output_type="ndarray")
+        clash = np.any(copy_id[close[:, 0]] != copy_id[close[:, 1]]) if len(close) else False
+        if not clash:
+            break
+        R *= 1.03
+    X = X - 0.0
+    xyz = _round_pdb(X)
+    n = xyz.shape[0]
+    # bonds within copies
+    ii = np.arange(n - 1)
+    same = copy_id[ii] == copy_id[ii + 1]
+    bonds = np.stack([ii[same], ii[same] + 1], axis=1).astype(np.int32)
+    x64 = xyz.astype(np.float64)
+    b_r0 = np.linalg.norm(x64[bonds[:, 1]] - x64[bonds[:, 0]], axis=1)
+    tree = cKDTree(x64)
+    pairs = tree.query_pairs(native_cutoff, output_type="ndarray")
+    pi, pj = np.minimum(pairs[:, 0], pairs[:, 1]), np.maximum(pairs[:, 0], pairs[:, 1])
+    inter = copy_id[pi] != copy_id[pj]
+    intra = (~inter) & (pj - pi > 2)
+    keep = inter | intra
+    pi, pj = pi[keep], pj[keep]
+    order = np.lexsort((pj, pi))
+    natives = np.stack([pi[order], pj[order]], axis=1).astype(np.int32)
+    n_r0 = np.linalg.norm(x64[natives[:, 1]] - x64[natives[:, 0]], axis=1)
+    sys_ = System(xyz, bonds, _round_top(b_r0), natives, _round_top(n_r0), np.full(len(n_r0), EH, np.float32))
+    info = {"radius_A": R, "copies": len(blocks), "chain_n": chain_n, "inter_natives": int(inter[keep].sum()),
+            "slab_A": slab, "min_separation_rad": best_sep}
+    return sys_, info

@@ -105,7 +105,7 @@ class OracleJob:
         shapes = {sopb.COORDS: ((self.n, 4), np.float32), sopb.SEEDS: ((self.n, 4), np.uint32),
                   sopb.TEMP: ((self.n,), np.float32), sopb.FORCES: ((self.n, 4), np.float32),
                   sopb.TIPFORCES: ((self.n, 4), np.float32), sopb.PULLSTATE: ((12,), np.float32),
-                  sopb.TIPSTATE: ((16,), np.float32)}
+                  sopb.TIPSTATE: ((16,), np.float32), sopb.HISTATE: ((4,), np.float32)}
         shape, dt = shapes[what]
         out = np.zeros(shape, dt)
         lib().orc_job_read(self.h, what, out.ctypes.data)

@@ -168,7 +168,7 @@ struct orc_job {
     float fav[4];
     /* HI (bdhitea.cu) */
     float *rf, *mf, *xc, *ci4, *eps;
-    float beta;
+    float beta, epsilon;
     float* tensor;
     int32_t status;
 };
@@ -689,6 +689,7 @@ static void tea_update(orc_job* j) {
     }
     if (eps > j->p.hi_epsmax) j->status = SOPB_ERR_HI;
     double a = (3. * n - 1.) * eps * eps - (3. * n - 2.) * eps;
+    j->epsilon = (float)eps;
     if (fabs(a) < 1e-7) {
         j->beta = .5f;
         if (j->p.hi_capricious && j->p.hi_a > 0.0f) j->status = SOPB_ERR_HI;
@@ -1060,6 +1061,13 @@ void orc_job_read(const orc_job* j, int32_t what, void* out) {
         memcpy(o + 3, j->cant, 12);
         memcpy(o + 6, j->cant0, 12);
         memcpy(o + 9, j->pullvec, 12);
+        break;
+    }
+    case SOPB_HISTATE: {
+        float* o = (float*)out;
+        o[0] = j->beta;
+        o[1] = j->epsilon;
+        o[2] = o[3] = 0.0f;
         break;
     }
     case SOPB_TIPSTATE: {

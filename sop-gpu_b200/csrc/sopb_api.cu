@@ -1003,6 +1003,15 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         std::memcpy(o + 9, j->h.pullvec, 12);
         return SOPB_OK;
     }
+    case SOPB_HISTATE: {
+        int rc = read_slot(j);
+        if (rc) return rc;
+        float* o = (float*)out;
+        o[0] = j->h.beta;
+        o[1] = j->h.epsilon;
+        o[2] = o[3] = 0.0f;
+        return SOPB_OK;
+    }
     case SOPB_TIPSTATE: {
         int rc = read_slot(j);
         if (rc) return rc;

@@ -32,6 +32,18 @@ def test_tea_tracks_oracle(gpu_ctx, n, unlisted, mode):
     g.destroy()
 
 
+@pytest.mark.parametrize("n,unlisted", [(100, 1), (300, 1), (300, 0), (2000, 1)])
+def test_tea_beta_and_epsilon_match_oracle(gpu_ctx, n, unlisted):
+    sp = hi_spec(n, 31, "free", hi_unlisted=unlisted)
+    g, o = gpu_ctx.job(sp), O.OracleJob(sp)
+    gpu_ctx.run([g], 1)            # the TEA updater runs at step 0
+    assert o.advance(1) == 0
+    hg, ho = g.read(sopb.HISTATE), o.read(sopb.HISTATE)
+    assert 0.0 < ho[1] < 1.0 and 0.0 < ho[0] < 1.0
+    assert abs(hg[1] - ho[1]) <= 1e-5 * ho[1] and abs(hg[0] - ho[0]) <= 1e-5 * ho[0]
+    g.destroy()
+
+
 @pytest.mark.parametrize("bmode", [sopb.HI_B_CHOLESKY, sopb.HI_B_REFCOMPAT])
 @pytest.mark.parametrize("n", [20, 40, 128])
 def test_exact_hi_tracks_oracle(gpu_ctx, n, bmode):

@@ -263,6 +263,28 @@ int sopb_job_rebuild_lists(sopb_job* job, int32_t possible, int32_t verlet);
 int sopb_jobs_upload_coords(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, const float* host_xyzw);
 int sopb_jobs_download_coords(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, float* host_xyzw);
 
+/* TEA coupling coefficients of one system, allocating no device memory.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * programs that own all device memory through their own pool and do not let
+ * a library allocate behind them, or code ordering work on a stream where an
+ * allocation would stall or break it.  Runs the TEA updater's kernels (all
+ * pairs, as hi_unlisted) on caller-owned device buffers:
+ *   d_xyzw     in:  float[4n] coordinates (x y z w);
+ *   d_ci4      out: float[4n] per bead, the squared row sums of the normalised
+ *                   RPY blocks (x y z) and the sum of their entries (w), the
+ *                   reference's d_ci / d_epsilon (bdhitea_kernel.cu:234-249);
+ *   d_beta_eps out: float[2] beta' and epsilon (bdhitea.cu:143-169, without
+ *                   the capricious abort).
+ * Scratch is a 4 MiB array in the library image (held by every GPU that
+ * loads the library until exit), shared by all calls: calls that overlap on
+ * the GPU race and must be ordered by the caller.  n up to 262144 beads
+ * (SOPB_ERR_CAPACITY above).  The first call on a device does a one-time
+ * set-up and should come before any stream capture.  Work is queued on
+ * `stream` (a cudaStream_t, NULL = the default stream); the call does not
+ * wait for it. */
+int sopb_tea_coefficients_noalloc(const float* d_xyzw, int32_t n, float hi_a, float* d_ci4, float* d_beta_eps,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1146,3 +1146,144 @@ extern "C" int sopb_jobs_download_coords(sopb_context* c, sopb_job* const* jobs,
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return SOPB_OK;
 }
+
+// ===========================================================================
+// No-allocation entry point: TEA coupling coefficients of one system.
+//
+// Some callers cannot call cudaMalloc: a host program that owns every byte of
+// device memory through its own pool and forbids libraries to allocate
+// behind it (a molecular-dynamics engine or a plugin host), or code that runs
+// where an allocation would stall or break the stream it is ordering work on.
+// This entry point serves them.  It runs the same kernels as the TEA updater
+// of sopb_run (the O(N^2) epsilon sums in j slices, the per-bead reduction
+// and the FP64 beta') on caller-owned inputs and outputs, and keeps its slice
+// partials in the file-scope array below instead of allocated scratch.
+//
+// The array is a fixed part of the library image: every GPU that loads the
+// library holds its 4 MiB until the process exits.  Every call shares it and
+// it keeps the last call's contents; each call overwrites every slot it reads
+// before reading it, so nothing has to start at zero.  Calls that overlap on
+// the GPU (two streams, or two host threads) race on the array and must be
+// ordered by the caller.  The first call on a device does the set-up (it
+// looks up the array's device address with cudaGetSymbolAddress, with that
+// device current); make that first call before any stream capture.
+// ===========================================================================
+#include <mutex>
+
+namespace {
+
+// Slice partials: at most kNoAllocSlots float4, i.e. n x (number of j slices).
+constexpr int kNoAllocSlots = 1 << 18;   // 4 MiB
+static __device__ __align__(256) float4 s_tea_partials[kNoAllocSlots];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;
+float4* g_partials[kMaxDevices] = {};     // device address of s_tea_partials, per device
+int g_sms[kMaxDevices] = {};
+
+// Unlisted branch of k_tea_eps_partial on plain pointers.
+__global__ void __launch_bounds__(kHiTile)
+k_tea_eps_partial_raw(const float4* __restrict__ x, int n, float a, int jsplit, float4* __restrict__ part) {
+    __shared__ float4 xs[kHiTile];
+    const int i = blockIdx.x * kHiTile + threadIdx.x, s = blockIdx.y;
+    const float4 xi = x[i < n ? i : 0];
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int span = ((n + jsplit - 1) / jsplit + kHiTile - 1) / kHiTile * kHiTile;
+    const int j0 = s * span, j1 = min(n, j0 + span);
+    for (int t0 = j0; t0 < j1; t0 += kHiTile) {
+        __syncthreads();
+        if (t0 + threadIdx.x < j1) xs[threadIdx.x] = x[t0 + threadIdx.x];
+        __syncthreads();
+        const int cnt = min(kHiTile, j1 - t0);
+        if (i < n)
+            for (int q = 0; q < cnt; ++q)
+                if (t0 + q != i) eps_stats(xi, xs[q], a, acc);
+    }
+    if (i < n) part[(size_t)s * n + i] = acc;
+}
+
+__global__ void __launch_bounds__(kGridBlock)
+k_tea_eps_reduce_raw(const float4* __restrict__ part, int n, int jsplit, float4* __restrict__ ci4) {
+    for (int i = blockIdx.x * kGridBlock + threadIdx.x; i < n; i += gridDim.x * kGridBlock) {
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int s = 0; s < jsplit; ++s) {
+            const float4 p = part[(size_t)s * n + i];
+            a.x += p.x; a.y += p.y; a.z += p.z; a.w += p.w;
+        }
+        ci4[i] = a;
+    }
+}
+
+// k_tea_beta's arithmetic: epsilon averaged over the 3N(3N-3) off-diagonal
+// entries in FP64, beta' = (1 - sqrt(1 - a)) / a, 0.5 when |a| < 1e-7.
+__global__ void __launch_bounds__(256)
+k_tea_beta_raw(const float4* __restrict__ ci4, int n, float* __restrict__ out) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += 256) s += (double)ci4[i].w;
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double eps = red[0];
+        if (n > 1) eps /= 3. * n * (3. * n - 3.);
+        if (eps > 1.0) eps = 1.0;
+        const double a = (3. * n - 1.) * eps * eps - (3. * n - 2.) * eps;
+        const double beta = fabs(a) < 1e-7 ? 0.5 : (1. - sqrt(1. - a)) / a;
+        out[0] = (float)beta;
+        out[1] = (float)eps;
+    }
+}
+
+}  // namespace
+
+// TEA coupling coefficients of one system, allocating nothing.  See the
+// declaration in include/sopb.h.
+extern "C" int sopb_tea_coefficients_noalloc(const float* d_xyzw, int32_t n, float hi_a, float* d_ci4,
+                                             float* d_beta_eps, void* stream) {
+    if (!d_xyzw || !d_ci4 || !d_beta_eps || n < 1 || !(hi_a > 0.0f)) return SOPB_ERR_INVALID;
+    if (n > kNoAllocSlots) return SOPB_ERR_CAPACITY;   // one slice of n partials must fit the array
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return SOPB_ERR_NODEVICE;
+    }
+    float4* part = nullptr;
+    int sms = 0;
+    {
+        // set-up, once per device, with that device current: the device
+        // address of the array (host code cannot use the symbol itself)
+        std::lock_guard<std::mutex> lock(g_mutex);
+        if (!g_partials[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, s_tea_partials);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return SOPB_ERR_CUDA;
+            }
+            if (cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+                cudaGetLastError();
+                return SOPB_ERR_CUDA;
+            }
+            g_partials[dev] = static_cast<float4*>(p);
+        }
+        part = g_partials[dev];
+        sms = g_sms[dev];
+    }
+    // the TEA updater's slicing (4 CTAs per SM), capped by the array
+    const int itiles = (n + kHiTile - 1) / kHiTile;
+    int jsplit = std::max(1, std::min((4 * sms + itiles - 1) / itiles, itiles));
+    jsplit = std::min(jsplit, kNoAllocSlots / n);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const float4* x = reinterpret_cast<const float4*>(d_xyzw);
+    float4* ci4 = reinterpret_cast<float4*>(d_ci4);
+    k_tea_eps_partial_raw<<<dim3(itiles, jsplit), kHiTile, 0, st>>>(x, n, hi_a, jsplit, part);
+    const int rb = std::max(1, std::min((n + kGridBlock - 1) / kGridBlock, sms * 8));
+    k_tea_eps_reduce_raw<<<rb, kGridBlock, 0, st>>>(part, n, jsplit, ci4);
+    k_tea_beta_raw<<<1, 256, 0, st>>>(ci4, n, d_beta_eps);
+    if (cudaGetLastError() != cudaSuccess) return SOPB_ERR_CUDA;
+    return SOPB_OK;
+}

@@ -101,6 +101,7 @@ def lib() -> C.CDLL:
             "sopb_job_rebuild_lists": ([vp, i32, i32], C.c_int),
             "sopb_jobs_upload_coords": ([vp, vp, i32, vp], C.c_int),
             "sopb_jobs_download_coords": ([vp, vp, i32, vp], C.c_int),
+            "sopb_tea_coefficients_noalloc": ([vp, i32, C.c_float, vp, vp, vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)

@@ -240,9 +240,9 @@ def run_gpu(args):
     log("rank %d: generated %d systems in %.1fs" % (rank, len(specs), time.perf_counter() - t0))
     tuned = None
     if args.policy:
-        lpb, wpt, maxb = args.policy.split(",")
-        ctx.set_shape_policy(int(lpb), float(wpt), int(maxb))
-        tuned = {"policy": (int(lpb), float(wpt), int(maxb))}
+        lpb, bpg, maxb = args.policy.split(",")
+        ctx.set_shape_policy(int(lpb), float(bpg), int(maxb))
+        tuned = {"policy": (int(lpb), float(bpg), int(maxb))}
     elif not args.no_autotune:
         import sopb_autotune
         t0 = time.perf_counter()
@@ -359,7 +359,7 @@ def run_gpu(args):
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": beads * 16, "d2h_bytes_per_step": beads * 16},
             "gpu_launches": launches,
             "shape_policy": None if tuned is None else {"lanes_per_bead": tuned["policy"][0],
-                                                        "work_per_thread": tuned["policy"][1],
+                                                        "beads_per_group": tuned["policy"][1],
                                                         "max_block": tuned["policy"][2]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
@@ -528,7 +528,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-quantum", type=int, default=1000)
     ap.add_argument("--serve-step-scale", type=float, default=0.1)
-    ap.add_argument("--policy", default="", help="lanes_per_bead,work_per_thread,max_block (skips the autotuner)")
+    ap.add_argument("--policy", default="", help="lanes_per_bead,beads_per_group,max_block (skips the autotuner)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

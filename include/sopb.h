@@ -201,12 +201,14 @@ int sopb_generate_seeds(int32_t seed, int64_t count, uint32_t* out4);
 int sopb_context_create(int32_t device, void* stream, sopb_context** out);
 int sopb_context_destroy(sopb_context* ctx);
 /* Shape policy of the resident kernel for jobs created from now on: lanes
- * cooperating on one bead, and threads per job (work_per_thread <= 0: one
- * bead per lane group; > 0: threads in proportion to the expected work of a
- * step).  The autotuner's knob; a job keeps the shape it was created with,
- * so its result is the same alone and in any mix.  No reference
- * counterpart (the reference runs one thread per bead, src/gsop.cuh:13). */
-int sopb_context_set_shape_policy(sopb_context* ctx, int32_t lanes_per_bead, float work_per_thread, int32_t max_block);
+ * cooperating on one bead's force sum (a power of two up to 32, default
+ * 32), and beads per lane group (default 8; the CTA holds about
+ * n / beads_per_group groups, between 64 threads and max_block; <= 0 means
+ * one bead per group).  The autotuner's knob; a job keeps the shape it was
+ * created with, so its result is the same alone and in any mix.  No
+ * reference counterpart (the reference runs one thread per bead,
+ * src/gsop.cuh:13). */
+int sopb_context_set_shape_policy(sopb_context* ctx, int32_t lanes_per_bead, float beads_per_group, int32_t max_block);
 
 /* Blocks until the context's stream drains; returns the first job error. */
 int sopb_context_sync(sopb_context* ctx);

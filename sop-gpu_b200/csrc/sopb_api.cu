@@ -62,8 +62,8 @@ inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 // Shape policy of the resident kernel (see launch_shape).
 struct ShapePolicy {
-    int32_t lpb = 4;
-    float work_per_thread = 0.0f;
+    int32_t lpb = 32;
+    float beads_per_group = 8.0f;
     int32_t max_block = 1024;
 };
 
@@ -143,27 +143,21 @@ int set_smem_attr(int device, int* dyn_out) {
 
 // Lanes per bead and CTA size of a job.  A function of the job and of the
 // context's shape policy only (never of the batch it runs in), so a job's
-// arithmetic is identical alone and in any mix.  Policy:
-//   work_per_thread <= 0: one bead per lane group (CTA = n * lanes, rounded up
-//                         to a power of two, at most max_block);
-//   work_per_thread  > 0: threads in proportion to the expected work of a
-//                         step, n x (Verlet partners per bead, ~20 n^0.28 for a
-//                         compact globule at a 20 A cutoff) / work_per_thread.
-// sopb_context_set_shape_policy sets it (the autotuner's knob).
+// arithmetic is identical alone and in any mix.  The CTA holds about
+// n / beads_per_group lane groups of `lpb` lanes (a power of two, 64..max_block
+// threads): lane groups take beads dynamically, so several beads per group
+// even out the differing list lengths.  sopb_context_set_shape_policy sets
+// it (the autotuner's knob).
 void launch_shape(const ShapePolicy& pol, int32_t n, int32_t lpb_req, int32_t* lpb, int32_t* block) {
     int32_t l = lpb_req > 0 ? lpb_req : pol.lpb;
     int32_t p2 = 1;
     while (p2 < l && p2 < 32) p2 <<= 1;
     l = p2;
     const int32_t maxb = pol.max_block >= 64 && pol.max_block <= 1024 ? pol.max_block : 1024;
+    const float bpg = pol.beads_per_group > 0.0f ? pol.beads_per_group : 1.0f;
+    const float want = std::ceil((float)n / bpg) * (float)l;
     int32_t b = 64;
-    if (pol.work_per_thread <= 0.0f) {
-        const int64_t want = (int64_t)n * l;
-        while (b < maxb && b < want) b <<= 1;
-    } else {
-        const float want = (float)n * 20.0f * powf((float)n, 0.28f) / pol.work_per_thread;
-        while (b < maxb && (float)b * 1.41421356f < want) b <<= 1;
-    }
+    while (b < maxb && (float)b < want) b <<= 1;
     while (b < 1024 && b < l) b <<= 1;
     *lpb = l;
     *block = b;
@@ -320,11 +314,11 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     return SOPB_OK;
 }
 
-extern "C" int sopb_context_set_shape_policy(sopb_context* c, int32_t lanes_per_bead, float work_per_thread,
+extern "C" int sopb_context_set_shape_policy(sopb_context* c, int32_t lanes_per_bead, float beads_per_group,
                                              int32_t max_block) {
     if (!c || lanes_per_bead < 1 || lanes_per_bead > 32 || max_block < 64 || max_block > 1024) return SOPB_ERR_INVALID;
     c->policy.lpb = lanes_per_bead;
-    c->policy.work_per_thread = work_per_thread;
+    c->policy.beads_per_group = beads_per_group;
     c->policy.max_block = max_block;
     return SOPB_OK;
 }
@@ -725,7 +719,28 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
         h.beta = 0.5f;
     }
     h.W = (n + 31) / 32;
-    h.mask = (!h.grid && resident_smem_bytes(n, h.W, true) <= (size_t)c->smem_dyn_max) ? 1 : 0;
+    h.mask = h.grid ? 0 : 1;
+    if (!h.grid) {
+        // shared-memory cache of the Verlet list: the list at the initial
+        // coordinates plus 15% and 8 entries per bead, as far as it fits
+        const float cut = std::min(p.pairlist_cutoff, p.pairs_threshold);
+        std::vector<uint8_t> bonded((size_t)n * n, 0);
+        for (int32_t i = 0; i < n; ++i) {
+            for (int32_t k = m.cov_off[i]; k < m.cov_off[i + 1]; ++k) bonded[(size_t)i * n + m.cov_j[k]] = 1;
+            for (int32_t k = m.nat_off[i]; k < m.nat_off[i + 1]; ++k) bonded[(size_t)i * n + m.nat_j[k]] = 1;
+        }
+        int64_t total = 0;
+        for (int32_t i = 0; i < n; ++i)
+            for (int32_t q = i + 1; q < n; ++q) {
+                const float dx = d->xyz[3 * q] - d->xyz[3 * i], dy = d->xyz[3 * q + 1] - d->xyz[3 * i + 1],
+                            dz = d->xyz[3 * q + 2] - d->xyz[3 * i + 2];
+                if (!bonded[(size_t)i * n + q] && std::sqrt(dx * dx + dy * dy + dz * dz) < cut) total += 2;
+            }
+        int64_t want = (int64_t)std::ceil(1.15 * (double)total) + 8 * (int64_t)n;
+        want = std::min<int64_t>(want, (int64_t)n * h.cap_pl);
+        const int64_t fit = ((int64_t)c->smem_dyn_max - (int64_t)resident_smem_bytes(n, 0)) / 2;
+        h.lcache = (int32_t)std::max<int64_t>(0, std::min(want, fit));
+    }
     if (h.grid) {
         h.lpb = kGridLpb;
         h.block = 1024;
@@ -755,12 +770,11 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     const size_t o_natpar = o_natj + align256(m.nat_j.size() * 4 + 4);
     const size_t o_ex = o_natpar + align256(m.nat_par.size() * 8 + 8);
     const size_t o_ppm = o_ex + align256(mask_bytes);
-    const size_t o_plm = o_ppm + (h.mask ? align256(mask_bytes) : 0);
-    const size_t o_ppcnt = o_plm + (h.mask ? align256(mask_bytes) : 0);
+    const size_t o_ppcnt = o_ppm + (h.mask ? align256(mask_bytes) : 0);
     const size_t o_plcnt = o_ppcnt + align256((size_t)n * 4);
     const size_t o_ppj = o_plcnt + align256((size_t)n * 4);
     const size_t o_plj = o_ppj + (h.mask ? 0 : align256((size_t)n * h.cap_pp * 4));
-    const size_t total = o_plj + (h.mask ? 0 : align256((size_t)n * h.cap_pl * 4));
+    const size_t total = o_plj + align256((size_t)n * h.cap_pl * 4);
     sopb_job* j = new (std::nothrow) sopb_job();
     if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
     cudaError_t e = cudaMalloc(&j->dmem, total);
@@ -779,11 +793,10 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.nat_par = (float2*)(base + o_natpar);
     h.ex_mask = h.grid ? nullptr : (uint32_t*)(base + o_ex);
     h.pp_mask = h.mask ? (uint32_t*)(base + o_ppm) : nullptr;
-    h.pl_mask = h.mask ? (uint32_t*)(base + o_plm) : nullptr;
     h.pp_cnt = (int32_t*)(base + o_ppcnt);
     h.pl_cnt = (int32_t*)(base + o_plcnt);
     h.pp_j = h.mask ? nullptr : (int32_t*)(base + o_ppj);
-    h.pl_j = h.mask ? nullptr : (int32_t*)(base + o_plj);
+    h.pl_j = (int32_t*)(base + o_plj);
     h.x = c->x + b0;
     h.xalt = c->xalt + b0;
     h.seeds = c->seeds + b0;
@@ -791,7 +804,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.tipF = c->tipF + b0;
     h.flags = c->flags + b0;
     cudaStream_t st = c->stream;
-    CUDA_TRY(cudaMemsetAsync(base + o_ppm, 0, o_ppj - o_ppm, st));   // masks and counts
+    CUDA_TRY(cudaMemsetAsync(base + o_ppm, 0, o_ppj - o_ppm, st));   // mask and counts
     if (!h.grid) CUDA_TRY(cudaMemcpyAsync(h.ex_mask, ex.data(), mask_bytes, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(h.cov_off, m.cov_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
     if (!m.cov_j.empty()) {
@@ -868,7 +881,7 @@ void group_jobs(sopb_job* const* jobs, int32_t njobs, std::vector<LaunchClass>& 
         L.block = h.block;
         L.mask = h.mask != 0;
         L.max_n = std::max(L.max_n, jobs[k]->n);
-        L.smem = std::max(L.smem, resident_smem_bytes(jobs[k]->n, h.W, L.mask));
+        L.smem = std::max(L.smem, resident_smem_bytes(jobs[k]->n, h.lcache));
         L.ids.push_back(jobs[k]->slot);
     }
     out.clear();
@@ -1052,11 +1065,10 @@ extern "C" int sopb_job_pairlist(sopb_job* j, int32_t possible, int32_t* counts,
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
     const int32_t n = j->n;
-    if (j->h.mask) {
+    if (j->h.mask && possible) {
         const int32_t W = j->h.W;
         std::vector<uint32_t> msk((size_t)n * W);
-        CUDA_TRY(cudaMemcpyAsync(msk.data(), possible ? j->h.pp_mask : j->h.pl_mask, msk.size() * 4,
-                                 cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(msk.data(), j->h.pp_mask, msk.size() * 4, cudaMemcpyDeviceToHost, c->stream));
         CUDA_TRY(cudaStreamSynchronize(c->stream));
         for (int32_t i = 0; i < n; ++i) {
             int32_t k = 0;

@@ -32,6 +32,7 @@ struct JobDev {
     int32_t max_pp;       // configured max_possiblePairs (overflow -> error)
     int32_t max_pl;       // configured max_pairs
     int32_t grid;         // 1: grid path (per-step kernels, CUDA graphs)
+    int32_t lcache;       // shared-memory cache of the Verlet list, entries
     int32_t stride;       // updater period (gsop.cu:117-122)
     int32_t nav;
     int32_t pairs_freq;
@@ -61,7 +62,6 @@ struct JobDev {
     int32_t* pl_j;        // [n * cap_pl]
     uint32_t* ex_mask;    // [n * W] bonded + native partners and self
     uint32_t* pp_mask;    // [n * W] possible pairs (MASK mode)
-    uint32_t* pl_mask;    // [n * W] Verlet pairs (MASK mode, between launches)
     // ---- force field ---------------------------------------------------------
     float ks, R2;         // FENE: kspring_cov, R_limit^2
     float a2, m6, cut2;   // repulsive: a^2, -6 el / a^2, pairs_cutoff^2

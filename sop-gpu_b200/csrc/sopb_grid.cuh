@@ -76,7 +76,7 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
         float3 f = make_float3(0.f, 0.f, 0.f);
         if (act) {
             bonded_partial(J, J.x, i, xi, l, lpb, f);
-            pairs_partial<false>(J, J.x, nullptr, i, xi, l, lpb, f);
+            pairs_partial(J, J.x, nullptr, nullptr, false, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {

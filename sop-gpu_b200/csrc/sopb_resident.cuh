@@ -9,28 +9,33 @@
 // and copies all coordinates to the host every `stride` steps for pulling,
 // src/Potentials/pulling.cu:152-165).
 //
-// Neighbour lists, two representations chosen per job:
-//   MASK  (jobs whose bitmasks fit in shared memory, n <= ~1100): the Verlet
-//         list of bead i is a bitmask over the job's beads held in shared
-//         memory (n*ceil(n/32) words), the possible-pairs list a bitmask in
-//         global memory, bonded/native exclusions a precomputed bitmask.
-//         Set bits are visited in increasing j, the reference's list order.
-//   ROWS  (larger jobs): fixed-capacity index rows in global memory, the
-//         reference's layout transposed to bead-major.
+// Neighbour lists.  The Verlet list of every job is a set of bead-major,
+// order-preserving index rows in global memory (the reference's slot-major
+// d_pairs transposed), cached in shared memory as a compact CSR copy of u16
+// indices whenever the whole list fits the job's cache; the possible-pairs
+// list is, per job,
+//   MASK  (n <= ~1100): a bitmask over the job's beads, with bonded/native
+//         exclusions as a precomputed bitmask;
+//   ROWS  (larger jobs): index rows like the Verlet list.
+// Partners are always visited in increasing j, the reference's list order.
 //
-// Work split: `lpb` lanes (a power of two <= 32, aligned inside a warp)
-// cooperate on one bead: they stride over its covalent, native and Verlet
-// entries (mask words) and combine partial forces with xor-shuffles; lane 0
-// then draws the bead's noise and integrates.  Loops containing warp
-// collectives have CTA-uniform trip counts.
+// One step is two phases.  Forces: a group of `lpb` lanes (a power of two
+// <= 32, a whole warp by default) takes beads from a shared counter, strides
+// over the bead's covalent, native and Verlet entries, combines the partial
+// forces with xor-shuffles and stores the bead's force in shared memory.
+// Integration: one thread per bead draws the noise and moves the bead.  A
+// bead's arithmetic depends only on the job and on lpb, never on which group
+// computed it or on the list's location (cache or global rows).
 #pragma once
 
 #include "sopb_device.cuh"
 
 namespace sopb {
 
-constexpr int kMaxResidentBeads = 4096;     // ROWS mode: 52 B of shared memory per bead
-constexpr int kResidentSmemPerBead = 52;
+constexpr int kMaxResidentBeads = 2048;
+// shared memory per bead: coordinates x2, RNG state, force (16 B each),
+// temperature and the cache's row offset (4 B each)
+constexpr int kResidentSmemPerBead = 72;
 
 struct StepScalars {
     float var;
@@ -84,36 +89,19 @@ __device__ __forceinline__ void bonded_partial(const JobDev& J, const float4* __
     for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[__ldg(&J.nat_j[k])], __ldg(&J.nat_par[k]), f);
 }
 
-// Verlet-pair terms: ROWS mode walks the bead's index row; MASK mode walks
-// the set bits of its mask words (lane l takes words l, l+lpb, ...).
-template <bool MASK>
-__device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const uint32_t* vm, int i,
-                                              float4 xi, int l, int lpb, float3& f) {
-    if (MASK) {
-        // two set bits per round: two independent shared-memory gathers in
-        // flight (the summation order within a lane stays increasing j)
-        const uint32_t* row = vm + (size_t)i * J.W;
-        for (int w = l; w < J.W; w += lpb) {
-            uint32_t m = row[w];
-            const float4* xw = xs + 32 * w;
-            while (m) {
-                const int b0 = __ffs(m) - 1;
-                m &= m - 1;
-                if (m) {
-                    const int b1 = __ffs(m) - 1;
-                    m &= m - 1;
-                    const float4 x0 = xw[b0], x1 = xw[b1];
-                    pair_term(xi, x0, J.a2, J.m6, J.cut2, f);
-                    pair_term(xi, x1, J.a2, J.m6, J.cut2, f);
-                } else {
-                    pair_term(xi, xw[b0], J.a2, J.m6, J.cut2, f);
-                }
-            }
-        }
+// Verlet-pair terms of bead i, lane l of lpb taking entries l, l+lpb, ...,
+// from the shared-memory cache when the list fits it, else from the rows.
+__device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const int32_t* off,
+                                              const uint16_t* nbr, bool cached, int i, float4 xi, int l, int lpb,
+                                              float3& f) {
+    if (cached) {
+        const int k0 = off[i], cnt = off[i + 1] - k0;
+        const uint16_t* r = nbr + k0;
+        for (int k = l; k < cnt; k += lpb) pair_term(xi, xs[r[k]], J.a2, J.m6, J.cut2, f);
     } else {
-        const int np = J.pl_cnt[i];
-        const int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
-        for (int k = l; k < np; k += lpb) pair_term(xi, xs[row[k]], J.a2, J.m6, J.cut2, f);
+        const int cnt = J.pl_cnt[i];
+        const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
+        for (int k = l; k < cnt; k += lpb) pair_term(xi, xs[r[k]], J.a2, J.m6, J.cut2, f);
     }
 }
 
@@ -170,7 +158,7 @@ __device__ void build_possible(const JobDev& J, const float4* __restrict__ xs, i
 // generate_pairs (src/Updaters/pairlist_kernel.cu:33-76): the possible pairs
 // with |r| < pairlist_cutoff, order kept.  More than max_pairs sets err.
 template <int BLOCK, bool MASK>
-__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, uint32_t* vm, int& err) {
+__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int& err) {
     const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
     const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
     for (int base = 0; base < n; base += ng) {
@@ -179,20 +167,38 @@ __device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, uin
         const float4 xi = xs[act ? i : 0];
         int cnt = 0;
         if (MASK) {
-            if (act) {
-                for (int w = l; w < J.W; w += lpb) {
-                    uint32_t m = J.pp_mask[(size_t)i * J.W + w], out = 0;
+            // words in order, lpb at a time; lanes' bits placed by an
+            // exclusive scan of their counts, so the row stays in increasing j
+            int32_t* row = J.pl_j + (size_t)(act ? i : 0) * J.cap_pl;
+            for (int wb = 0; wb < J.W; wb += lpb) {
+                const int w = wb + l;
+                uint32_t out = 0;
+                if (act && w < J.W) {
+                    uint32_t m = J.pp_mask[(size_t)i * J.W + w];
                     while (m) {
                         const int b = __ffs(m) - 1;
                         m &= m - 1;
                         if (within_cutoff(xi, xs[32 * w + b], J.pl_cut)) out |= 1u << b;
                     }
-                    vm[(size_t)i * J.W + w] = out;
-                    cnt += __popc(out);
                 }
+                const int c = __popc(out);
+                int incl = c;
+                for (int o = 1; o < lpb; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o, lpb);
+                    if (l >= o) incl += t;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, lpb - 1, lpb);
+                int pos = cnt + incl - c;
+                while (out) {
+                    const int b = __ffs(out) - 1;
+                    out &= out - 1;
+                    if (pos < J.cap_pl) row[pos] = 32 * w + b;
+                    else err = SOPB_STATUS_CAPACITY;
+                    ++pos;
+                }
+                cnt += total;
             }
-            cnt = group_sum(cnt, lpb);
-            if (act && l == 0 && cnt > J.max_pl) err = SOPB_STATUS_CAPACITY;
+            if (act && l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
         } else {
             const int gbase = (tid & 31) & ~(lpb - 1);
             const unsigned gm = group_mask(lpb);
@@ -267,11 +273,52 @@ __device__ __noinline__ void tip_update(const JobDev& J, StepScalars& sc, float3
     sc.fav[3] = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], f[0]), __fmul_rn(f[1], f[1])), __fmul_rn(f[2], f[2])));
 }
 
+// Shared-memory cache of the Verlet rows as compact CSR: offsets by a CTA
+// scan of the row counts, then the entries as u16.  Returns 1 when the whole
+// list fits `cap` entries (else the rows are read from global memory).
+template <int BLOCK>
+__device__ int fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap, int* tot_smem) {
+    const int n = J.n, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int per = (n + BLOCK - 1) / BLOCK, b0 = tid * per, b1 = min(n, b0 + per);
+    int s = 0;
+    for (int i = b0; i < b1; ++i) s += J.pl_cnt[i];
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    __shared__ int wsum[BLOCK / 32];
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (tid == 0) {
+        int run = 0;
+        for (int q = 0; q < BLOCK / 32; ++q) { const int v = wsum[q]; wsum[q] = run; run += v; }
+        *tot_smem = run;
+    }
+    __syncthreads();
+    int run = wsum[w] + incl - s;
+    for (int i = b0; i < b1; ++i) { off[i] = run; run += J.pl_cnt[i]; }
+    if (tid == 0) off[n] = *tot_smem;
+    __syncthreads();
+    const int fits = *tot_smem <= cap;
+    if (fits) {
+        const int lpb = J.lpb, g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
+        for (int i = g; i < n; i += ng) {
+            const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
+            const int k0 = off[i], cnt = off[i + 1] - k0;
+            for (int k = l; k < cnt; k += lpb) nbr[k0 + k] = (uint16_t)r[k];
+        }
+    }
+    __syncthreads();
+    return fits;
+}
+
 // The updaters of one `stride` boundary in the reference order
 // (creation order in src/gsop.cu:80-101; loop in src/gsop.cu:129-133).
+// Returns 1 when the Verlet list was rebuilt.
 template <int BLOCK, bool MASK>
-__device__ __noinline__ void run_updaters(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, float* Ts, uint32_t* vm,
-                             float (*red)[4], int64_t step, int& err) {
+__device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, float* Ts,
+                                         float (*red)[4], int64_t step, int& err) {
     const int tid = threadIdx.x, n = J.n;
     if (J.indent) {
         if (tid == 0 && step == J.retraction_step) sc.V = -sc.V;
@@ -298,9 +345,10 @@ __device__ __noinline__ void run_updaters(const JobDev& J, StepScalars& sc, cons
     if (pp) build_possible<BLOCK, MASK>(J, xs, err);
     if (step % J.nav == 0)
         for (int i = tid; i < n; i += BLOCK) Ts[i] = 0.0f;   // output_manager.cu:125-127
-    if (step % J.pairs_freq == 0) {
+    const bool verlet = step % J.pairs_freq == 0;
+    if (verlet) {
         if (pp) __syncthreads();
-        build_verlet<BLOCK, MASK>(J, xs, vm, err);
+        build_verlet<BLOCK, MASK>(J, xs, err);
     }
     if (J.heating && tid == 0 && step % J.temp_freq == 0) {
         // TemperatureUpdater (src/Integrators/langevin.cu:129-135, 44-48)
@@ -308,11 +356,12 @@ __device__ __noinline__ void run_updaters(const JobDev& J, StepScalars& sc, cons
         sc.var = __fsqrt_rn(__fdiv_rn(__fmul_rn(__fmul_rn(2.0f, temp), J.zeta), J.h));
     }
     __syncthreads();
+    return verlet ? 1 : 0;
 }
 
 // Shared-memory bytes of a job's resident launch.
-__host__ __device__ inline size_t resident_smem_bytes(int n, int W, bool mask) {
-    return (size_t)n * kResidentSmemPerBead + (mask ? (size_t)n * W * 4 : 0);
+__host__ __device__ inline size_t resident_smem_bytes(int n, int cache_entries) {
+    return ((size_t)n * kResidentSmemPerBead + 16 + (size_t)cache_entries * 2 + 15) & ~(size_t)15;
 }
 
 // Register cap of 64 per thread: 1024 threads of resident CTAs per SM.
@@ -328,19 +377,20 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ StepScalars sc;
     __shared__ float red[BLOCK / 32][4];
+    __shared__ int list_total;
     const int n = J.n, tid = threadIdx.x;
     float4* xa = reinterpret_cast<float4*>(smem);
     float4* xb = xa + n;
     uint4* sd = reinterpret_cast<uint4*>(xb + n);
-    float* Ts = reinterpret_cast<float*>(sd + n);
-    uint32_t* vm = reinterpret_cast<uint32_t*>(Ts + n);   // MASK mode Verlet masks
+    float4* F = reinterpret_cast<float4*>(sd + n);
+    float* Ts = reinterpret_cast<float*>(F + n);
+    int32_t* off = reinterpret_cast<int32_t*>(Ts + n);
+    uint16_t* nbr = reinterpret_cast<uint16_t*>(off + n + 4);
     for (int i = tid; i < n; i += BLOCK) {
         xa[i] = J.x[i];
         sd[i] = J.seeds[i];
         Ts[i] = J.T[i];
     }
-    if (MASK)
-        for (int w = tid; w < n * J.W; w += BLOCK) vm[w] = J.pl_mask[w];
     if (tid == 0) {
         sc.var = J.var;
         for (int c = 0; c < 3; ++c) {
@@ -358,6 +408,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
         sc.err = 0;
     }
     __syncthreads();
+    int cached = fill_cache<BLOCK>(J, off, nbr, J.lcache, &list_total);
 
     const int lpb = J.lpb, l = tid % lpb;
     const unsigned gmask = group_mask(lpb) << ((tid & 31) & ~(lpb - 1));
@@ -370,13 +421,11 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     if (tid < 2) next_bead[tid] = 0;
     __syncthreads();
     for (int64_t s = 0; s < nsteps; ++s, ++step) {
-        if (phase == 0) run_updaters<BLOCK, MASK>(J, sc, xc, Ts, vm, red, step, err);
+        if (phase == 0 && run_updaters<BLOCK, MASK>(J, sc, xc, Ts, red, step, err))
+            cached = fill_cache<BLOCK>(J, off, nbr, J.lcache, &list_total);
         if (++phase == J.stride) phase = 0;
-        const float var = sc.var;
         int* counter = &next_bead[s & 1];
-        // lane groups take beads from a shared counter: the busiest groups
-        // stop taking work early instead of holding the CTA at the barrier;
-        // a bead's arithmetic does not depend on which group computes it
+        // forces: lane groups take beads from a shared counter
         for (;;) {
             int i = 0;
             if (l == 0) i = atomicAdd(counter, 1);
@@ -385,7 +434,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
             const float4 xi = xc[i];
             float3 f = make_float3(0.f, 0.f, 0.f);
             bonded_partial(J, xc, i, xi, l, lpb, f);
-            pairs_partial<MASK>(J, xc, vm, i, xi, l, lpb, f);
+            pairs_partial(J, xc, off, nbr, cached, i, xi, l, lpb, f);
             f = group_reduce(f, lpb, gmask);
             if (l == 0) {
                 if (J.indent) {
@@ -395,27 +444,36 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
                     t.x += tf.x; t.y += tf.y; t.z += tf.z;
                     J.tipF[i] = t;
                 }
-                // integrateLangevin_kernel (src/Integrators/langevin_kernel.cu:17-58)
-                if (!J.minimization) {
-                    uint4 st = sd[i];
-                    const float4 gg = gaussian4(st);
-                    sd[i] = st;
-                    f.x += gg.x * var;
-                    f.y += gg.y * var;
-                    f.z += gg.z * var;
-                }
-                if (J.pulling) {
-                    const uint8_t fl = J.flags[i];
-                    if (fl == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
-                    if (fl == FLAG_PULLED) { f.x += sc.pullF[0]; f.y += sc.pullF[1]; f.z += sc.pullF[2]; }
-                }
-                const float dx = J.hOverZeta * f.x, dy = J.hOverZeta * f.y, dz = J.hOverZeta * f.z;
-                xn[i] = make_float4(xi.x + dx, xi.y + dy, xi.z + dz, xi.w);
-                Ts[i] += J.tempNorm * (dx * dx + dy * dy + dz * dz);
+                F[i] = make_float4(f.x, f.y, f.z, 0.f);
             }
         }
         __syncthreads();
         if (tid == 0) *counter = 0;          // reused two steps from now, after a barrier
+        // integrateLangevin_kernel (src/Integrators/langevin_kernel.cu:17-58),
+        // one thread per bead
+        const float var = sc.var;
+        for (int i = tid; i < n; i += BLOCK) {
+            const float4 f4 = F[i];
+            float3 f = make_float3(f4.x, f4.y, f4.z);
+            if (!J.minimization) {
+                uint4 st = sd[i];
+                const float4 gg = gaussian4(st);
+                sd[i] = st;
+                f.x += gg.x * var;
+                f.y += gg.y * var;
+                f.z += gg.z * var;
+            }
+            if (J.pulling) {
+                const uint8_t fl = J.flags[i];
+                if (fl == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
+                if (fl == FLAG_PULLED) { f.x += sc.pullF[0]; f.y += sc.pullF[1]; f.z += sc.pullF[2]; }
+            }
+            const float4 xi = xc[i];
+            const float dx = J.hOverZeta * f.x, dy = J.hOverZeta * f.y, dz = J.hOverZeta * f.z;
+            xn[i] = make_float4(xi.x + dx, xi.y + dy, xi.z + dz, xi.w);
+            Ts[i] += J.tempNorm * (dx * dx + dy * dy + dz * dz);
+        }
+        __syncthreads();
         float4* t = xc; xc = xn; xn = t;
     }
     for (int i = tid; i < n; i += BLOCK) {
@@ -425,8 +483,6 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
         J.seeds[i] = sd[i];
         J.T[i] = Ts[i];
     }
-    if (MASK)
-        for (int w = tid; w < n * J.W; w += BLOCK) J.pl_mask[w] = vm[w];
     if (err) atomicMax(&sc.err, err);
     __syncthreads();
     if (tid == 0) {
@@ -447,8 +503,8 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
 }
 
 // Potential forces only (SOPPotential::compute of every potential, no
-// integrator) at the job's current coordinates, reading the Verlet list the
-// last launch left in global memory; does not touch the tip accumulator.
+// integrator) at the job's current coordinates and Verlet rows, with the
+// step kernel's lane split; does not touch the tip accumulator.
 template <int BLOCK, bool MASK>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, float4* __restrict__ out) {
@@ -467,7 +523,7 @@ k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, 
         float3 f = make_float3(0.f, 0.f, 0.f);
         if (act) {
             bonded_partial(J, J.x, i, xi, l, lpb, f);
-            pairs_partial<MASK>(J, J.x, J.pl_mask, i, xi, l, lpb, f);
+            pairs_partial(J, J.x, nullptr, nullptr, false, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {
@@ -494,7 +550,7 @@ k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int 
     int err = 0;
     if (possible) build_possible<BLOCK, MASK>(J, J.x, err);
     __syncthreads();
-    if (verlet) build_verlet<BLOCK, MASK>(J, J.x, J.pl_mask, err);
+    if (verlet) build_verlet<BLOCK, MASK>(J, J.x, err);
     if (err) atomicMax(&errs, err);
     __syncthreads();
     if (threadIdx.x == 0 && errs) Jp->status = errs;

@@ -14,11 +14,11 @@ from typing import Iterable, List, Optional, Sequence, Tuple
 
 import sopb
 
-Policy = Tuple[int, float, int]   # (lanes per bead, work per thread, max CTA size)
+Policy = Tuple[int, float, int]   # (lanes per bead, beads per lane group, max CTA size)
 
 DEFAULT_CANDIDATES: List[Policy] = [
-    (lpb, wpt, maxb)
-    for lpb, wpt, maxb in itertools.product((2, 4, 8), (0.0, 40.0, 80.0), (512, 1024))
+    (lpb, bpg, maxb)
+    for lpb, bpg, maxb in itertools.product((8, 16, 32), (2.0, 4.0, 8.0), (512, 1024))
 ]
 
 
@@ -47,7 +47,7 @@ def autotune(ctx: "sopb.Context", specs: Sequence["sopb.JobSpec"], steps: int = 
         dt = time_policy(ctx, specs, pol, steps)
         table.append((pol, dt, beads * steps / dt))
         if log:
-            log("autotune lpb=%d wpt=%g maxb=%d: %.3e bead-steps/s" % (pol[0], pol[1], pol[2], beads * steps / dt))
+            log("autotune lpb=%d bpg=%g maxb=%d: %.3e bead-steps/s" % (pol[0], pol[1], pol[2], beads * steps / dt))
     best = min(table, key=lambda t: t[1])[0]
     ctx.set_shape_policy(*best)
     return {"policy": best, "table": table}

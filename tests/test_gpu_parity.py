@@ -101,7 +101,7 @@ def test_list_representation_by_size(gpu_ctx):
         j.destroy()
 
 
-@pytest.mark.parametrize("n", [300, 1500])
+@pytest.mark.parametrize("n", [300, 2500])
 def test_forces_match_oracle_both_list_modes(gpu_ctx, n):
     sp = spec(n, 21, "free")
     g, o = pair(gpu_ctx, sp)

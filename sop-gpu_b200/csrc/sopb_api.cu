@@ -94,6 +94,9 @@ struct sopb_context {
     cudaEvent_t ev_join[kSideStreams] = {};
     int32_t last_error = SOPB_OK;
     int smem_dyn_max = 1 << 30;   // dynamic shared memory available to the resident kernel
+    int smem_per_sm = 0;          // shared memory of one SM
+    int smem_reserved = 0;        // shared memory the runtime reserves per CTA
+    int smem_static[5] = {};      // static shared memory of k_resident_steps<64..1024>
     ShapePolicy policy;
 };
 
@@ -128,17 +131,33 @@ namespace {
 
 // Opt the resident kernel in to the largest dynamic shared memory the device
 // allows next to the kernel's static shared memory.
-template <int B, bool M>
-int set_smem_attr(int device, int* dyn_out) {
+template <int B>
+int set_smem_attr(int device, int* dyn_out, int* static_out) {
     int optin = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     cudaFuncAttributes fa;
-    CUDA_TRY(cudaFuncGetAttributes(&fa, k_resident_steps<B, M>));
+    CUDA_TRY(cudaFuncGetAttributes(&fa, k_resident_steps<B>));
     const int dyn = optin - (int)fa.sharedSizeBytes;
     if (dyn < kMaxResidentBeads * kResidentSmemPerBead) return SOPB_ERR_UNSUPPORTED;
-    CUDA_TRY(cudaFuncSetAttribute(k_resident_steps<B, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
+    CUDA_TRY(cudaFuncSetAttribute(k_resident_steps<B>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn));
     if (dyn < *dyn_out) *dyn_out = dyn;
+    *static_out = (int)fa.sharedSizeBytes;
     return SOPB_OK;
+}
+
+int block_index(int block) { return block == 64 ? 0 : block == 128 ? 1 : block == 256 ? 2 : block == 512 ? 3 : 4; }
+
+// Smallest float t with sqrtf(t) >= cut: for every float r2,
+// sqrtf(r2) < cut exactly when r2 < t, because a correctly rounded square
+// root is monotonic (the host's sqrtf is the IEEE operation, as the
+// device's __fsqrt_rn).  The list builders compare r^2 against t.
+float sqrt_threshold(float cut) {
+    if (!(cut > 0.0f)) return 0.0f;                         // nothing is closer than cut <= 0 (or NaN)
+    if (std::isinf(cut)) return cut;
+    float t = cut * cut;
+    while (t > 0.0f && std::sqrt(std::nextafter(t, 0.0f)) >= cut) t = std::nextafter(t, 0.0f);
+    while (std::sqrt(t) < cut) t = std::nextafter(t, INFINITY);
+    return t;
 }
 
 // Lanes per bead and CTA size of a job.  A function of the job and of the
@@ -163,37 +182,36 @@ void launch_shape(const ShapePolicy& pol, int32_t n, int32_t lpb_req, int32_t* l
     *block = b;
 }
 
-#define SOPB_BLOCK_SWITCH(block, MASK, LAUNCH)             \
-    switch (block) {                                     \
-    case 64: LAUNCH(64, MASK); break;                    \
-    case 128: LAUNCH(128, MASK); break;                  \
-    case 256: LAUNCH(256, MASK); break;                  \
-    case 512: LAUNCH(512, MASK); break;                  \
-    case 1024: LAUNCH(1024, MASK); break;                \
-    default: return SOPB_ERR_INVALID;                    \
+#define SOPB_BLOCK_SWITCH(block, LAUNCH) \
+    switch (block) {                      \
+    case 64: LAUNCH(64); break;           \
+    case 128: LAUNCH(128); break;         \
+    case 256: LAUNCH(256); break;         \
+    case 512: LAUNCH(512); break;         \
+    case 1024: LAUNCH(1024); break;       \
+    default: return SOPB_ERR_INVALID;     \
     }
 
-int launch_resident(int block, bool mask, int grid, size_t smem, cudaStream_t st, JobDev* jobs, const int32_t* ids,
+int launch_resident(int block, int grid, size_t smem, cudaStream_t st, JobDev* jobs, const int32_t* ids,
                     int64_t nsteps) {
-#define L_RES(B, M) k_resident_steps<B, M><<<grid, B, smem, st>>>(jobs, ids, nsteps)
-    if (mask) { SOPB_BLOCK_SWITCH(block, true, L_RES) } else { SOPB_BLOCK_SWITCH(block, false, L_RES) }
+#define L_RES(B) k_resident_steps<B><<<grid, B, smem, st>>>(jobs, ids, nsteps)
+    SOPB_BLOCK_SWITCH(block, L_RES)
 #undef L_RES
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
 
-int launch_forces(int block, bool mask, int grid, cudaStream_t st, const JobDev* jobs, const int32_t* ids, float4* out) {
-#define L_FRC(B, M) k_forces_only<B, M><<<grid, B, 0, st>>>(jobs, ids, out)
-    if (mask) { SOPB_BLOCK_SWITCH(block, true, L_FRC) } else { SOPB_BLOCK_SWITCH(block, false, L_FRC) }
+int launch_forces(int block, int grid, cudaStream_t st, const JobDev* jobs, const int32_t* ids, float4* out) {
+#define L_FRC(B) k_forces_only<B><<<grid, B, 0, st>>>(jobs, ids, out)
+    SOPB_BLOCK_SWITCH(block, L_FRC)
 #undef L_FRC
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
 
-int launch_rebuild(int block, bool mask, int grid, cudaStream_t st, JobDev* jobs, const int32_t* ids, int possible,
-                   int verlet) {
-#define L_REB(B, M) k_rebuild_lists<B, M><<<grid, B, 0, st>>>(jobs, ids, possible, verlet)
-    if (mask) { SOPB_BLOCK_SWITCH(block, true, L_REB) } else { SOPB_BLOCK_SWITCH(block, false, L_REB) }
+int launch_rebuild(int block, int grid, cudaStream_t st, JobDev* jobs, const int32_t* ids, int possible, int verlet) {
+#define L_REB(B) k_rebuild_lists<B><<<grid, B, 0, st>>>(jobs, ids, possible, verlet)
+    SOPB_BLOCK_SWITCH(block, L_REB)
 #undef L_REB
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
@@ -276,12 +294,13 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
     CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     int rc;
     int* dm = &c->smem_dyn_max;
-    if ((rc = set_smem_attr<64, false>(device, dm)) || (rc = set_smem_attr<64, true>(device, dm)) ||
-        (rc = set_smem_attr<128, false>(device, dm)) || (rc = set_smem_attr<256, false>(device, dm)) ||
-        (rc = set_smem_attr<512, false>(device, dm)) || (rc = set_smem_attr<1024, false>(device, dm)) ||
-        (rc = set_smem_attr<128, true>(device, dm)) || (rc = set_smem_attr<256, true>(device, dm)) ||
-        (rc = set_smem_attr<512, true>(device, dm)) || (rc = set_smem_attr<1024, true>(device, dm)))
+    int* ss = c->smem_static;
+    if ((rc = set_smem_attr<64>(device, dm, &ss[0])) || (rc = set_smem_attr<128>(device, dm, &ss[1])) ||
+        (rc = set_smem_attr<256>(device, dm, &ss[2])) || (rc = set_smem_attr<512>(device, dm, &ss[3])) ||
+        (rc = set_smem_attr<1024>(device, dm, &ss[4])))
         return rc;
+    CUDA_TRY(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    CUDA_TRY(cudaDeviceGetAttribute(&c->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
     *out = c;
     return SOPB_OK;
 }
@@ -633,6 +652,8 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.cut2 = p.pairs_cutoff * p.pairs_cutoff;
     h.pl_cut = p.pairlist_cutoff;
     h.pp_thr = p.pairs_threshold;
+    h.pl_t = sqrt_threshold(p.pairlist_cutoff);
+    h.pp_t = sqrt_threshold(p.pairs_threshold);
     h.h = p.timestep;
     h.zeta = p.zeta;
     h.hOverZeta = p.timestep / p.zeta;
@@ -865,23 +886,33 @@ namespace {
 // jobs' class first so the longest CTAs start first.
 struct LaunchClass {
     int block = 0;
-    bool mask = false;
     int32_t max_n = 0;
     size_t smem = 0;
     std::vector<int32_t> ids;
 };
-void group_jobs(sopb_job* const* jobs, int32_t njobs, std::vector<LaunchClass>& out) {
-    std::map<int, LaunchClass> cls;   // key: block * 2 + mask
+// CTAs of a job's resident launch that fit one SM: 1024 threads' worth of
+// registers (the kernel's launch bound) and the SM's shared memory.
+int ctas_per_sm(const sopb_context* c, int block, size_t smem) {
+    const int by_regs = 1024 / block;
+    const size_t per_cta = smem + (size_t)c->smem_static[block_index(block)] + (size_t)c->smem_reserved;
+    const int by_smem = (int)((size_t)c->smem_per_sm / per_cta);
+    return std::max(1, std::min(by_regs, by_smem));
+}
+// Jobs of one class share a CTA size and the number of CTAs an SM holds, so
+// the class's largest shared-memory request never lowers the residency of
+// its smaller jobs.
+void group_jobs(const sopb_context* c, sopb_job* const* jobs, int32_t njobs, std::vector<LaunchClass>& out) {
+    std::map<int, LaunchClass> cls;   // key: block * 64 + CTAs per SM
     std::vector<int32_t> order(njobs);
     for (int32_t k = 0; k < njobs; ++k) order[k] = k;
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return jobs[a]->n > jobs[b]->n; });
     for (int32_t k : order) {
         const JobDev& h = jobs[k]->h;
-        LaunchClass& L = cls[h.block * 2 + h.mask];
+        const size_t smem = resident_smem_bytes(jobs[k]->n, h.lcache);
+        LaunchClass& L = cls[h.block * 64 + ctas_per_sm(c, h.block, smem)];
         L.block = h.block;
-        L.mask = h.mask != 0;
         L.max_n = std::max(L.max_n, jobs[k]->n);
-        L.smem = std::max(L.smem, resident_smem_bytes(jobs[k]->n, h.lcache));
+        L.smem = std::max(L.smem, smem);
         L.ids.push_back(jobs[k]->slot);
     }
     out.clear();
@@ -916,7 +947,7 @@ extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, i
         return SOPB_OK;
     }
     std::vector<LaunchClass> cls;
-    group_jobs(jobs, njobs, cls);
+    group_jobs(c, jobs, njobs, cls);
     std::vector<int32_t> ids;
     std::vector<size_t> off;
     for (auto& L : cls) {
@@ -928,13 +959,13 @@ extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, i
     CUDA_TRY(cudaMemcpyAsync(c->d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->stream));
     if (cls.size() == 1) {
         const LaunchClass& L = cls[0];
-        return launch_resident(L.block, L.mask, (int)L.ids.size(), L.smem, c->stream, c->d_jobs, c->d_ids, nsteps);
+        return launch_resident(L.block, (int)L.ids.size(), L.smem, c->stream, c->d_jobs, c->d_ids, nsteps);
     }
     CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
     for (size_t k = 0; k < cls.size(); ++k) {
         cudaStream_t s = c->side[k % kSideStreams];
         CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
-        rc = launch_resident(cls[k].block, cls[k].mask, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs,
+        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs,
                              c->d_ids + off[k], nsteps);
         if (rc) return rc;
     }
@@ -1001,7 +1032,7 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         if (rc) return rc;
         const int32_t id = j->slot;
         CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
-        rc = launch_forces(j->h.block, j->h.mask != 0, 1, c->stream, c->d_jobs, c->d_ids, c->d_scratch4);
+        rc = launch_forces(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, c->d_scratch4);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(out, c->d_scratch4, n * 16, cudaMemcpyDeviceToHost, c->stream));
         break;
@@ -1115,7 +1146,7 @@ extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t ver
     if (rc) return rc;
     const int32_t id = j->slot;
     CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
-    rc = launch_rebuild(j->h.block, j->h.mask != 0, 1, c->stream, c->d_jobs, c->d_ids, possible, verlet);
+    rc = launch_rebuild(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, possible, verlet);
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return SOPB_OK;

@@ -67,6 +67,7 @@ struct JobDev {
     float a2, m6, cut2;   // repulsive: a^2, -6 el / a^2, pairs_cutoff^2
     float pl_cut;         // pairlist_cutoff
     float pp_thr;         // pairs_threshold
+    float pl_t, pp_t;     // r^2 thresholds equivalent to sqrt(r^2) < pl_cut, < pp_thr
     // ---- integrator ------------------------------------------------------------
     float hOverZeta, tempNorm, var, zeta, h;
     int32_t minimization, heating;
@@ -128,15 +129,17 @@ __device__ __forceinline__ float4 gaussian4(uint4& s) {
     return g;
 }
 
-// Distance test used by both list builders, in IEEE round-to-nearest with no
-// contraction: sqrt(dx*dx + dy*dy + dz*dz) < cut, the reference's test
-// (possiblepairlist_kernel.cu:45-46, pairlist_kernel.cu:57-63) evaluated
-// exactly as the CPU oracle evaluates it, so list membership is bit-exact.
-__device__ __forceinline__ bool within_cutoff(float4 xi, float4 xj, float cut) {
-    float dx = __fsub_rn(xj.x, xi.x), dy = __fsub_rn(xj.y, xi.y), dz = __fsub_rn(xj.z, xi.z);
-    float r2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-    return __fsqrt_rn(r2) < cut;
+// List membership test sqrt(r^2) < cut of the reference
+// (possiblepairlist_kernel.cu:45-46, pairlist_cutoff in pairlist_kernel.cu:57-63),
+// with r^2 formed exactly as the CPU oracle forms it.  Because a correctly
+// rounded square root is monotonic, sqrt(r^2) < cut holds exactly when
+// r^2 < t for the threshold t = sqrt_threshold(cut) computed on the host,
+// so the test needs no square root and list membership stays bit-exact.
+__device__ __forceinline__ float dist2_rn(float4 xi, float4 xj) {
+    const float dx = __fsub_rn(xj.x, xi.x), dy = __fsub_rn(xj.y, xi.y), dz = __fsub_rn(xj.z, xi.z);
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
 }
+__device__ __forceinline__ bool within_cutoff(float4 xi, float4 xj, float t) { return dist2_rn(xi, xj) < t; }
 
 // FENE term (covalent_kernel.cu:28-51): Ks*(r-r0)/(r*(1-(r-r0)^2/R0^2)).
 // r - r0 cancels for a near-relaxed bond, so r is formed with a correctly

@@ -214,7 +214,7 @@ k_g_possible_brute(JobDev* __restrict__ Jp, int force) {
         const int c0 = J.cov_off[i], c1 = J.cov_off[i + 1], n0 = J.nat_off[i], n1 = J.nat_off[i + 1];
         for (int qb = 0; qb < n; qb += lpb) {
             const int q = qb + l;
-            bool ok = q < n && q != i && within_cutoff(xi, J.x[q < n ? q : 0], J.pp_thr);
+            bool ok = q < n && q != i && within_cutoff(xi, J.x[q < n ? q : 0], J.pp_t);
             if (ok) {
                 for (int k = c0; k < c1 && ok; ++k) ok = J.cov_j[k] != q;
                 for (int k = n0; k < n1 && ok; ++k) ok = J.nat_j[k] != q;
@@ -398,7 +398,7 @@ k_cl_possible(JobDev* __restrict__ Jp, GridAux aux, int force) {
                         bool ok = false;
                         if (k < s1) {
                             q = aux.cell_beads[k];
-                            ok = q != i && within_cutoff(xi, J.x[q], J.pp_thr);
+                            ok = q != i && within_cutoff(xi, J.x[q], J.pp_t);
                             for (int t = c0; t < c1 && ok; ++t) ok = J.cov_j[t] != q;
                             for (int t = n0; t < n1 && ok; ++t) ok = J.nat_j[t] != q;
                         }
@@ -487,7 +487,7 @@ k_g_verlet(JobDev* __restrict__ Jp, int force) {
             bool ok = k < npp;
             if (ok) {
                 q = prow[k];
-                ok = within_cutoff(xi, J.x[q], J.pl_cut);
+                ok = within_cutoff(xi, J.x[q], J.pl_t);
             }
             const unsigned m = __ballot_sync(0xffffffffu, ok);
             if (ok) {

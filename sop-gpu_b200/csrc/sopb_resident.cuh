@@ -9,15 +9,14 @@
 // and copies all coordinates to the host every `stride` steps for pulling,
 // src/Potentials/pulling.cu:152-165).
 //
-// Neighbour lists.  The Verlet list of every job is a set of bead-major,
-// order-preserving index rows in global memory (the reference's slot-major
-// d_pairs transposed), cached in shared memory as a compact CSR copy of u16
-// indices whenever the whole list fits the job's cache; the possible-pairs
-// list is, per job,
-//   MASK  (n <= ~1100): a bitmask over the job's beads, with bonded/native
-//         exclusions as a precomputed bitmask;
-//   ROWS  (larger jobs): index rows like the Verlet list.
-// Partners are always visited in increasing j, the reference's list order.
+// Neighbour lists.  The possible-pairs list of a job is a bitmask over its
+// beads (n <= 2048, so at most 64 words a row), with bonded/native
+// exclusions as a precomputed bitmask.  The Verlet list is a set of
+// bead-major, order-preserving index rows in global memory (the reference's
+// slot-major d_pairs transposed), cached in shared memory as a compact CSR
+// copy of u16 indices whenever the whole list fits the job's cache.  Both
+// are rebuilt a warp per bead with ballots, so partners are always visited
+// in increasing j, the reference's list order.
 //
 // One step is two phases.  Forces: a group of `lpb` lanes (a power of two
 // <= 32, a whole warp by default) takes beads from a shared counter, strides
@@ -89,140 +88,89 @@ __device__ __forceinline__ void bonded_partial(const JobDev& J, const float4* __
     for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[__ldg(&J.nat_j[k])], __ldg(&J.nat_par[k]), f);
 }
 
-// Verlet-pair terms of bead i, lane l of lpb taking entries l, l+lpb, ...,
-// from the shared-memory cache when the list fits it, else from the rows.
+// Verlet-pair terms of bead i, lane l of lpb taking entries l, l+lpb, ...
+// in that order, from the shared-memory cache when the list fits it, else
+// from the rows.  Two entries are fetched per iteration so two gathers are
+// in flight; the per-lane summation order is unchanged.
+template <typename Idx>
+__device__ __forceinline__ void pair_run(const JobDev& J, const float4* __restrict__ xs, const Idx* __restrict__ r,
+                                         int cnt, float4 xi, int l, int lpb, float3& f) {
+    int k = l;
+    for (; k + lpb < cnt; k += 2 * lpb) {
+        const int j0 = r[k], j1 = r[k + lpb];
+        const float4 x0 = xs[j0], x1 = xs[j1];
+        pair_term(xi, x0, J.a2, J.m6, J.cut2, f);
+        pair_term(xi, x1, J.a2, J.m6, J.cut2, f);
+    }
+    if (k < cnt) pair_term(xi, xs[r[k]], J.a2, J.m6, J.cut2, f);
+}
+
 __device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const int32_t* off,
                                               const uint16_t* nbr, bool cached, int i, float4 xi, int l, int lpb,
                                               float3& f) {
     if (cached) {
-        const int k0 = off[i], cnt = off[i + 1] - k0;
-        const uint16_t* r = nbr + k0;
-        for (int k = l; k < cnt; k += lpb) pair_term(xi, xs[r[k]], J.a2, J.m6, J.cut2, f);
+        const int k0 = off[i];
+        pair_run(J, xs, nbr + k0, off[i + 1] - k0, xi, l, lpb, f);
     } else {
-        const int cnt = J.pl_cnt[i];
-        const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
-        for (int k = l; k < cnt; k += lpb) pair_term(xi, xs[r[k]], J.a2, J.m6, J.cut2, f);
+        pair_run(J, xs, J.pl_j + (size_t)i * J.cap_pl, J.pl_cnt[i], xi, l, lpb, f);
     }
 }
 
 // generate_possiblepairs (src/Updaters/possiblepairlist_kernel.cu:18-71):
 // every q of the job with |r| < pairs_threshold that is neither i nor a
-// covalent or native partner.  More than max_possiblePairs sets err (the
-// reference writes past its rows there).
-template <int BLOCK, bool MASK>
+// covalent or native partner, as a bitmask row.  A warp takes one bead;
+// lane b tests bead 32w+b of word w and a ballot forms the word.  More than
+// max_possiblePairs sets err (the reference writes past its rows there).
+template <int BLOCK>
 __device__ void build_possible(const JobDev& J, const float4* __restrict__ xs, int& err) {
-    const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
-    const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
-    for (int base = 0; base < n; base += ng) {
-        const int i = base + g;
-        const bool act = i < n;
-        const float4 xi = xs[act ? i : 0];
+    const int n = J.n, W = J.W, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x >> 5; i < n; i += BLOCK / 32) {
+        const float4 xi = xs[i];
+        const uint32_t* ex = J.ex_mask + (size_t)i * W;
+        uint32_t* row = J.pp_mask + (size_t)i * W;
         int cnt = 0;
-        if (MASK) {
-            if (act) {
-                for (int w = l; w < J.W; w += lpb) {
-                    uint32_t bits = 0;
-                    const int q0 = 32 * w;
-                    const int qn = min(32, n - q0);
-                    for (int b = 0; b < qn; ++b)
-                        if (within_cutoff(xi, xs[q0 + b], J.pp_thr)) bits |= 1u << b;
-                    bits &= ~__ldg(&J.ex_mask[(size_t)i * J.W + w]);
-                    J.pp_mask[(size_t)i * J.W + w] = bits;
-                    cnt += __popc(bits);
-                }
-            }
-            cnt = group_sum(cnt, lpb);
-            if (act && l == 0 && cnt > J.max_pp) err = SOPB_STATUS_CAPACITY;
-        } else {
-            const int gbase = (tid & 31) & ~(lpb - 1);
-            const unsigned gm = group_mask(lpb);
-            int32_t* row = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
-            const uint32_t* ex = J.ex_mask ? J.ex_mask + (size_t)(act ? i : 0) * J.W : nullptr;
-            for (int qb = 0; qb < n; qb += lpb) {
-                const int q = qb + l;
-                bool ok = act && q < n && within_cutoff(xi, xs[q < n ? q : 0], J.pp_thr);
-                if (ok) ok = !((__ldg(&ex[q >> 5]) >> (q & 31)) & 1u);
-                const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
-                if (ok) {
-                    const int pos = cnt + __popc(m & ((1u << l) - 1u));
-                    if (pos < J.cap_pp) row[pos] = q;
-                    else err = SOPB_STATUS_CAPACITY;
-                }
-                cnt += __popc(m);
-            }
-            if (act && l == 0) J.pp_cnt[i] = cnt < J.cap_pp ? cnt : J.cap_pp;
+        for (int w = 0; w < W; ++w) {
+            const int q = 32 * w + lane;
+            const bool ok = q < n && within_cutoff(xi, xs[q < n ? q : 0], J.pp_t);
+            const uint32_t bits = __ballot_sync(0xffffffffu, ok) & ~__ldg(&ex[w]);
+            if (lane == 0) row[w] = bits;
+            cnt += __popc(bits);
         }
+        if (lane == 0 && cnt > J.max_pp) err = SOPB_STATUS_CAPACITY;
     }
 }
 
 // generate_pairs (src/Updaters/pairlist_kernel.cu:33-76): the possible pairs
-// with |r| < pairlist_cutoff, order kept.  More than max_pairs sets err.
-template <int BLOCK, bool MASK>
+// with |r| < pairlist_cutoff, in increasing j (the reference's order), as
+// index rows.  A warp takes one bead: the possible-pairs words are held two
+// per lane (W <= 64), lane b tests candidate 32w+b and a ballot places the
+// hits.  A row longer than its capacity sets err.
+template <int BLOCK>
 __device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int& err) {
-    const int n = J.n, lpb = J.lpb, tid = threadIdx.x;
-    const int g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
-    for (int base = 0; base < n; base += ng) {
-        const int i = base + g;
-        const bool act = i < n;
-        const float4 xi = xs[act ? i : 0];
+    static_assert(kMaxResidentBeads <= 64 * 32, "two mask words per lane");
+    const int n = J.n, W = J.W, lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    for (int i = threadIdx.x >> 5; i < n; i += BLOCK / 32) {
+        const float4 xi = xs[i];
+        const uint32_t* pm = J.pp_mask + (size_t)i * W;
+        const uint32_t m0 = lane < W ? pm[lane] : 0u;
+        const uint32_t m1 = lane + 32 < W ? pm[lane + 32] : 0u;
+        int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
         int cnt = 0;
-        if (MASK) {
-            // words in order, lpb at a time; lanes' bits placed by an
-            // exclusive scan of their counts, so the row stays in increasing j
-            int32_t* row = J.pl_j + (size_t)(act ? i : 0) * J.cap_pl;
-            for (int wb = 0; wb < J.W; wb += lpb) {
-                const int w = wb + l;
-                uint32_t out = 0;
-                if (act && w < J.W) {
-                    uint32_t m = J.pp_mask[(size_t)i * J.W + w];
-                    while (m) {
-                        const int b = __ffs(m) - 1;
-                        m &= m - 1;
-                        if (within_cutoff(xi, xs[32 * w + b], J.pl_cut)) out |= 1u << b;
-                    }
-                }
-                const int c = __popc(out);
-                int incl = c;
-                for (int o = 1; o < lpb; o <<= 1) {
-                    const int t = __shfl_up_sync(0xffffffffu, incl, o, lpb);
-                    if (l >= o) incl += t;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, lpb - 1, lpb);
-                int pos = cnt + incl - c;
-                while (out) {
-                    const int b = __ffs(out) - 1;
-                    out &= out - 1;
-                    if (pos < J.cap_pl) row[pos] = 32 * w + b;
-                    else err = SOPB_STATUS_CAPACITY;
-                    ++pos;
-                }
-                cnt += total;
+        for (int w = 0; w < W; ++w) {
+            const uint32_t m = __shfl_sync(0xffffffffu, w < 32 ? m0 : m1, w & 31);
+            const int q = 32 * w + lane;
+            const bool ok = ((m >> lane) & 1u) && q < n && within_cutoff(xi, xs[q], J.pl_t);
+            const uint32_t hit = __ballot_sync(0xffffffffu, ok);
+            if (ok) {
+                const int pos = cnt + __popc(hit & below);
+                if (pos < J.cap_pl) row[pos] = q;
             }
-            if (act && l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
-        } else {
-            const int gbase = (tid & 31) & ~(lpb - 1);
-            const unsigned gm = group_mask(lpb);
-            const int npp = act ? J.pp_cnt[i] : 0;
-            const int32_t* prow = J.pp_j + (size_t)(act ? i : 0) * J.cap_pp;
-            int32_t* row = J.pl_j + (size_t)(act ? i : 0) * J.cap_pl;
-            const int kmax = __reduce_max_sync(0xffffffffu, npp);
-            for (int kb = 0; kb < kmax; kb += lpb) {
-                const int k = kb + l;
-                int q = 0;
-                bool ok = k < npp;
-                if (ok) {
-                    q = prow[k];
-                    ok = within_cutoff(xi, xs[q], J.pl_cut);
-                }
-                const unsigned m = (__ballot_sync(0xffffffffu, ok) >> gbase) & gm;
-                if (ok) {
-                    const int pos = cnt + __popc(m & ((1u << l) - 1u));
-                    if (pos < J.cap_pl) row[pos] = q;
-                    else err = SOPB_STATUS_CAPACITY;
-                }
-                cnt += __popc(m);
-            }
-            if (act && l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
+            cnt += __popc(hit);
+        }
+        if (lane == 0) {
+            if (cnt > J.cap_pl) err = SOPB_STATUS_CAPACITY;
+            J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
         }
     }
 }
@@ -302,11 +250,22 @@ __device__ int fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap,
     __syncthreads();
     const int fits = *tot_smem <= cap;
     if (fits) {
-        const int lpb = J.lpb, g = tid / lpb, l = tid % lpb, ng = BLOCK / lpb;
-        for (int i = g; i < n; i += ng) {
+        for (int i = w; i < n; i += BLOCK / 32) {
             const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
             const int k0 = off[i], cnt = off[i + 1] - k0;
-            for (int k = l; k < cnt; k += lpb) nbr[k0 + k] = (uint16_t)r[k];
+            for (int kb = 0; kb < cnt; kb += 128) {
+                int v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = kb + 32 * u + lane;
+                    v[u] = k < cnt ? r[k] : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int k = kb + 32 * u + lane;
+                    if (k < cnt) nbr[k0 + k] = (uint16_t)v[u];
+                }
+            }
         }
     }
     __syncthreads();
@@ -316,7 +275,7 @@ __device__ int fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap,
 // The updaters of one `stride` boundary in the reference order
 // (creation order in src/gsop.cu:80-101; loop in src/gsop.cu:129-133).
 // Returns 1 when the Verlet list was rebuilt.
-template <int BLOCK, bool MASK>
+template <int BLOCK>
 __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, float* Ts,
                                          float (*red)[4], int64_t step, int& err) {
     const int tid = threadIdx.x, n = J.n;
@@ -342,13 +301,13 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
         for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
     }
     const bool pp = step % J.pp_freq == 0;
-    if (pp) build_possible<BLOCK, MASK>(J, xs, err);
+    if (pp) build_possible<BLOCK>(J, xs, err);
     if (step % J.nav == 0)
         for (int i = tid; i < n; i += BLOCK) Ts[i] = 0.0f;   // output_manager.cu:125-127
     const bool verlet = step % J.pairs_freq == 0;
     if (verlet) {
         if (pp) __syncthreads();
-        build_verlet<BLOCK, MASK>(J, xs, err);
+        build_verlet<BLOCK>(J, xs, err);
     }
     if (J.heating && tid == 0 && step % J.temp_freq == 0) {
         // TemperatureUpdater (src/Integrators/langevin.cu:129-135, 44-48)
@@ -365,7 +324,7 @@ __host__ __device__ inline size_t resident_smem_bytes(int n, int cache_entries) 
 }
 
 // Register cap of 64 per thread: 1024 threads of resident CTAs per SM.
-template <int BLOCK, bool MASK>
+template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
 k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int64_t nsteps) {
     JobDev* Jp = &jobs[ids[blockIdx.x]];
@@ -421,7 +380,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     if (tid < 2) next_bead[tid] = 0;
     __syncthreads();
     for (int64_t s = 0; s < nsteps; ++s, ++step) {
-        if (phase == 0 && run_updaters<BLOCK, MASK>(J, sc, xc, Ts, red, step, err))
+        if (phase == 0 && run_updaters<BLOCK>(J, sc, xc, Ts, red, step, err))
             cached = fill_cache<BLOCK>(J, off, nbr, J.lcache, &list_total);
         if (++phase == J.stride) phase = 0;
         int* counter = &next_bead[s & 1];
@@ -505,7 +464,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
 // Potential forces only (SOPPotential::compute of every potential, no
 // integrator) at the job's current coordinates and Verlet rows, with the
 // step kernel's lane split; does not touch the tip accumulator.
-template <int BLOCK, bool MASK>
+template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, float4* __restrict__ out) {
     __shared__ JobDev Js;
@@ -537,7 +496,7 @@ k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, 
 }
 
 // Rebuilds the possible-pairs and/or Verlet lists now, without the step gate.
-template <int BLOCK, bool MASK>
+template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1)
 k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int possible, int verlet) {
     JobDev* Jp = &jobs[ids[blockIdx.x]];
@@ -548,9 +507,9 @@ k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int 
     if (threadIdx.x == 0) errs = 0;
     __syncthreads();
     int err = 0;
-    if (possible) build_possible<BLOCK, MASK>(J, J.x, err);
+    if (possible) build_possible<BLOCK>(J, J.x, err);
     __syncthreads();
-    if (verlet) build_verlet<BLOCK, MASK>(J, J.x, err);
+    if (verlet) build_verlet<BLOCK>(J, J.x, err);
     if (err) atomicMax(&errs, err);
     __syncthreads();
     if (threadIdx.x == 0 && errs) Jp->status = errs;

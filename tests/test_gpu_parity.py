@@ -67,6 +67,35 @@ def test_lists_bit_exact_at_exact_cutoff_ties(gpu_ctx):
     g.destroy()
 
 
+@pytest.mark.parametrize("cut", [20.0, 13.7, 7.3])
+def test_lists_bit_exact_within_ulps_of_the_cutoff(gpu_ctx, cut):
+    # isolated pairs whose separation is the cutoff give or take a few ulps,
+    # in random directions: the squared-distance threshold must classify
+    # every one as sqrt(r^2) < cut does
+    rng = np.random.default_rng(int(cut * 10))
+    npair = 256
+    u = rng.normal(size=(npair, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    d = np.float32(cut) * (1.0 + rng.integers(-6, 7, npair) * 6e-8)
+    base = np.zeros((npair, 3))
+    base[:, 0] = np.arange(npair) * 4.0 * cut
+    xi = base.astype(np.float32)
+    xj = (base + d[:, None] * u).astype(np.float32)
+    pts = np.empty((2 * npair, 3), np.float32)
+    pts[0::2], pts[1::2] = xi, xj
+    p = sopb.default_params(timestep=0.08, pairs_threshold=cut, pairlist_cutoff=cut, pairs_freq=10)
+    sp = sopb.JobSpec(pts, np.zeros((0, 2)), [], np.zeros((0, 2)), [], [], p, seed=3)
+    g, o = pair(gpu_ctx, sp)
+    g.rebuild(True, True)
+    o.rebuild(True, True)
+    for possible in (True, False):
+        cg, rg = g.pairlist(possible)
+        co, ro = o.pairlist(possible)
+        assert np.array_equal(cg, co) and np.array_equal(rg, ro)
+    assert 0 < cg.sum() < 2 * npair           # both sides of the cutoff occur
+    g.destroy()
+
+
 @pytest.mark.parametrize("lpb", [1, 2, 4, 8, 32])
 @pytest.mark.parametrize("mode", ["free", "indent"])
 def test_forces_match_oracle(gpu_ctx, lpb, mode):

@@ -647,8 +647,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     // force field constants as the reference hosts compute them
     h.ks = p.kspring_cov;
     h.R2 = p.R_limit * p.R_limit;
-    h.a2 = p.a * p.a;
-    h.m6 = -6.0f * p.el / h.a2;
+    h.c8 = (float)(-6.0 * (double)p.el * std::pow((double)p.a, 6.0));
     h.cut2 = p.pairs_cutoff * p.pairs_cutoff;
     h.pl_cut = p.pairlist_cutoff;
     h.pp_thr = p.pairs_threshold;
@@ -741,9 +740,13 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     }
     h.W = (n + 31) / 32;
     h.mask = h.grid ? 0 : 1;
+    h.ncov = m.cov_off[n];
+    h.nnat = m.nat_off[n];
     if (!h.grid) {
-        // shared-memory cache of the Verlet list: the list at the initial
-        // coordinates plus 15% and 8 entries per bead, as far as it fits
+        // bonded maps in shared memory when they fit beside the per-bead
+        // state; then a cache of the Verlet list: the list at the initial
+        // coordinates plus 10% and 4 entries per bead, as far as it fits
+        h.bsm = resident_layout(n, h.ncov, h.nnat, 1, 0).total <= (size_t)c->smem_dyn_max ? 1 : 0;
         const float cut = std::min(p.pairlist_cutoff, p.pairs_threshold);
         std::vector<uint8_t> bonded((size_t)n * n, 0);
         for (int32_t i = 0; i < n; ++i) {
@@ -757,9 +760,10 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
                             dz = d->xyz[3 * q + 2] - d->xyz[3 * i + 2];
                 if (!bonded[(size_t)i * n + q] && std::sqrt(dx * dx + dy * dy + dz * dz) < cut) total += 2;
             }
-        int64_t want = (int64_t)std::ceil(1.15 * (double)total) + 8 * (int64_t)n;
+        int64_t want = (int64_t)std::ceil(1.10 * (double)total) + 4 * (int64_t)n;
         want = std::min<int64_t>(want, (int64_t)n * h.cap_pl);
-        const int64_t fit = ((int64_t)c->smem_dyn_max - (int64_t)resident_smem_bytes(n, 0)) / 2;
+        const int64_t fit =
+            ((int64_t)c->smem_dyn_max - (int64_t)resident_layout(n, h.ncov, h.nnat, h.bsm, 0).total - 16) / 2;
         h.lcache = (int32_t)std::max<int64_t>(0, std::min(want, fit));
     }
     if (h.grid) {
@@ -908,7 +912,7 @@ void group_jobs(const sopb_context* c, sopb_job* const* jobs, int32_t njobs, std
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return jobs[a]->n > jobs[b]->n; });
     for (int32_t k : order) {
         const JobDev& h = jobs[k]->h;
-        const size_t smem = resident_smem_bytes(jobs[k]->n, h.lcache);
+        const size_t smem = resident_smem_bytes(h);
         LaunchClass& L = cls[h.block * 64 + ctas_per_sm(c, h.block, smem)];
         L.block = h.block;
         L.max_n = std::max(L.max_n, jobs[k]->n);

@@ -33,6 +33,8 @@ struct JobDev {
     int32_t max_pl;       // configured max_pairs
     int32_t grid;         // 1: grid path (per-step kernels, CUDA graphs)
     int32_t lcache;       // shared-memory cache of the Verlet list, entries
+    int32_t bsm;          // 1: bonded maps copied to shared memory for a launch
+    int32_t ncov, nnat;   // covalent / native map entries (both directions)
     int32_t stride;       // updater period (gsop.cu:117-122)
     int32_t nav;
     int32_t pairs_freq;
@@ -64,7 +66,7 @@ struct JobDev {
     uint32_t* pp_mask;    // [n * W] possible pairs (MASK mode)
     // ---- force field ---------------------------------------------------------
     float ks, R2;         // FENE: kspring_cov, R_limit^2
-    float a2, m6, cut2;   // repulsive: a^2, -6 el / a^2, pairs_cutoff^2
+    float c8, cut2;       // repulsive: -6 el a^6, pairs_cutoff^2
     float pl_cut;         // pairlist_cutoff
     float pp_thr;         // pairs_threshold
     float pl_t, pp_t;     // r^2 thresholds equivalent to sqrt(r^2) < pl_cut, < pp_thr
@@ -163,18 +165,19 @@ __device__ __forceinline__ void native_term(float4 xi, float4 xj, float2 par, fl
     f.y += dy * w;
     f.z += dz * w;
 }
-// Repulsive r^-6 term with the force cutoff (pairs_kernel.cu:33-59).
-__device__ __forceinline__ void pair_term(float4 xi, float4 xj, float a2, float m6, float cut2, float3& f) {
-    float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-    float w = dx * dx + dy * dy + dz * dz;
-    if (w < cut2) {
-        w = a2 / w;
-        w = w * w;
-        w = m6 * w * w;
-        f.x += dx * w;
-        f.y += dy * w;
-        f.z += dz * w;
-    }
+// Repulsive r^-6 term with the force cutoff (pairs_kernel.cu:33-59): the
+// force on i is r_ij * (-6 el a^6 / r^8), formed as c8 * (1/r^2)^4 with
+// c8 = -6 el a^6 precomputed, and zero beyond pairs_cutoff.
+__device__ __forceinline__ void pair_term(float4 xi, float4 xj, float c8, float cut2, float3& f) {
+    const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    float w = 1.0f / r2;
+    w = w * w;
+    w = c8 * (w * w);
+    w = r2 < cut2 ? w : 0.0f;
+    f.x += dx * w;
+    f.y += dy * w;
+    f.z += dz * w;
 }
 
 // Tip and continuous-surface terms (indentation_kernel.cu:71-128).  Returns

@@ -75,8 +75,8 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
         const float4 xi = J.x[act ? i : 0];
         float3 f = make_float3(0.f, 0.f, 0.f);
         if (act) {
-            bonded_partial(J, J.x, i, xi, l, lpb, f);
-            pairs_partial(J, J.x, nullptr, nullptr, false, i, xi, l, lpb, f);
+            bonded_partial(J, global_bonded(J), J.x, i, xi, l, lpb, f);
+            pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {

@@ -32,9 +32,48 @@
 namespace sopb {
 
 constexpr int kMaxResidentBeads = 2048;
-// shared memory per bead: coordinates x2, RNG state, force (16 B each),
-// temperature and the cache's row offset (4 B each)
-constexpr int kResidentSmemPerBead = 72;
+// shared memory per bead that every resident job holds: coordinates, RNG
+// state and force (16 B each), temperature and the cache's row offset
+// (4 B each), pulling flag (1 B)
+constexpr int kResidentSmemPerBead = 57;
+
+// Shared-memory layout of a resident launch (byte offsets, 16-B aligned
+// arrays).  The bonded maps (covalent and native CSR with parameters) are
+// copied in when `bonded` is set; the Verlet cache takes `cache` u16 entries.
+struct ResidentLayout {
+    size_t x, F, sd, nat_par, Ts, off, cov_off, nat_off, cov_r0, cov_j, nat_j, flags, nbr, total;
+};
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+__host__ __device__ inline ResidentLayout resident_layout(int n, int ncov, int nnat, int bonded, int cache) {
+    ResidentLayout L;
+    const size_t b = bonded ? 1 : 0;
+    size_t o = 0;
+    L.x = o;        o = align16(o + (size_t)n * 16);
+    L.F = o;        o = align16(o + (size_t)n * 16);
+    L.sd = o;       o = align16(o + (size_t)n * 16);
+    L.nat_par = o;  o = align16(o + b * (size_t)nnat * 8);
+    L.Ts = o;       o = align16(o + (size_t)n * 4);
+    L.off = o;      o = align16(o + (size_t)(n + 4) * 4);
+    L.cov_off = o;  o = align16(o + b * (size_t)(n + 1) * 4);
+    L.nat_off = o;  o = align16(o + b * (size_t)(n + 1) * 4);
+    L.cov_r0 = o;   o = align16(o + b * (size_t)ncov * 4);
+    L.cov_j = o;    o = align16(o + b * (size_t)ncov * 4);
+    L.nat_j = o;    o = align16(o + b * (size_t)nnat * 4);
+    L.flags = o;    o = align16(o + (size_t)n);
+    L.nbr = o;      o = align16(o + (size_t)cache * 2);
+    L.total = o;
+    return L;
+}
+
+// Where a job's covalent and native maps are read from during a launch.
+struct BondedView {
+    const int32_t* cov_off;
+    const int32_t* cov_j;
+    const float* cov_r0;
+    const int32_t* nat_off;
+    const int32_t* nat_j;
+    const float2* nat_par;
+};
 
 struct StepScalars {
     float var;
@@ -80,37 +119,45 @@ __device__ __forceinline__ int group_sum(int v, int lpb) {
 // Covalent then native terms of bead i, strided over the group's lanes
 // (the reference sums its kernels' contributions in this order,
 // src/gsop.cu:80-85).  The maps are read-only for a launch.
-__device__ __forceinline__ void bonded_partial(const JobDev& J, const float4* __restrict__ xs, int i, float4 xi, int l,
-                                               int lpb, float3& f) {
-    const int c0 = __ldg(&J.cov_off[i]), c1 = __ldg(&J.cov_off[i + 1]);
-    for (int k = c0 + l; k < c1; k += lpb) fene_term(xi, xs[__ldg(&J.cov_j[k])], __ldg(&J.cov_r0[k]), J.ks, J.R2, f);
-    const int n0 = __ldg(&J.nat_off[i]), n1 = __ldg(&J.nat_off[i + 1]);
-    for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[__ldg(&J.nat_j[k])], __ldg(&J.nat_par[k]), f);
+__device__ __forceinline__ void bonded_partial(const JobDev& J, const BondedView& B, const float4* __restrict__ xs,
+                                               int i, float4 xi, int l, int lpb, float3& f) {
+    const int c0 = B.cov_off[i], c1 = B.cov_off[i + 1];
+    const int n0 = B.nat_off[i], n1 = B.nat_off[i + 1];
+    for (int k = c0 + l; k < c1; k += lpb) fene_term(xi, xs[B.cov_j[k]], B.cov_r0[k], J.ks, J.R2, f);
+    for (int k = n0 + l; k < n1; k += lpb) native_term(xi, xs[B.nat_j[k]], B.nat_par[k], f);
+}
+
+__device__ __forceinline__ BondedView global_bonded(const JobDev& J) {
+    return BondedView{J.cov_off, J.cov_j, J.cov_r0, J.nat_off, J.nat_j, J.nat_par};
 }
 
 // Verlet-pair terms of bead i, lane l of lpb taking entries l, l+lpb, ...
 // in that order, from the shared-memory cache when the list fits it, else
-// from the rows.  Two entries are fetched per iteration so two gathers are
+// from the rows.  Four entries are fetched per iteration so four gathers are
 // in flight; the per-lane summation order is unchanged.
 template <typename Idx>
 __device__ __forceinline__ void pair_run(const JobDev& J, const float4* __restrict__ xs, const Idx* __restrict__ r,
                                          int cnt, float4 xi, int l, int lpb, float3& f) {
+    const float c8 = J.c8, cut2 = J.cut2;
     int k = l;
-    for (; k + lpb < cnt; k += 2 * lpb) {
-        const int j0 = r[k], j1 = r[k + lpb];
-        const float4 x0 = xs[j0], x1 = xs[j1];
-        pair_term(xi, x0, J.a2, J.m6, J.cut2, f);
-        pair_term(xi, x1, J.a2, J.m6, J.cut2, f);
+    for (; k + 3 * lpb < cnt; k += 4 * lpb) {
+        const int j0 = r[k], j1 = r[k + lpb], j2 = r[k + 2 * lpb], j3 = r[k + 3 * lpb];
+        const float4 x0 = xs[j0], x1 = xs[j1], x2 = xs[j2], x3 = xs[j3];
+        pair_term(xi, x0, c8, cut2, f);
+        pair_term(xi, x1, c8, cut2, f);
+        pair_term(xi, x2, c8, cut2, f);
+        pair_term(xi, x3, c8, cut2, f);
     }
-    if (k < cnt) pair_term(xi, xs[r[k]], J.a2, J.m6, J.cut2, f);
+    for (; k < cnt; k += lpb) pair_term(xi, xs[r[k]], c8, cut2, f);
 }
 
 __device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const int32_t* off,
-                                              const uint16_t* nbr, bool cached, int i, float4 xi, int l, int lpb,
+                                              const uint16_t* nbr, int cap, int i, float4 xi, int l, int lpb,
                                               float3& f) {
-    if (cached) {
+    const int k1 = off ? off[i + 1] : 0x7fffffff;
+    if (k1 <= cap) {
         const int k0 = off[i];
-        pair_run(J, xs, nbr + k0, off[i + 1] - k0, xi, l, lpb, f);
+        pair_run(J, xs, nbr + k0, k1 - k0, xi, l, lpb, f);
     } else {
         pair_run(J, xs, J.pl_j + (size_t)i * J.cap_pl, J.pl_cnt[i], xi, l, lpb, f);
     }
@@ -222,10 +269,10 @@ __device__ __noinline__ void tip_update(const JobDev& J, StepScalars& sc, float3
 }
 
 // Shared-memory cache of the Verlet rows as compact CSR: offsets by a CTA
-// scan of the row counts, then the entries as u16.  Returns 1 when the whole
-// list fits `cap` entries (else the rows are read from global memory).
+// scan of the row counts, then the entries as u16 for every bead whose row
+// ends within `cap` entries (the beads after it read their global rows).
 template <int BLOCK>
-__device__ int fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap, int* tot_smem) {
+__device__ void fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap, int* tot_smem) {
     const int n = J.n, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int per = (n + BLOCK - 1) / BLOCK, b0 = tid * per, b1 = min(n, b0 + per);
     int s = 0;
@@ -248,11 +295,11 @@ __device__ int fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap,
     for (int i = b0; i < b1; ++i) { off[i] = run; run += J.pl_cnt[i]; }
     if (tid == 0) off[n] = *tot_smem;
     __syncthreads();
-    const int fits = *tot_smem <= cap;
-    if (fits) {
+    {
         for (int i = w; i < n; i += BLOCK / 32) {
             const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
             const int k0 = off[i], cnt = off[i + 1] - k0;
+            if (off[i + 1] > cap) break;
             for (int kb = 0; kb < cnt; kb += 128) {
                 int v[4];
 #pragma unroll
@@ -269,7 +316,6 @@ __device__ int fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap,
         }
     }
     __syncthreads();
-    return fits;
 }
 
 // The updaters of one `stride` boundary in the reference order
@@ -319,8 +365,8 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
 }
 
 // Shared-memory bytes of a job's resident launch.
-__host__ __device__ inline size_t resident_smem_bytes(int n, int cache_entries) {
-    return ((size_t)n * kResidentSmemPerBead + 16 + (size_t)cache_entries * 2 + 15) & ~(size_t)15;
+__host__ __device__ inline size_t resident_smem_bytes(const JobDev& J) {
+    return resident_layout(J.n, J.ncov, J.nnat, J.bsm, J.lcache).total;
 }
 
 // Register cap of 64 per thread: 1024 threads of resident CTAs per SM.
@@ -338,18 +384,36 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
     __shared__ float red[BLOCK / 32][4];
     __shared__ int list_total;
     const int n = J.n, tid = threadIdx.x;
-    float4* xa = reinterpret_cast<float4*>(smem);
-    float4* xb = xa + n;
-    uint4* sd = reinterpret_cast<uint4*>(xb + n);
-    float4* F = reinterpret_cast<float4*>(sd + n);
-    float* Ts = reinterpret_cast<float*>(F + n);
-    int32_t* off = reinterpret_cast<int32_t*>(Ts + n);
-    uint16_t* nbr = reinterpret_cast<uint16_t*>(off + n + 4);
+    const ResidentLayout lay = resident_layout(n, J.ncov, J.nnat, J.bsm, J.lcache);
+    float4* xs = reinterpret_cast<float4*>(smem + lay.x);
+    float4* F = reinterpret_cast<float4*>(smem + lay.F);
+    uint4* sd = reinterpret_cast<uint4*>(smem + lay.sd);
+    float* Ts = reinterpret_cast<float*>(smem + lay.Ts);
+    int32_t* off = reinterpret_cast<int32_t*>(smem + lay.off);
+    uint8_t* fl = smem + lay.flags;
+    uint16_t* nbr = reinterpret_cast<uint16_t*>(smem + lay.nbr);
     for (int i = tid; i < n; i += BLOCK) {
-        xa[i] = J.x[i];
+        xs[i] = J.x[i];
         sd[i] = J.seeds[i];
         Ts[i] = J.T[i];
+        fl[i] = J.pulling ? J.flags[i] : (uint8_t)FLAG_FREE;
     }
+    __shared__ BondedView Bs;                 // read as a broadcast, not held in registers
+    if (tid == 0) Bs = global_bonded(J);
+    if (J.bsm) {
+        // the maps are constant for the launch: one copy into shared memory
+        int32_t* co = reinterpret_cast<int32_t*>(smem + lay.cov_off);
+        int32_t* no = reinterpret_cast<int32_t*>(smem + lay.nat_off);
+        int32_t* cj = reinterpret_cast<int32_t*>(smem + lay.cov_j);
+        float* cr = reinterpret_cast<float*>(smem + lay.cov_r0);
+        int32_t* nj = reinterpret_cast<int32_t*>(smem + lay.nat_j);
+        float2* np = reinterpret_cast<float2*>(smem + lay.nat_par);
+        for (int i = tid; i <= n; i += BLOCK) { co[i] = J.cov_off[i]; no[i] = J.nat_off[i]; }
+        for (int k = tid; k < J.ncov; k += BLOCK) { cj[k] = J.cov_j[k]; cr[k] = J.cov_r0[k]; }
+        for (int k = tid; k < J.nnat; k += BLOCK) { nj[k] = J.nat_j[k]; np[k] = J.nat_par[k]; }
+        if (tid == 0) Bs = BondedView{co, cj, cr, no, nj, np};
+    }
+    const BondedView& B = Bs;
     if (tid == 0) {
         sc.var = J.var;
         for (int c = 0; c < 3; ++c) {
@@ -367,35 +431,37 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
         sc.err = 0;
     }
     __syncthreads();
-    int cached = fill_cache<BLOCK>(J, off, nbr, J.lcache, &list_total);
+    const int cap = J.lcache;
+    fill_cache<BLOCK>(J, off, nbr, cap, &list_total);
 
     const int lpb = J.lpb, l = tid % lpb;
-    const unsigned gmask = group_mask(lpb) << ((tid & 31) & ~(lpb - 1));
     int err = 0;
     int64_t step = J.step;
     int phase = (int)(step % J.stride);       // steps since the last updater pass
-    float4* xc = xa;
-    float4* xn = xb;
     __shared__ int next_bead[2];              // per-step bead counters, double buffered
     if (tid < 2) next_bead[tid] = 0;
     __syncthreads();
     for (int64_t s = 0; s < nsteps; ++s, ++step) {
-        if (phase == 0 && run_updaters<BLOCK>(J, sc, xc, Ts, red, step, err))
-            cached = fill_cache<BLOCK>(J, off, nbr, J.lcache, &list_total);
+        if (phase == 0 && run_updaters<BLOCK>(J, sc, xs, Ts, red, step, err))
+            fill_cache<BLOCK>(J, off, nbr, cap, &list_total);
         if (++phase == J.stride) phase = 0;
         int* counter = &next_bead[s & 1];
-        // forces: lane groups take beads from a shared counter
+        // forces: each warp claims one bead per lane group from a shared
+        // counter, the groups sum their beads' terms and reduce by shuffles
         for (;;) {
-            int i = 0;
-            if (l == 0) i = atomicAdd(counter, 1);
-            i = __shfl_sync(gmask, i, 0, lpb);
-            if (i >= n) break;
-            const float4 xi = xc[i];
+            int base = 0;
+            if ((tid & 31) == 0) base = atomicAdd(counter, 32 / lpb);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= n) break;
+            const int i = base + (tid & 31) / lpb;
             float3 f = make_float3(0.f, 0.f, 0.f);
-            bonded_partial(J, xc, i, xi, l, lpb, f);
-            pairs_partial(J, xc, off, nbr, cached, i, xi, l, lpb, f);
-            f = group_reduce(f, lpb, gmask);
-            if (l == 0) {
+            const float4 xi = xs[i < n ? i : 0];
+            if (i < n) {
+                bonded_partial(J, B, xs, i, xi, l, lpb, f);
+                pairs_partial(J, xs, off, nbr, cap, i, xi, l, lpb, f);
+            }
+            f = group_reduce(f, lpb);
+            if (l == 0 && i < n) {
                 if (J.indent) {
                     float3 tf;
                     indentation_term(xi, sc.ig, f, tf);
@@ -409,7 +475,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
         __syncthreads();
         if (tid == 0) *counter = 0;          // reused two steps from now, after a barrier
         // integrateLangevin_kernel (src/Integrators/langevin_kernel.cu:17-58),
-        // one thread per bead
+        // one thread per bead, in place: every force of the step is final
         const float var = sc.var;
         for (int i = tid; i < n; i += BLOCK) {
             const float4 f4 = F[i];
@@ -422,21 +488,18 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int
                 f.y += gg.y * var;
                 f.z += gg.z * var;
             }
-            if (J.pulling) {
-                const uint8_t fl = J.flags[i];
-                if (fl == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
-                if (fl == FLAG_PULLED) { f.x += sc.pullF[0]; f.y += sc.pullF[1]; f.z += sc.pullF[2]; }
-            }
-            const float4 xi = xc[i];
+            const uint8_t fi = fl[i];
+            if (fi == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
+            if (fi == FLAG_PULLED) { f.x += sc.pullF[0]; f.y += sc.pullF[1]; f.z += sc.pullF[2]; }
+            const float4 xi = xs[i];
             const float dx = J.hOverZeta * f.x, dy = J.hOverZeta * f.y, dz = J.hOverZeta * f.z;
-            xn[i] = make_float4(xi.x + dx, xi.y + dy, xi.z + dz, xi.w);
+            xs[i] = make_float4(xi.x + dx, xi.y + dy, xi.z + dz, xi.w);
             Ts[i] += J.tempNorm * (dx * dx + dy * dy + dz * dz);
         }
         __syncthreads();
-        float4* t = xc; xc = xn; xn = t;
     }
     for (int i = tid; i < n; i += BLOCK) {
-        const float4 v = xc[i];
+        const float4 v = xs[i];
         if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) err = SOPB_STATUS_NONFINITE;
         J.x[i] = v;
         J.seeds[i] = sd[i];
@@ -481,8 +544,8 @@ k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, 
         const float4 xi = J.x[act ? i : 0];
         float3 f = make_float3(0.f, 0.f, 0.f);
         if (act) {
-            bonded_partial(J, J.x, i, xi, l, lpb, f);
-            pairs_partial(J, J.x, nullptr, nullptr, false, i, xi, l, lpb, f);
+            bonded_partial(J, global_bonded(J), J.x, i, xi, l, lpb, f);
+            pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {

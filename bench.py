@@ -103,6 +103,20 @@ def alg_bytes_per_bead_step(st, pairs_freq):
             + (4 * st["n_possible"] + 4 * st["n_pair"]) / pairs_freq)
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) that ncu measured
+# over every launch of one bench step, per bead-step, for the bench's own
+# command lines: batch512 (--policy 4,1,1024), 200 Langevin steps per step
+# over three launch classes; the values scale with the bead-steps of a step.
+NCU_DRAM_BYTES_PER_BEAD_STEP = {
+    "batch512": (71.892736e6 + 18.4832e6 + 5.900544e6 + 0.024064e6 + 0.466432e6 + 0.002048e6) / (113612 * 200),
+}
+
+
+def traffic_per_step(workload, bead_steps):
+    b = NCU_DRAM_BYTES_PER_BEAD_STEP.get(workload)
+    return None if b is None else b * bead_steps
+
+
 def peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -362,8 +376,9 @@ def run_gpu(args):
                                                         "beads_per_group": tuned["policy"][1],
                                                         "max_block": tuned["policy"][2]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "alg_bytes_per_bead_step": bps, "lists": stats},
+                         "frac": achieved / peak, "traffic": traffic_per_step("batch512", beads * chunk),
+                         "traffic_scope": "DRAM bytes of one bench step (all launch classes), ncu",
+                         "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats},
             "plain": plain,
             "batched_over_plain": value / plain["value"] if plain else None,
             "cpu_baseline": cpu,
@@ -454,7 +469,9 @@ def run_capsid(args):
                       "l2": "flushed between timed steps"},
            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": spec.n * 16, "d2h_bytes_per_step": spec.n * 16},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "traffic": None, "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats},
+                        "traffic": traffic_per_step("capsid", spec.n * chunk),
+                        "traffic_scope": "DRAM bytes of one bench step (every launch of the step), ncu",
+                        "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats},
            "tip": job.read(sopb.TIPSTATE)[:11].tolist(), "clocks": clk.summary()}
     print(json.dumps(out), flush=True)
     ctx.close()

@@ -478,6 +478,121 @@ def run_capsid(args):
     return 0
 
 
+def hi_spec(n, exact, refresh=10, seed=4000):
+    """The HI configuration: one n-bead globule (the plain configuration's
+    generator and force-ramp pull), RPY radius 3.8 A; exact (Cholesky factor
+    refreshed every `refresh` steps) or TEA (epsilon every 10 steps)."""
+    import sopb
+    import sopb_synth as S
+    s = S.make_system(n, seed)
+    p = plain_params(pulling=1, deltax=0.5, k_trans=0.05, pullFreq=1000, fixedEnd=0, pulledEnd=n - 1,
+                     hi_on=1, hi_a=3.8, hi_exact=1 if exact else 0, hi_refresh=refresh, hi_epsilon_freq=10,
+                     hi_capricious=0, max_possiblePairs=4096)
+    return sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[n - 1], seed=1119727)
+
+
+def factor_error(job, ctx, spec):
+    """||L L^T - D|| / ||D|| (Frobenius) of the factor the job holds, with D
+    assembled in FP64 from the coordinates it was factorised at; FP64 on the
+    device with torch (measurement only)."""
+    import torch
+    import sopb
+    x0 = job.read(sopb.COORDS)[:, :3].astype(np.float64)
+    ctx.run([job], 1)                       # the next step refreshes at x0
+    ctx.sync()
+    L = torch.from_numpy(job.read(sopb.HIFACTOR)).cuda().double().tril_()
+    x = torch.from_numpy(x0).cuda()
+    n, a = x.shape[0], float(spec.params.hi_a)
+    d = x[None, :, :] - x[:, None, :]                       # d[i, q] = x_q - x_i
+    r = d.norm(dim=2)
+    r.fill_diagonal_(1.0)
+    e = d / r[:, :, None]
+    ra = r / a
+    far = ra > 2.0
+    crr = torch.where(far, 0.75 / ra * (1.0 - 2.0 / ra ** 2), 3.0 * ra / 32.0)
+    cii = torch.where(far, 0.75 / ra * (1.0 + 2.0 / 3.0 / ra ** 2), 1.0 - 9.0 * ra / 32.0)
+    blk = e[:, :, :, None] * e[:, :, None, :] * crr[:, :, None, None] + \
+        torch.eye(3, dtype=torch.float64, device=x.device) * cii[:, :, None, None]
+    idx = torch.arange(n, device=x.device)
+    blk[idx, idx] = torch.eye(3, dtype=torch.float64, device=x.device)
+    D = blk.permute(0, 2, 1, 3).reshape(3 * n, 3 * n)
+    del blk, d, e
+    err = float(torch.linalg.matrix_norm(L @ L.T - D) / torch.linalg.matrix_norm(D))
+    del L, D
+    torch.cuda.empty_cache()
+    return err
+
+
+def run_hi(args):
+    """HI workload: one 4000-bead job with exact hydrodynamics (blocked
+    Cholesky of the 12 000 x 12 000 tensor, refreshed every 10 steps) and the
+    same job with TEA, on the grid path."""
+    import torch
+    import sopb
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    ctx = sopb.Context(dev, stream=stream.cuda_stream)
+    n = args.hi_beads
+    chunk = args.chunk
+    res = {}
+    clocks = None
+    for kind in ("exact", "tea"):
+        spec = hi_spec(n, kind == "exact")
+        job = ctx.job(spec)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                ctx.run([job], chunk)
+        ctx.sync()
+        if job.status() != 0:
+            raise RuntimeError("hi %s job failed in warm-up: status %d" % (kind, job.status()))
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        with ClockSampler(dev) as clk:
+            with torch.cuda.stream(stream):
+                for k in range(args.steps):
+                    starts[k].record(stream)
+                    ctx.run([job], chunk)
+                    ends[k].record(stream)
+            torch.cuda.synchronize()
+        total_ms = sum(s_.elapsed_time(e) for s_, e in zip(starts, ends))
+        if job.status() != 0:
+            raise RuntimeError("hi %s job failed: status %d" % (kind, job.status()))
+        res[kind] = {"value": n * chunk * args.steps / (total_ms / 1e3), "ms_per_langevin_step": total_ms / (chunk * args.steps)}
+        if kind == "exact":
+            clocks = clk.summary()
+            host = torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy()
+            ctx.download_coords([job], host)
+            t0 = time.perf_counter()
+            for k in range(args.steps):
+                ctx.upload_coords([job], host)
+                ctx.run([job], chunk)
+                ctx.download_coords([job], host)
+            torch.cuda.synchronize()
+            e2e = n * chunk * args.steps / (time.perf_counter() - t0)
+            # land on a refresh boundary, then measure the factor made there
+            left = (-job.step()) % 10
+            if left:
+                ctx.run([job], left)
+            res["exact"]["factor_rel_error_fp64"] = factor_error(job, ctx, spec)
+        job.destroy()
+    m = 3 * n
+    refresh_flop = m ** 3 / 3.0
+    out = {"metric": "bead-steps/s (exact HI, %d beads)" % n, "value": res["exact"]["value"], "unit": UNIT,
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic (seeded globule)",
+           "config": {"workload": "hi%d_exact_refresh10" % n, "beads": n, "langevin_steps_per_step": chunk,
+                      "hi_a_A": 3.8, "hi_refresh": 10, "tensor": "%d x %d FP32" % (m, m)},
+           "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": n * 16},
+           "exact": res["exact"], "tea": res["tea"],
+           "flop_per_refresh": refresh_flop,
+           "clocks": clocks}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
 def run_serve(args):
     """Serving workload: a seeded Poisson stream of pulling, clamp and
     indentation jobs (sizes log-normal in [50, 5000], 30% with HI: exact for
@@ -540,7 +655,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--workload", default="batch512", choices=["batch512", "serve", "capsid"])
+    ap.add_argument("--workload", default="batch512", choices=["batch512", "serve", "capsid", "hi"])
+    ap.add_argument("--hi-beads", type=int, default=4000)
     ap.add_argument("--serve-jobs", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-quantum", type=int, default=1000)
@@ -553,6 +669,8 @@ def main():
         return run_serve(args)
     if args.workload == "capsid":
         return run_capsid(args)
+    if args.workload == "hi":
+        return run_hi(args)
     return run_gpu(args)
 
 

@@ -169,7 +169,10 @@ enum {
     SOPB_TIPFORCES = 4,/* float[4n]  per-bead tip force accumulator           */
     SOPB_PULLSTATE = 5,/* float[12]  extForce[3] cant[3] cant0[3] vec[3]      */
     SOPB_TIPSTATE = 6, /* float[16]  tip[3] chip[3] micaR[3] V dx fav[4] pad  */
-    SOPB_HISTATE = 7   /* float[4]   TEA beta', epsilon (computeTEAeps), 0, 0 */
+    SOPB_HISTATE = 7,  /* float[4]   TEA beta', epsilon (computeTEAeps), 0, 0 */
+    SOPB_HIFACTOR = 8  /* float[9n^2] exact HI: the (3n)^2 tensor, row-major, */
+                       /*            its lower triangle the Cholesky factor L */
+                       /*            of D at the last refresh (read only)     */
 };
 
 /* ---- host utilities ---------------------------------------------------- */

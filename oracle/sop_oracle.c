@@ -171,6 +171,7 @@ struct orc_job {
     float beta, epsilon;
     float* tensor;
     int32_t status;
+    int32_t refresh_due;   /* exact HI: refactorise D at the next step */
 };
 
 static int32_t compute_stride(const sopb_params* p) {
@@ -182,6 +183,7 @@ static int32_t compute_stride(const sopb_params* p) {
     if (p->pulling && p->deltax != 0.0f) MINF(p->pullFreq > 0 ? p->pullFreq : p->nav);
     if (p->heating) MINF(p->tempFreq);
     if (p->hi_on && !p->hi_exact) MINF(p->hi_epsilon_freq);
+    if (p->hi_on && p->hi_exact && p->hi_refresh > 1) MINF(p->hi_refresh);   /* factor refresh updater */
 #undef MINF
     return s;
 }
@@ -710,6 +712,7 @@ static void run_updaters(orc_job* j) {
     if (p->heating && j->step % p->tempFreq == 0) /* langevin.cu:129-135 */
         set_temperature(j, p->initialT + (float)(j->step / p->tempFreq) * p->deltaT);
     if (p->hi_on && !p->hi_exact) tea_update(j);
+    if (p->hi_on && p->hi_exact && p->hi_refresh > 1 && j->step % p->hi_refresh == 0) j->refresh_due = 1;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -853,7 +856,7 @@ static void tea_integrate(orc_job* j) {
 /* integrateCholesky_D (src/Integrators/bdhitea_kernel.cu:89-152).  The
  * reference thread writes mforce[i] while others read mforce[j]; here every
  * bead reads the prepared forces (the race-free intent). */
-static void chol_D(orc_job* j) {
+static void chol_D(orc_job* j, int assemble) {
     const int32_t n = j->n, m = 3 * n;
     float* M = j->tensor;
     float* nm = (float*)malloc(16 * (size_t)n);
@@ -866,9 +869,11 @@ static void chol_D(orc_job* j) {
             float* row1 = row0 + m;
             float* row2 = row1 + m;
             if (q == i) {
-                row0[0] = 1; row0[1] = 0; row0[2] = 0;
-                row1[0] = 0; row1[1] = 1; row1[2] = 0;
-                row2[0] = 0; row2[1] = 0; row2[2] = 1;
+                if (assemble) {
+                    row0[0] = 1; row0[1] = 0; row0[2] = 0;
+                    row1[0] = 0; row1[1] = 1; row1[2] = 0;
+                    row2[0] = 0; row2[1] = 0; row2[2] = 1;
+                }
                 continue;
             }
             const float* xq = F4(j->x, q);
@@ -879,9 +884,11 @@ static void chol_D(orc_job* j) {
             d[2] /= d[3];
             float D[6];
             rpy(d[0], d[1], d[2], d[3], j->p.hi_a, D);
-            row0[0] = D[0]; row0[1] = D[1]; row0[2] = D[2];
-            row1[0] = D[1]; row1[1] = D[3]; row1[2] = D[4];
-            row2[0] = D[2]; row2[1] = D[4]; row2[2] = D[5];
+            if (assemble) {
+                row0[0] = D[0]; row0[1] = D[1]; row0[2] = D[2];
+                row1[0] = D[1]; row1[1] = D[3]; row1[2] = D[4];
+                row2[0] = D[2]; row2[1] = D[4]; row2[2] = D[5];
+            }
             const float* fq = F4(j->mf, q);
             f[0] += D[0] * fq[0] + D[1] * fq[1] + D[2] * fq[2];
             f[1] += D[1] * fq[0] + D[3] * fq[1] + D[4] * fq[2];
@@ -1014,8 +1021,12 @@ static void one_step(orc_job* j) {
         if (!j->p.hi_exact) {
             tea_integrate(j);
         } else {
-            chol_D(j);
-            orc_cholesky_ref(3 * n, j->tensor);
+            /* the factor of D is refreshed every step (hi_refresh 1, the
+             * reference) or at the updater boundaries due for it */
+            const int refresh = j->p.hi_refresh <= 1 || j->refresh_due;
+            chol_D(j, refresh);
+            if (refresh) orc_cholesky_ref(3 * n, j->tensor);
+            j->refresh_due = 0;
             chol_L(j);
         }
     }

@@ -16,6 +16,7 @@
 #include "sopb_resident.cuh"
 #include "sopb_grid.cuh"
 #include "sopb_hi.cuh"
+#include "sopb_chol.cuh"
 
 using namespace sopb;
 
@@ -113,6 +114,7 @@ struct sopb_job {
     void* amem = nullptr;
     int64_t host_step = 0;             // the device step counter, tracked on the host
     cudaGraphExec_t chunk = nullptr;   // one stride chunk: updaters + stride steps
+    cudaGraphExec_t chunk_r = nullptr; // the same with the Cholesky refresh at its first step
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
 };
@@ -247,6 +249,7 @@ int32_t compute_stride(const sopb_params& p) {
     if (p.pulling && p.deltax != 0.0f) mn(p.pullFreq > 0 ? p.pullFreq : p.nav);
     if (p.heating) mn(p.tempFreq);
     if (p.hi_on && !p.hi_exact) mn(p.hi_epsilon_freq);
+    if (p.hi_on && p.hi_exact && p.hi_refresh > 1) mn(p.hi_refresh);   // the factor refresh is an updater
     return s;
 }
 
@@ -300,6 +303,9 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
         (rc = set_smem_attr<1024>(device, dm, &ss[4])))
         return rc;
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholPotrfSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholTrsmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_apply_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kCholMaxBeads * 12));
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
     *out = c;
     return SOPB_OK;
@@ -388,7 +394,10 @@ int validate_desc(const sopb_job_desc* d) {
         if (p.minimization) return SOPB_ERR_INVALID;
         if (p.hi_a <= 0.0f) return SOPB_ERR_INVALID;
         if (!p.hi_exact && p.hi_epsilon_freq <= 0) return SOPB_ERR_INVALID;
-        if (p.hi_exact && n > 128) return SOPB_ERR_UNSUPPORTED;   // blocked factorisation: not in this build
+        if (p.hi_exact && n > kCholMaxBeads) return SOPB_ERR_UNSUPPORTED;
+        // the reference-compatible B (symmetrised upper blocks) exists for the
+        // reference's own size range only
+        if (p.hi_exact && n > 128 && p.hi_b_mode == SOPB_HI_B_REFCOMPAT) return SOPB_ERR_UNSUPPORTED;
     }
     return SOPB_OK;
 }
@@ -438,7 +447,8 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
     const bool hi = p.hi_on != 0;
     const int itiles = (n + kHiTile - 1) / kHiTile;
     j->jsplit = 1;
-    if (hi && !p.hi_exact && p.hi_unlisted)
+    const bool blocked = hi && p.hi_exact && n > 128;
+    if ((hi && !p.hi_exact && p.hi_unlisted) || blocked)
         j->jsplit = std::max(1, std::min((4 * c->sm_count + itiles - 1) / itiles, itiles));
     const size_t part_elems = std::max<size_t>(2 * (size_t)a.npart, hi ? (size_t)j->jsplit * n : 0);
     size_t off = 0;
@@ -451,8 +461,8 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
         o_ci = off; off += align256((size_t)n * 16);
         o_eps = off; off += align256((size_t)n * 4);
         if (p.hi_exact) {
-            a.ld = 3 * n;
-            o_ten = off; off += align256((size_t)a.ld * a.ld * 4);
+            a.ld = blocked ? chol_ld(n) : 3 * n;
+            o_ten = off; off += align256((size_t)3 * n * a.ld * 4);
         }
     }
     const size_t o_geo = off; off += align256(8 * sizeof(float));
@@ -516,7 +526,25 @@ int grid_possible(sopb_job* j, JobDev* Jp, cudaStream_t st, int force) {
 
 // Updaters of a stride boundary (each gated on the device step), then
 // `steps` Langevin steps, then the step counter moves by `steps`.
-int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps) {
+// Exact HI of a job above 128 beads: assemble D and factorise it in place.
+int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
+    GridAux& a = j->aux;
+    const int n = j->n, m = 3 * n, sms = j->ctx->sm_count;
+    k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Jp, a);
+    for (int k = 0; k < m; k += kCholNB) {
+        k_chol_potrf<<<1, 256, kCholPotrfSmem, st>>>(Jp, a, k);
+        const int t0 = k + kCholNB;
+        if (t0 >= m) break;
+        const int rows = m - t0;
+        k_chol_trsm<<<std::min((rows + 7) / 8, 2 * sms), 256, kCholTrsmSmem, st>>>(Jp, a, k);
+        const int t = (rows + kCholTile - 1) / kCholTile;
+        k_chol_syrk<<<t * (t + 1) / 2, 256, 0, st>>>(Jp, a, k);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return SOPB_OK;
+}
+
+int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, bool refresh_first = false) {
     sopb_context* c = j->ctx;
     JobDev* Jp = &c->d_jobs[j->slot];
     GridAux& a = j->aux;
@@ -548,10 +576,24 @@ int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps) {
             k_tea_force_partial<<<tg, kHiTile, 0, st>>>(Jp, a, j->jsplit);
             k_tea_integrate<<<nb, kGridBlock, 0, st>>>(Jp, a, j->jsplit);
         } else {
+            // the factor is refreshed every step (hi_refresh 1, the
+            // reference) or at the updater boundaries due for it
+            const bool refresh = j->h.hi_refresh <= 1 || (s == 0 && refresh_first);
             k_hi_prepare<<<nb, kGridBlock, 0, st>>>(Jp, a);
-            k_chol_D<<<nb, kGridBlock, 0, st>>>(Jp, a);
-            k_chol_factor_small<<<1, 384, 0, st>>>(Jp, a);
-            k_chol_apply<<<nb, kGridBlock, 0, st>>>(Jp, a);
+            if (j->n <= 128) {
+                k_chol_D<<<nb, kGridBlock, 0, st>>>(Jp, a, refresh ? 1 : 0);
+                if (refresh) k_chol_factor_small<<<1, 384, 0, st>>>(Jp, a);
+                k_chol_apply<<<nb, kGridBlock, 0, st>>>(Jp, a);
+            } else {
+                const dim3 tg((j->n + kHiTile - 1) / kHiTile, j->jsplit);
+                k_hi_df_partial<<<tg, kHiTile, 0, st>>>(Jp, a, j->jsplit);
+                if (refresh) {
+                    int rc = chol_refresh(j, Jp, st);
+                    if (rc) return rc;
+                }
+                const int ab = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 8);
+                k_chol_apply_rows<<<ab, 256, (size_t)j->n * 12, st>>>(Jp, a, j->jsplit);
+            }
         }
     }
     k_g_advance<<<1, 32, 0, st>>>(Jp, steps);
@@ -570,25 +612,31 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
         j->host_step++;
         left--;
     }
+    // Cholesky refresh at an updater boundary (hi_refresh > 1)
+    const int32_t refresh = j->h.hi && j->h.hi_exact ? j->h.hi_refresh : 0;
+    auto refresh_due = [&](int64_t step) { return refresh > 1 && step % refresh == 0; };
     const int64_t chunks = left / stride;
-    if (chunks > 0) {
-        if (!j->chunk) {
+    for (int64_t k = 0; k < chunks; ++k) {
+        const bool r = refresh_due(j->host_step);
+        cudaGraphExec_t& ge = r ? j->chunk_r : j->chunk;
+        if (!ge) {
             cudaGraph_t g;
             cudaStream_t cap = j->ctx->side[kSideStreams - 1];
             CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-            rc = grid_launch(j, cap, true, stride);
+            rc = grid_launch(j, cap, true, stride, r);
             cudaError_t e = cudaStreamEndCapture(cap, &g);
             if (rc) return rc;
             CUDA_TRY(e);
-            CUDA_TRY(cudaGraphInstantiate(&j->chunk, g, 0));
+            CUDA_TRY(cudaGraphInstantiate(&ge, g, 0));
             cudaGraphDestroy(g);
         }
-        for (int64_t k = 0; k < chunks; ++k) CUDA_TRY(cudaGraphLaunch(j->chunk, st));
-        j->host_step += chunks * stride;
-        left -= chunks * stride;
+        CUDA_TRY(cudaGraphLaunch(ge, st));
+        j->host_step += stride;
+        left -= stride;
     }
     while (left > 0) {
-        if ((rc = grid_launch(j, st, j->host_step % stride == 0, 1))) return rc;
+        const bool boundary = j->host_step % stride == 0;
+        if ((rc = grid_launch(j, st, boundary, 1, boundary && refresh_due(j->host_step)))) return rc;
         j->host_step++;
         left--;
     }
@@ -876,6 +924,7 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     if (j->chunk) cudaGraphExecDestroy(j->chunk);
+    if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
     if (j->amem) cudaFree(j->amem);
     cudaFree(j->dmem);
     c->beads.release(j->b0, j->n);
@@ -1059,6 +1108,13 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         o[1] = j->h.epsilon;
         o[2] = o[3] = 0.0f;
         return SOPB_OK;
+    }
+    case SOPB_HIFACTOR: {
+        if (!j->h.hi || !j->h.hi_exact || !j->aux.tensor) return SOPB_ERR_INVALID;
+        const size_t m = 3 * (size_t)n;
+        CUDA_TRY(cudaMemcpy2DAsync(out, m * 4, j->aux.tensor, (size_t)j->aux.ld * 4, m * 4, m,
+                                   cudaMemcpyDeviceToHost, c->stream));
+        break;
     }
     case SOPB_TIPSTATE: {
         int rc = read_slot(j);

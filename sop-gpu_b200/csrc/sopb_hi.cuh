@@ -273,10 +273,11 @@ k_tea_integrate(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
 
 // ---- exact HI, n <= 128 ---------------------------------------------------------
 // integrateCholesky_D (bdhitea_kernel.cu:89-152): bead i's block column of
-// D (identity diagonal blocks) and D F with every bead reading the prepared
-// forces (the reference reads them while other threads overwrite them).
+// D (identity diagonal blocks; written when the factor is refreshed) and
+// D F with every bead reading the prepared forces (the reference reads them
+// while other threads overwrite them).
 __global__ void __launch_bounds__(kGridBlock)
-k_chol_D(JobDev* __restrict__ Jp, GridAux aux) {
+k_chol_D(JobDev* __restrict__ Jp, GridAux aux, int assemble) {
     const JobDev& J = *Jp;
     if (J.status) return;
     const int n = J.n, ld = aux.ld;
@@ -288,15 +289,19 @@ k_chol_D(JobDev* __restrict__ Jp, GridAux aux) {
             float* r1 = r0 + ld;
             float* r2 = r1 + ld;
             if (q == i) {
-                r0[0] = 1.f; r0[1] = 0.f; r0[2] = 0.f;
-                r1[0] = 0.f; r1[1] = 1.f; r1[2] = 0.f;
-                r2[0] = 0.f; r2[1] = 0.f; r2[2] = 1.f;
+                if (assemble) {
+                    r0[0] = 1.f; r0[1] = 0.f; r0[2] = 0.f;
+                    r1[0] = 0.f; r1[1] = 1.f; r1[2] = 0.f;
+                    r2[0] = 0.f; r2[1] = 0.f; r2[2] = 1.f;
+                }
                 continue;
             }
             const Blk6 d = rpy_between(xi, J.x[q], J.hi_a);
-            r0[0] = d.xx; r0[1] = d.xy; r0[2] = d.xz;
-            r1[0] = d.xy; r1[1] = d.yy; r1[2] = d.yz;
-            r2[0] = d.xz; r2[1] = d.yz; r2[2] = d.zz;
+            if (assemble) {
+                r0[0] = d.xx; r0[1] = d.xy; r0[2] = d.xz;
+                r1[0] = d.xy; r1[1] = d.yy; r1[2] = d.yz;
+                r2[0] = d.xz; r2[1] = d.yz; r2[2] = d.zz;
+            }
             const float4 fq = aux.mf[q];
             f.x += d.xx * fq.x + d.xy * fq.y + d.xz * fq.z;
             f.y += d.xy * fq.x + d.yy * fq.y + d.yz * fq.z;

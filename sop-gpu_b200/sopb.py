@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "libsopb.so")
 OK, ERR_INVALID, ERR_CAPACITY, ERR_NONFINITE, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_HI, ERR_NODEVICE = range(10)
 PULL_END_TO_END, PULL_VECTOR = 0, 1
 HI_B_CHOLESKY, HI_B_REFCOMPAT = 0, 1
-COORDS, SEEDS, TEMP, FORCES, TIPFORCES, PULLSTATE, TIPSTATE, HISTATE = range(8)
+COORDS, SEEDS, TEMP, FORCES, TIPFORCES, PULLSTATE, TIPSTATE, HISTATE, HIFACTOR = range(9)
 
 F3 = C.c_float * 3
 
@@ -219,7 +219,8 @@ class Job:
     def read(self, what: int) -> np.ndarray:
         shapes = {COORDS: ((self.n, 4), np.float32), SEEDS: ((self.n, 4), np.uint32), TEMP: ((self.n,), np.float32),
                   FORCES: ((self.n, 4), np.float32), TIPFORCES: ((self.n, 4), np.float32),
-                  PULLSTATE: ((12,), np.float32), TIPSTATE: ((16,), np.float32), HISTATE: ((4,), np.float32)}
+                  PULLSTATE: ((12,), np.float32), TIPSTATE: ((16,), np.float32), HISTATE: ((4,), np.float32),
+                  HIFACTOR: ((3 * self.n, 3 * self.n), np.float32)}
         shape, dt = shapes[what]
         out = np.zeros(shape, dt)
         check(lib().sopb_job_read(self.handle, what, out.ctypes.data), "job_read")

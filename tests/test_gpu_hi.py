@@ -1,6 +1,8 @@
 """Hydrodynamic interactions on the CUDA path against the oracle: TEA with
-all-pairs and listed couplings, and exact HI (n <= 128) with the true
-Cholesky factor and with the reference-compatible noise matrix."""
+all-pairs and listed couplings, and exact HI with the true Cholesky factor
+(the reference's single-CTA factorisation up to 128 beads, the blocked one
+above, refreshed every step or every hi_refresh steps) and with the
+reference-compatible noise matrix."""
 import numpy as np
 import pytest
 
@@ -58,10 +60,55 @@ def test_exact_hi_tracks_oracle(gpu_ctx, n, bmode):
     g.destroy()
 
 
-def test_exact_hi_above_128_beads_is_reported_unsupported(gpu_ctx):
+def test_reference_noise_matrix_above_128_beads_is_unsupported(gpu_ctx):
+    # the symmetrised-upper-block B exists for the reference's sizes only
     with pytest.raises(sopb.SopbError) as e:
-        gpu_ctx.job(hi_spec(200, 1, hi_exact=1))
+        gpu_ctx.job(hi_spec(200, 1, hi_exact=1, hi_b_mode=sopb.HI_B_REFCOMPAT))
     assert e.value.code == sopb.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("n", [129, 200, 451])
+def test_blocked_factor_matches_fp64_cholesky(gpu_ctx, n):
+    sp = hi_spec(n, 37, "free", hi_exact=1)
+    g = gpu_ctx.job(sp)
+    x0 = g.read(sopb.COORDS)[:, :3].copy()
+    gpu_ctx.run([g], 1)                       # step 0 factorises D at x0
+    assert g.status() == 0
+    L = np.tril(g.read(sopb.HIFACTOR).astype(np.float64))
+    D = O.rpy_tensor(x0, sp.params.hi_a)
+    L64 = np.linalg.cholesky(D)
+    assert np.max(np.abs(L - L64)) < 2e-4
+    assert np.linalg.norm(L @ L.T - D) / np.linalg.norm(D) < 2e-6
+    g.destroy()
+
+
+@pytest.mark.parametrize("n,refresh", [(150, 1), (300, 1), (300, 10), (100, 10)])
+def test_exact_hi_with_refresh_tracks_oracle(gpu_ctx, n, refresh):
+    # the blocked factorisation above 128 beads and the refresh updater on
+    # both paths against the oracle's column Cholesky
+    sp = hi_spec(n, 41, "clamp", hi_exact=1, hi_refresh=refresh)
+    g, o = gpu_ctx.job(sp), O.OracleJob(sp)
+    steps = 23
+    gpu_ctx.run([g], steps)
+    assert o.advance(steps) == 0
+    assert g.status() == 0
+    assert np.array_equal(g.read(sopb.SEEDS), o.read(sopb.SEEDS))
+    dx = np.max(np.abs(g.read(sopb.COORDS) - o.read(sopb.COORDS)))
+    assert dx < 1e-3, dx
+    g.destroy()
+
+
+def test_stale_factor_differs_from_fresh_one(gpu_ctx):
+    # with refresh 10 the factor read after 5 steps is still the step-0 one
+    sp = hi_spec(200, 43, "free", hi_exact=1, hi_refresh=10)
+    g = gpu_ctx.job(sp)
+    gpu_ctx.run([g], 1)
+    L0 = g.read(sopb.HIFACTOR).copy()
+    gpu_ctx.run([g], 4)
+    assert np.array_equal(np.tril(g.read(sopb.HIFACTOR)), np.tril(L0))
+    gpu_ctx.run([g], 6)                       # step 10 refreshes
+    assert not np.array_equal(np.tril(g.read(sopb.HIFACTOR)), np.tril(L0))
+    g.destroy()
 
 
 def test_hi_with_minimization_is_rejected(gpu_ctx):

@@ -596,7 +596,7 @@ def run_hi(args):
 def run_serve(args):
     """Serving workload: a seeded Poisson stream of pulling, clamp and
     indentation jobs (sizes log-normal in [50, 5000], 30% with HI: exact for
-    n <= 128, TEA above), served by continuous batching; throughput and
+    n <= 1500, TEA above), served by continuous batching; throughput and
     p50/p99 completion latency, next to each sampled job's time alone."""
     import torch
     import sopb

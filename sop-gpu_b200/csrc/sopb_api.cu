@@ -23,7 +23,8 @@ using namespace sopb;
 namespace {
 
 constexpr int kJobSlots = 16384;
-constexpr int kSideStreams = 4;
+constexpr int kSideStreams = 4;   // resident launch classes run side by side
+constexpr int kGridStreams = 8;   // grid-path jobs run side by side
 constexpr int64_t kDefaultBeadCapacity = int64_t(1) << 22;
 
 // First-fit allocator over index ranges [0, cap).
@@ -91,6 +92,9 @@ struct sopb_context {
     std::vector<sopb_job*> slots;
     std::vector<int> free_slots;
     cudaStream_t side[kSideStreams] = {};
+    cudaStream_t gside[kGridStreams] = {};
+    cudaEvent_t gev_join[kGridStreams] = {};
+    cudaStream_t capture = nullptr;   // CUDA graph capture of grid-path chunks
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[kSideStreams] = {};
     int32_t last_error = SOPB_OK;
@@ -294,6 +298,11 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
         CUDA_TRY(cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking));
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));
     }
+    for (int k = 0; k < kGridStreams; ++k) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&c->gside[k], cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&c->gev_join[k], cudaEventDisableTiming));
+    }
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
     int rc;
     int* dm = &c->smem_dyn_max;
@@ -303,7 +312,6 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
         (rc = set_smem_attr<1024>(device, dm, &ss[4])))
         return rc;
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
-    CUDA_TRY(cudaFuncSetAttribute(k_chol_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholPotrfSmem));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholTrsmSmem));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_apply_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kCholMaxBeads * 12));
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
@@ -317,6 +325,9 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     cudaStreamSynchronize(c->stream);
     for (sopb_job* j : c->slots)
         if (j) {
+            if (j->chunk) cudaGraphExecDestroy(j->chunk);
+            if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
+            if (j->amem) cudaFree(j->amem);
             cudaFree(j->dmem);
             delete j;
         }
@@ -333,6 +344,11 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
         cudaStreamDestroy(c->side[k]);
         cudaEventDestroy(c->ev_join[k]);
     }
+    for (int k = 0; k < kGridStreams; ++k) {
+        cudaStreamDestroy(c->gside[k]);
+        cudaEventDestroy(c->gev_join[k]);
+    }
+    cudaStreamDestroy(c->capture);
     cudaEventDestroy(c->ev_fork);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -532,11 +548,11 @@ int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     const int n = j->n, m = 3 * n, sms = j->ctx->sm_count;
     k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Jp, a);
     for (int k = 0; k < m; k += kCholNB) {
-        k_chol_potrf<<<1, 256, kCholPotrfSmem, st>>>(Jp, a, k);
+        k_chol_potrf<<<1, kPotrfThreads, 0, st>>>(Jp, a, k);
         const int t0 = k + kCholNB;
         if (t0 >= m) break;
         const int rows = m - t0;
-        k_chol_trsm<<<std::min((rows + 7) / 8, 2 * sms), 256, kCholTrsmSmem, st>>>(Jp, a, k);
+        k_chol_trsm<<<std::min((rows + 8 * kTrsmRows - 1) / (8 * kTrsmRows), 2 * sms), 256, kCholTrsmSmem, st>>>(Jp, a, k);
         const int t = (rows + kCholTile - 1) / kCholTile;
         k_chol_syrk<<<t * (t + 1) / 2, 256, 0, st>>>(Jp, a, k);
     }
@@ -621,7 +637,7 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
         cudaGraphExec_t& ge = r ? j->chunk_r : j->chunk;
         if (!ge) {
             cudaGraph_t g;
-            cudaStream_t cap = j->ctx->side[kSideStreams - 1];
+            cudaStream_t cap = j->ctx->capture;
             CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
             rc = grid_launch(j, cap, true, stride, r);
             cudaError_t e = cudaStreamEndCapture(cap, &g);
@@ -894,6 +910,8 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     CUDA_TRY(cudaMemcpyAsync(h.flags, flags.data(), (size_t)n, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemsetAsync(h.T, 0, (size_t)n * 4, st));
     CUDA_TRY(cudaMemsetAsync(h.tipF, 0, (size_t)n * 16, st));
+    j->b0 = b0;   // the grid buffers are views of the job's bead range
+    j->n = n;
     if (h.grid) {
         int rc2 = grid_alloc(c, j, p, n);
         if (rc2) {
@@ -982,49 +1000,46 @@ extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, i
     CUDA_TRY(cudaSetDevice(c->device));
     std::vector<sopb_job*> resident, grid;
     for (int32_t k = 0; k < njobs; ++k) (jobs[k]->h.grid ? grid : resident).push_back(jobs[k]);
-    if (resident.empty()) {
-        for (sopb_job* j : grid) {
-            int rc = grid_run(j, c->stream, nsteps);
-            if (rc) return rc;
-        }
-        return SOPB_OK;
-    }
-    if (!grid.empty()) {
-        // grid jobs on the context stream, resident classes beside them
-        int rc = sopb_run(c, resident.data(), (int32_t)resident.size(), nsteps);
-        if (rc) return rc;
-        for (sopb_job* j : grid) {
-            rc = grid_run(j, c->stream, nsteps);
-            if (rc) return rc;
-        }
-        return SOPB_OK;
-    }
+    // resident jobs: one launch per class; the class table goes up first
     std::vector<LaunchClass> cls;
-    group_jobs(c, jobs, njobs, cls);
-    std::vector<int32_t> ids;
     std::vector<size_t> off;
-    for (auto& L : cls) {
-        off.push_back(ids.size());
-        ids.insert(ids.end(), L.ids.begin(), L.ids.end());
+    int rc;
+    if (!resident.empty()) {
+        group_jobs(c, resident.data(), (int32_t)resident.size(), cls);
+        std::vector<int32_t> ids;
+        for (auto& L : cls) {
+            off.push_back(ids.size());
+            ids.insert(ids.end(), L.ids.begin(), L.ids.end());
+        }
+        if ((rc = ensure_ids(c, (int64_t)ids.size()))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(c->d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->stream));
     }
-    int rc = ensure_ids(c, (int64_t)ids.size());
-    if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(c->d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->stream));
-    if (cls.size() == 1) {
-        const LaunchClass& L = cls[0];
-        return launch_resident(L.block, (int)L.ids.size(), L.smem, c->stream, c->d_jobs, c->d_ids, nsteps);
-    }
+    // one class or one grid job alone: straight on the context stream
+    if (grid.empty() && cls.size() == 1)
+        return launch_resident(cls[0].block, (int)cls[0].ids.size(), cls[0].smem, c->stream, c->d_jobs, c->d_ids, nsteps);
+    if (resident.empty() && grid.size() == 1) return grid_run(grid[0], c->stream, nsteps);
+    // otherwise fork: classes on the side streams, grid jobs (each a chain
+    // of small launches) round-robin on their own streams, then join
     CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
     for (size_t k = 0; k < cls.size(); ++k) {
         cudaStream_t s = c->side[k % kSideStreams];
         CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
-        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs,
-                             c->d_ids + off[k], nsteps);
+        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs, c->d_ids + off[k],
+                             nsteps);
         if (rc) return rc;
+    }
+    for (size_t g = 0; g < grid.size(); ++g) {
+        cudaStream_t s = c->gside[g % kGridStreams];
+        if (g < (size_t)kGridStreams) CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
+        if ((rc = grid_run(grid[g], s, nsteps))) return rc;
     }
     for (int k = 0; k < kSideStreams && k < (int)cls.size(); ++k) {
         CUDA_TRY(cudaEventRecord(c->ev_join[k], c->side[k]));
         CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_join[k], 0));
+    }
+    for (int k = 0; k < kGridStreams && k < (int)grid.size(); ++k) {
+        CUDA_TRY(cudaEventRecord(c->gev_join[k], c->gside[k]));
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->gev_join[k], 0));
     }
     return SOPB_OK;
 }

@@ -6,12 +6,14 @@
 // limits it to n <= 128 (integrateCholesky_decompose,
 // src/Integrators/bdhitea_kernel.cu:154-190).  Here D is assembled into a
 // row-major matrix with a 32-float aligned leading dimension and factorised
-// in place, lower triangle, by a right-looking blocked algorithm with 128-wide
+// in place, lower triangle, by a right-looking blocked algorithm with 64-wide
 // panels:
-//   k_chol_potrf   the 128 x 128 diagonal block, one CTA in shared memory;
+//   k_chol_potrf   the 64 x 64 diagonal block, one CTA, entries in registers;
 //   k_chol_trsm    the panel below it, L_ik = A_ik L_kk^-T, a warp per row;
 //   k_chol_syrk    the trailing lower triangle, A_ij -= L_ik L_jk^T, in
 //                  128 x 128 output tiles with 8 x 8 FP32 register tiles.
+// The trailing update does nearly all of the (3n)^3/3 flops; the panel
+// kernels sit on the critical path, one panel after the other.
 // The factor is refreshed every `hi_refresh` steps (an updater; 1 = every
 // step, as the reference).  Every step applies it: (L g)_i by a warp per bead
 // over the bead's three rows, D F by the TEA-style tiles, then the move
@@ -23,13 +25,13 @@
 
 namespace sopb {
 
-constexpr int kCholNB = 128;     // panel width
+constexpr int kCholNB = 64;      // panel width
+constexpr int kCholCPL = kCholNB / 32;   // panel columns per lane in the panel solve
 constexpr int kCholLdp = kCholNB + 1;
 constexpr int kCholTile = 128;   // trailing-update output tile
 constexpr int kCholKC = 8;       // K columns staged per round
 
 __host__ __device__ inline int chol_ld(int n) { return (3 * n + 31) & ~31; }
-constexpr size_t kCholPotrfSmem = (size_t)(kCholNB * kCholLdp + kCholNB) * 4;
 constexpr size_t kCholTrsmSmem = (size_t)(kCholNB * kCholLdp + kCholNB) * 4;
 constexpr int kCholMaxBeads = 16384;   // 3n floats of g in shared memory
 
@@ -58,44 +60,66 @@ k_hi_assemble(const JobDev* __restrict__ Jp, GridAux aux) {
     }
 }
 
-// Cholesky of the diagonal block at (k, k), nb <= 128 rows, in shared memory.
-// Column c: every thread reads the pivot d = A_cc and subtracts
-// A_rc A_sc / d from the lower trailing entries it owns, while the scaled
-// column A_rc / sqrt(d) is parked in the unused upper triangle; one barrier
-// per column.  A pivot that is not positive sets the job's status.
-__global__ void __launch_bounds__(256)
+// Cholesky of the diagonal block at (k, k), nb <= 64 rows: 1024 threads,
+// each holding up to 3 entries of the block's packed lower triangle in
+// registers for the whole factorisation.  Column c: the owners of column c
+// publish its entries (double-buffered), one barrier, then every thread
+// finishes its column-c entries (L_cc = sqrt(a_cc), L_rc = a_rc / L_cc) and
+// updates its entries right of c, a_rs -= a_rc a_sc / a_cc.  One barrier per
+// column.  A pivot that is not positive sets the job's status.
+constexpr int kPotrfThreads = 1024;
+constexpr int kPotrfPer = (kCholNB * (kCholNB + 1) / 2 + kPotrfThreads - 1) / kPotrfThreads;
+
+__global__ void __launch_bounds__(kPotrfThreads)
 k_chol_potrf(JobDev* __restrict__ Jp, GridAux aux, int k) {
-    extern __shared__ float A[];   // [kCholNB][kCholLdp], then the pivots' square roots
+    __shared__ float col[2][kCholNB];
     if (Jp->status) return;
     const int m = 3 * Jp->n, ld = aux.ld, nb = min(kCholNB, m - k);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, total = nb * (nb + 1) / 2;
     float* M = aux.tensor + (size_t)k * ld + k;
-    for (int r = warp; r < nb; r += 8)
-        for (int s = lane; s <= r; s += 32) A[r * kCholLdp + s] = M[(size_t)r * ld + s];
-    __syncthreads();
-    float* dg = A + kCholNB * kCholLdp;
+    float a[kPotrfPer];
+    int rs[kPotrfPer];   // row << 8 | column
+#pragma unroll
+    for (int u = 0; u < kPotrfPer; ++u) {
+        const int e = tid + u * kPotrfThreads;
+        int r = (int)((sqrtf(8.f * (float)e + 1.f) - 1.f) * 0.5f);
+        while ((r + 1) * (r + 2) / 2 <= e) ++r;
+        while (r * (r + 1) / 2 > e) --r;
+        const int c = e - r * (r + 1) / 2;
+        rs[u] = e < total ? (r << 8 | c) : -1;
+        a[u] = e < total ? M[(size_t)r * ld + c] : 0.f;
+    }
     int bad = 0;
     for (int c = 0; c < nb; ++c) {
-        const float d = A[c * kCholLdp + c];   // final: column c-1's updates are behind the barrier
-        if (!(d > 0.f)) bad = 1;
-        const float rs = rsqrtf(d), inv = 1.0f / d;
-        for (int r = c + 1 + warp; r < nb; r += 8) {
-            const float arc = A[r * kCholLdp + c];
-            if (lane == 0) A[c * kCholLdp + r] = arc * rs;
-            for (int s = c + 1 + lane; s <= r; s += 32) A[r * kCholLdp + s] -= arc * A[s * kCholLdp + c] * inv;
-        }
-        if (tid == 0) dg[c] = sqrtf(d);
+        float* cb = col[c & 1];
+#pragma unroll
+        for (int u = 0; u < kPotrfPer; ++u)
+            if (rs[u] >= 0 && (rs[u] & 255) == c) cb[rs[u] >> 8] = a[u];
         __syncthreads();
+        const float d = cb[c];
+        if (!(d > 0.f)) bad = 1;
+        const float inv = 1.0f / d, rsd = rsqrtf(d);
+#pragma unroll
+        for (int u = 0; u < kPotrfPer; ++u) {
+            if (rs[u] < 0) continue;
+            const int r = rs[u] >> 8, s = rs[u] & 255;
+            if (s == c) a[u] = r == c ? sqrtf(d) : a[u] * rsd;
+            else if (s > c) a[u] -= cb[r] * cb[s] * inv;
+        }
     }
-    for (int r = warp; r < nb; r += 8)
-        for (int s = lane; s <= r; s += 32) M[(size_t)r * ld + s] = s == r ? dg[r] : A[s * kCholLdp + r];
+#pragma unroll
+    for (int u = 0; u < kPotrfPer; ++u)
+        if (rs[u] >= 0) M[(size_t)(rs[u] >> 8) * ld + (rs[u] & 255)] = a[u];
     if (bad && tid == 0) Jp->status = SOPB_ERR_HI;
 }
 
 // Panel solve below the diagonal block: row r of A[k+nb.., k..k+nb) becomes
-// x with x L_kk^T = a, by forward substitution; a warp per row, lane l holds
-// columns l, l+32, l+64, l+96.  L_kk and its reciprocal diagonal are staged
-// in shared memory once per CTA.
+// x with x L_kk^T = a, by forward substitution.  A warp takes four rows at
+// once (independent chains, one shared read of L per column); lane l holds
+// columns l and l+32 of each.  L_kk and its reciprocal diagonal are
+// staged in shared memory once per CTA.
+constexpr int kTrsmRows = 4;
+
 __global__ void __launch_bounds__(256)
 k_chol_trsm(JobDev* __restrict__ Jp, GridAux aux, int k) {
     extern __shared__ float L[];   // [kCholNB][kCholLdp] + inverse diagonal
@@ -109,31 +133,48 @@ k_chol_trsm(JobDev* __restrict__ Jp, GridAux aux, int k) {
     __syncthreads();
     for (int c = tid; c < nb; c += 256) dinv[c] = 1.0f / L[c * kCholLdp + c];
     __syncthreads();
-    const int warps = gridDim.x * 8;
-    for (int r = k + nb + blockIdx.x * 8 + (tid >> 5); r < m; r += warps) {
-        float* row = aux.tensor + (size_t)r * ld + k;
-        float a[4];
+    const int groups = gridDim.x * 8;
+    for (int r0 = k + nb + (blockIdx.x * 8 + (tid >> 5)) * kTrsmRows; r0 < m; r0 += groups * kTrsmRows) {
+        float a[kTrsmRows][kCholCPL];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) a[u] = lane + 32 * u < nb ? row[lane + 32 * u] : 0.f;
+        for (int q = 0; q < kTrsmRows; ++q)
+#pragma unroll
+            for (int u = 0; u < kCholCPL; ++u)
+                a[q][u] = (r0 + q < m && lane + 32 * u < nb) ? aux.tensor[(size_t)(r0 + q) * ld + k + lane + 32 * u] : 0.f;
         for (int c = 0; c < nb; ++c) {
             const int owner = c & 31, slot = c >> 5;
-            float mine = slot == 0 ? a[0] : slot == 1 ? a[1] : slot == 2 ? a[2] : a[3];
-            const float x = __shfl_sync(0xffffffffu, mine, owner) * dinv[c];
+            float lc[kCholCPL];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < kCholCPL; ++u) {
                 const int cc = lane + 32 * u;
-                if (cc == c) a[u] = x;
-                else if (cc > c && cc < nb) a[u] -= x * L[cc * kCholLdp + c];
+                lc[u] = (cc > c && cc < nb) ? L[cc * kCholLdp + c] : 0.f;
+            }
+            const float di = dinv[c];
+#pragma unroll
+            for (int q = 0; q < kTrsmRows; ++q) {
+                float mine = a[q][0];
+#pragma unroll
+                for (int u = 1; u < kCholCPL; ++u)
+                    if (slot == u) mine = a[q][u];
+                const float x = __shfl_sync(0xffffffffu, mine, owner) * di;
+#pragma unroll
+                for (int u = 0; u < kCholCPL; ++u) {
+                    if (lane + 32 * u == c) a[q][u] = x;
+                    else a[q][u] -= x * lc[u];
+                }
             }
         }
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-            if (lane + 32 * u < nb) row[lane + 32 * u] = a[u];
+        for (int q = 0; q < kTrsmRows; ++q)
+            if (r0 + q < m)
+#pragma unroll
+                for (int u = 0; u < kCholCPL; ++u)
+                    if (lane + 32 * u < nb) aux.tensor[(size_t)(r0 + q) * ld + k + lane + 32 * u] = a[q][u];
     }
 }
 
 // Trailing update of the lower triangle right of the panel:
-// A[i][j] -= sum_c P[i][c] P[j][c] over the panel's columns, 128 x 128 output
+// A[i][j] -= sum_c P[i][c] P[j][c] over the panel's 64 columns, 128 x 128 output
 // tiles (lower tiles only, blockIdx.x enumerates them row by row), 256
 // threads with 8 x 8 outputs each, K staged 8 columns at a time.
 __global__ void __launch_bounds__(256, 2)

@@ -15,8 +15,12 @@ def job_spec(kind, n, seed, hi=False, rng_seed=1):
     extra = {}
     if hi:
         extra = dict(hi_on=1, hi_a=1.9, hi_epsilon_freq=10, hi_capricious=0)
-        if n <= 128:
+        if n <= 1500:
+            # exact HI (Cholesky factor), refreshed every step up to the
+            # reference's 128 beads and every 10 steps above
             extra["hi_exact"] = 1
+            if n > 128:
+                extra["hi_refresh"] = 10
     if kind == "ramp":
         p = plain_params(pulling=1, deltax=0.05, k_trans=0.05, pullFreq=100, fixedEnd=0, pulledEnd=n - 1, **extra)
         return sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[n - 1], seed=rng_seed)

@@ -54,3 +54,26 @@ def test_large_job_on_grid_path(gpu_ctx):
     assert np.array_equal(g.read(sopb.SEEDS), o.read(sopb.SEEDS))
     assert np.max(np.abs(g.read(sopb.COORDS) - o.read(sopb.COORDS))) < 1e-3
     g.destroy()
+
+
+def test_concurrent_grid_jobs_equal_alone(gpu_ctx):
+    # grid-path jobs of one sopb_run execute side by side on their own
+    # streams; each must equal itself run alone (no shared scratch)
+    specs = [spec(100, 11, "clamp", hi_on=1, hi_exact=1, hi_a=1.9, hi_capricious=0),
+             spec(300, 12, "ramp", hi_on=1, hi_exact=1, hi_refresh=10, hi_a=1.9, hi_capricious=0),
+             spec(3000, 13, "clamp", pairs_threshold=30.0, max_possiblePairs=2048),
+             spec(2000, 14, "free", hi_on=1, hi_a=1.9, hi_epsilon_freq=10, hi_capricious=0),
+             spec(250, 15, "clamp")]                       # a resident job beside them
+    alone = []
+    for sp in specs:
+        j = gpu_ctx.job(sp)
+        gpu_ctx.run([j], 60)
+        alone.append(j.read(sopb.COORDS))
+        j.destroy()
+    jobs = [gpu_ctx.job(sp) for sp in specs]
+    for q in (20, 20, 20):
+        gpu_ctx.run(jobs, q)
+    for j, ref in zip(jobs, alone):
+        assert j.status() == 0
+        assert np.array_equal(j.read(sopb.COORDS), ref)
+        j.destroy()

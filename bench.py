@@ -622,7 +622,8 @@ def run_serve(args):
     wall = time.perf_counter() - t0
     summ = sopb_serve.summarize(res, wall)
     # the same jobs alone (a sample): latency without the mix
-    alone = []
+    alone, slow = [], []
+    served = {x.rid: x for x in res}
     for r in reqs[:: max(1, len(reqs) // 16)]:
         j = ctx.job(r.spec)
         ctx.sync()
@@ -630,6 +631,7 @@ def run_serve(args):
         ctx.run([j], r.steps)
         ctx.sync()
         alone.append(time.perf_counter() - ta)
+        slow.append(served[r.rid].latency / alone[-1])
         j.destroy()
     out = {"metric": "bead-steps/s (served Poisson stream)", "value": summ["throughput"], "unit": UNIT,
            "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
@@ -639,7 +641,9 @@ def run_serve(args):
                       "quantum": args.serve_quantum},
            "serve": summ, "peak_inflight": srv.peak_inflight,
            "alone_sample": {"jobs": len(alone), "p50_s": float(np.percentile(alone, 50)),
-                            "p99_s": float(np.percentile(alone, 99))}}
+                            "p99_s": float(np.percentile(alone, 99)),
+                            "slowdown_p50": float(np.percentile(slow, 50)),
+                            "slowdown_p99": float(np.percentile(slow, 99))}}
     print(json.dumps(out), flush=True)
     ctx.close()
     return 0

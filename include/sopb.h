@@ -213,7 +213,8 @@ int sopb_context_destroy(sopb_context* ctx);
  * src/gsop.cuh:13). */
 int sopb_context_set_shape_policy(sopb_context* ctx, int32_t lanes_per_bead, float beads_per_group, int32_t max_block);
 
-/* Blocks until the context's stream drains; returns the first job error. */
+/* Blocks until the context's stream and the streams its jobs last ran on
+ * drain. */
 int sopb_context_sync(sopb_context* ctx);
 
 /* Device bytes a job needs (admission by HBM footprint). */
@@ -234,6 +235,24 @@ int sopb_job_destroy(sopb_job* job);
  * reset, pairlist, heating, TEA), then all potentials are summed and the
  * integrator moves the beads.  Asynchronous on the context stream. */
 int sopb_run(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, int64_t nsteps);
+
+/* sopb_run ordered on `stream` (a cudaStream_t; NULL = the context stream)
+ * instead of the context stream, so groups of jobs advance independently:
+ * a serving loop gives each long job its own stream and polls for
+ * completion instead of waiting for the slowest job of a batch.  A job's
+ * work stays ordered across streams (a run starts after the job's previous
+ * work, wherever it ran).  Reads, writes and sopb_job_destroy of a job are
+ * ordered on the stream it last ran on; destroy does not wait: the job's
+ * memory, bead range and slot are released once its last work finished.
+ * No reference counterpart (the reference runs one job on the default
+ * stream, src/gsop.cu:111-163). */
+int sopb_run_on(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, int64_t nsteps, void* stream);
+
+/* sopb_run_on with a step count per job (nsteps[k] >= 0 for jobs[k]): one
+ * launch serves jobs that need different numbers of steps, each CTA of the
+ * replica-resident kernel stopping at its own job's count.  No reference
+ * counterpart. */
+int sopb_run_ragged(sopb_context* ctx, sopb_job* const* jobs, int32_t njobs, const int64_t* nsteps, void* stream);
 
 /* Device-reported status of a job (after sopb_context_sync). */
 int sopb_job_status(sopb_job* job);

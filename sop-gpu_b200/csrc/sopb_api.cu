@@ -85,18 +85,38 @@ struct sopb_context {
     uint8_t* flags = nullptr;
     RangeAlloc beads;
     JobDev* d_jobs = nullptr;
-    int32_t* d_ids = nullptr;
-    int64_t ids_cap = 0;
+    // job-slot tables of resident launches, one per stream runs are ordered on
+    struct Ids {
+        int32_t* d = nullptr;
+        int64_t cap = 0;
+    };
+    std::map<cudaStream_t, Ids> ids;
+    // bead ranges and slots of destroyed jobs, released once the work that
+    // used them has finished
+    struct Deferred {
+        cudaEvent_t done;
+        int64_t b0;
+        int32_t n;
+        int slot;
+    };
+    std::vector<Deferred> deferred;
+    cudaStream_t upload = nullptr;    // job set-up copies
+    cudaStream_t io = nullptr;        // reads and writes of single jobs
     float4* d_scratch4 = nullptr;
     int64_t scratch4_cap = 0;
     std::vector<sopb_job*> slots;
     std::vector<int> free_slots;
-    cudaStream_t side[kSideStreams] = {};
-    cudaStream_t gside[kGridStreams] = {};
-    cudaEvent_t gev_join[kGridStreams] = {};
+    // fork/join streams of a run, one set per stream priority so a run's
+    // side work keeps the priority of the stream it was ordered on
+    struct Fork {
+        cudaStream_t side[kSideStreams] = {};
+        cudaEvent_t join[kSideStreams] = {};
+        cudaStream_t gside[kGridStreams] = {};
+        cudaEvent_t gjoin[kGridStreams] = {};
+        cudaEvent_t fork = nullptr;
+    };
+    std::map<int, Fork> forks;
     cudaStream_t capture = nullptr;   // CUDA graph capture of grid-path chunks
-    cudaEvent_t ev_fork = nullptr;
-    cudaEvent_t ev_join[kSideStreams] = {};
     int32_t last_error = SOPB_OK;
     int smem_dyn_max = 1 << 30;   // dynamic shared memory available to the resident kernel
     int smem_per_sm = 0;          // shared memory of one SM
@@ -107,6 +127,8 @@ struct sopb_context {
 
 struct sopb_job {
     sopb_context* ctx = nullptr;
+    cudaStream_t st = nullptr;         // the stream the job's last work was ordered on
+    cudaEvent_t ev = nullptr;          // recorded after every piece of the job's work
     int slot = -1;
     int64_t b0 = 0;
     int32_t n = 0;
@@ -131,6 +153,12 @@ struct sopb_job {
                          __FILE__, __LINE__);                                                  \
             return e_ == cudaErrorMemoryAllocation ? SOPB_ERR_NOMEM : SOPB_ERR_CUDA;           \
         }                                                                                      \
+    } while (0)
+
+#define SOPB_TRY(call)           \
+    do {                         \
+        const int r_ = (call);   \
+        if (r_) return r_;       \
     } while (0)
 
 namespace {
@@ -199,8 +227,8 @@ void launch_shape(const ShapePolicy& pol, int32_t n, int32_t lpb_req, int32_t* l
     }
 
 int launch_resident(int block, int grid, size_t smem, cudaStream_t st, JobDev* jobs, const int32_t* ids,
-                    int64_t nsteps) {
-#define L_RES(B) k_resident_steps<B><<<grid, B, smem, st>>>(jobs, ids, nsteps)
+                    const int64_t* steps) {
+#define L_RES(B) k_resident_steps<B><<<grid, B, smem, st>>>(jobs, ids, steps)
     SOPB_BLOCK_SWITCH(block, L_RES)
 #undef L_RES
     CUDA_TRY(cudaGetLastError());
@@ -223,17 +251,80 @@ int launch_rebuild(int block, int grid, cudaStream_t st, JobDev* jobs, const int
     return SOPB_OK;
 }
 
-int ensure_ids(sopb_context* c, int64_t need) {
-    if (need <= c->ids_cap) return SOPB_OK;
-    if (c->d_ids) cudaFreeAsync(c->d_ids, c->stream);
-    int64_t cap = std::max<int64_t>(need, 1024);
-    CUDA_TRY(cudaMallocAsync((void**)&c->d_ids, cap * sizeof(int32_t), c->stream));
-    c->ids_cap = cap;
+// The launch table of resident launches ordered on `st`: `need` job slots
+// (int32) and, after them, as many step counts (int64).  Stream-ordered, so
+// a table is reused only after the launches that read it.
+int ensure_ids(sopb_context* c, cudaStream_t st, int64_t need, int32_t** out, int64_t** steps = nullptr) {
+    sopb_context::Ids& t = c->ids[st];
+    if (need > t.cap) {
+        if (t.d) cudaFreeAsync(t.d, st);
+        const int64_t cap = (std::max<int64_t>(need, 1024) + 1) & ~int64_t(1);   // even: the steps stay 8-B aligned
+        CUDA_TRY(cudaMallocAsync((void**)&t.d, cap * (sizeof(int32_t) + sizeof(int64_t)), st));
+        t.cap = cap;
+    }
+    *out = t.d;
+    if (steps) *steps = reinterpret_cast<int64_t*>(t.d + t.cap);
+    return SOPB_OK;
+}
+
+// The fork/join streams for a run ordered on `st`, at st's priority.
+int fork_set(sopb_context* c, cudaStream_t st, sopb_context::Fork** out) {
+    int prio = 0;
+    CUDA_TRY(cudaStreamGetPriority(st, &prio));
+    auto it = c->forks.find(prio);
+    if (it == c->forks.end()) {
+        sopb_context::Fork f;
+        for (int k = 0; k < kSideStreams; ++k) {
+            CUDA_TRY(cudaStreamCreateWithPriority(&f.side[k], cudaStreamNonBlocking, prio));
+            CUDA_TRY(cudaEventCreateWithFlags(&f.join[k], cudaEventDisableTiming));
+        }
+        for (int k = 0; k < kGridStreams; ++k) {
+            CUDA_TRY(cudaStreamCreateWithPriority(&f.gside[k], cudaStreamNonBlocking, prio));
+            CUDA_TRY(cudaEventCreateWithFlags(&f.gjoin[k], cudaEventDisableTiming));
+        }
+        CUDA_TRY(cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming));
+        it = c->forks.emplace(prio, f).first;
+    }
+    *out = &it->second;
+    return SOPB_OK;
+}
+
+// Releases the bead ranges and slots of destroyed jobs whose last work has
+// finished (all of them when `wait`).
+void reclaim(sopb_context* c, bool wait) {
+    std::vector<sopb_context::Deferred> keep;
+    for (auto& d : c->deferred) {
+        if (wait) cudaEventSynchronize(d.done);
+        if (cudaEventQuery(d.done) == cudaSuccess) {
+            cudaEventDestroy(d.done);
+            c->beads.release(d.b0, d.n);
+            c->free_slots.push_back(d.slot);
+        } else {
+            cudaGetLastError();
+            keep.push_back(d);
+        }
+    }
+    c->deferred.swap(keep);
+}
+
+// The io stream after the job's last work (its work on other streams after
+// that is unrelated); `modify`: the job's next work comes after this io.
+int io_begin(sopb_job* j) {
+    CUDA_TRY(cudaStreamWaitEvent(j->ctx->io, j->ev, 0));
+    return SOPB_OK;
+}
+int io_end(sopb_job* j, bool modify) {
+    sopb_context* c = j->ctx;
+    if (modify) {
+        CUDA_TRY(cudaEventRecord(j->ev, c->io));
+        j->st = c->io;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->io));
     return SOPB_OK;
 }
 
 int read_slot(sopb_job* j) {
-    CUDA_TRY(cudaStreamSynchronize(j->ctx->stream));
+    CUDA_TRY(cudaEventSynchronize(j->ev));
     CUDA_TRY(cudaMemcpy(&j->h, &j->ctx->d_jobs[j->slot], sizeof(JobDev), cudaMemcpyDeviceToHost));
     return SOPB_OK;
 }
@@ -294,16 +385,9 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
     c->beads.init(B);
     c->slots.assign(kJobSlots, nullptr);
     for (int s = kJobSlots - 1; s >= 0; --s) c->free_slots.push_back(s);
-    for (int k = 0; k < kSideStreams; ++k) {
-        CUDA_TRY(cudaStreamCreateWithFlags(&c->side[k], cudaStreamNonBlocking));
-        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_join[k], cudaEventDisableTiming));
-    }
-    for (int k = 0; k < kGridStreams; ++k) {
-        CUDA_TRY(cudaStreamCreateWithFlags(&c->gside[k], cudaStreamNonBlocking));
-        CUDA_TRY(cudaEventCreateWithFlags(&c->gev_join[k], cudaEventDisableTiming));
-    }
     CUDA_TRY(cudaStreamCreateWithFlags(&c->capture, cudaStreamNonBlocking));
-    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->io, cudaStreamNonBlocking));
     int rc;
     int* dm = &c->smem_dyn_max;
     int* ss = c->smem_static;
@@ -322,13 +406,15 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
 extern "C" int sopb_context_destroy(sopb_context* c) {
     if (!c) return SOPB_ERR_INVALID;
     cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
+    cudaDeviceSynchronize();
+    reclaim(c, true);
     for (sopb_job* j : c->slots)
         if (j) {
             if (j->chunk) cudaGraphExecDestroy(j->chunk);
             if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
             if (j->amem) cudaFree(j->amem);
             cudaFree(j->dmem);
+            cudaEventDestroy(j->ev);
             delete j;
         }
     cudaFree(c->x);
@@ -338,18 +424,24 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     cudaFree(c->tipF);
     cudaFree(c->flags);
     cudaFree(c->d_jobs);
-    if (c->d_ids) cudaFree(c->d_ids);
+    for (auto& kv : c->ids)
+        if (kv.second.d) cudaFree(kv.second.d);
     if (c->d_scratch4) cudaFree(c->d_scratch4);
-    for (int k = 0; k < kSideStreams; ++k) {
-        cudaStreamDestroy(c->side[k]);
-        cudaEventDestroy(c->ev_join[k]);
-    }
-    for (int k = 0; k < kGridStreams; ++k) {
-        cudaStreamDestroy(c->gside[k]);
-        cudaEventDestroy(c->gev_join[k]);
+    for (auto& kv : c->forks) {
+        sopb_context::Fork& f = kv.second;
+        for (int k = 0; k < kSideStreams; ++k) {
+            cudaStreamDestroy(f.side[k]);
+            cudaEventDestroy(f.join[k]);
+        }
+        for (int k = 0; k < kGridStreams; ++k) {
+            cudaStreamDestroy(f.gside[k]);
+            cudaEventDestroy(f.gjoin[k]);
+        }
+        cudaEventDestroy(f.fork);
     }
     cudaStreamDestroy(c->capture);
-    cudaEventDestroy(c->ev_fork);
+    cudaStreamDestroy(c->upload);
+    cudaStreamDestroy(c->io);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return SOPB_OK;
@@ -366,7 +458,10 @@ extern "C" int sopb_context_set_shape_policy(sopb_context* c, int32_t lanes_per_
 
 extern "C" int sopb_context_sync(sopb_context* c) {
     if (!c) return SOPB_ERR_INVALID;
+    CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (sopb_job* j : c->slots)
+        if (j) CUDA_TRY(cudaEventSynchronize(j->ev));
     return SOPB_OK;
 }
 
@@ -489,7 +584,7 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
         o_cb = off; off += align256((size_t)n * 4);
         o_bc = off; off += align256((size_t)n * 4);
     }
-    if (cudaMalloc(&j->amem, off) != cudaSuccess) {
+    if (cudaMallocAsync(&j->amem, off, c->upload) != cudaSuccess) {
         cudaGetLastError();
         return SOPB_ERR_NOMEM;
     }
@@ -511,7 +606,7 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
         a.cell_beads = (int32_t*)(b + o_cb);
         a.bead_cell = (int32_t*)(b + o_bc);
     }
-    CUDA_TRY(cudaMemsetAsync(j->amem, 0, off, c->stream));
+    CUDA_TRY(cudaMemsetAsync(j->amem, 0, off, c->upload));
     return SOPB_OK;
 }
 
@@ -687,9 +782,13 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     CUDA_TRY(cudaSetDevice(c->device));
     const int32_t n = d->n;
     const sopb_params& p = d->params;
-    if (c->free_slots.empty()) return SOPB_ERR_NOMEM;
+    reclaim(c, false);
     int64_t b0;
-    if (!c->beads.alloc(n, &b0)) return SOPB_ERR_NOMEM;
+    if (c->free_slots.empty() || !c->beads.alloc(n, &b0)) {
+        reclaim(c, true);   // ranges of destroyed jobs still in use: wait for them
+        if (c->free_slots.empty()) return SOPB_ERR_NOMEM;
+        if (!c->beads.alloc(n, &b0)) return SOPB_ERR_NOMEM;
+    }
 
     HostMaps m;
     build_maps(d, m);
@@ -866,7 +965,9 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     const size_t total = o_plj + align256((size_t)n * h.cap_pl * 4);
     sopb_job* j = new (std::nothrow) sopb_job();
     if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
-    cudaError_t e = cudaMalloc(&j->dmem, total);
+    // stream-ordered allocation: a destroyed job's memory returns to the
+    // pool after its last work, without stalling other streams
+    cudaError_t e = cudaMallocAsync(&j->dmem, total, c->upload);
     if (e != cudaSuccess) {
         cudaGetLastError();
         c->beads.release(b0, n);
@@ -892,7 +993,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.T = c->T + b0;
     h.tipF = c->tipF + b0;
     h.flags = c->flags + b0;
-    cudaStream_t st = c->stream;
+    cudaStream_t st = c->upload;   // set-up copies do not wait for running work
     CUDA_TRY(cudaMemsetAsync(base + o_ppm, 0, o_ppj - o_ppm, st));   // mask and counts
     if (!h.grid) CUDA_TRY(cudaMemcpyAsync(h.ex_mask, ex.data(), mask_bytes, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(h.cov_off, m.cov_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, st));
@@ -915,7 +1016,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     if (h.grid) {
         int rc2 = grid_alloc(c, j, p, n);
         if (rc2) {
-            cudaFree(j->dmem);
+            cudaFreeAsync(j->dmem, c->upload);
             c->beads.release(b0, n);
             delete j;
             return rc2;
@@ -925,6 +1026,9 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     c->free_slots.pop_back();
     CUDA_TRY(cudaMemcpyAsync(&c->d_jobs[slot], &h, sizeof(JobDev), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaStreamSynchronize(st));   // host staging vectors go out of scope
+    CUDA_TRY(cudaEventCreateWithFlags(&j->ev, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventRecord(j->ev, st));
+    j->st = st;
     j->ctx = c;
     j->slot = slot;
     j->b0 = b0;
@@ -939,15 +1043,17 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
 extern "C" int sopb_job_destroy(sopb_job* j) {
     if (!j) return SOPB_ERR_INVALID;
     sopb_context* c = j->ctx;
-    cudaSetDevice(c->device);
-    cudaStreamSynchronize(c->stream);
+    CUDA_TRY(cudaSetDevice(c->device));
+    // nothing waits here: graphs and memory are released after the job's
+    // last work on its stream, the bead range and slot once it has finished
     if (j->chunk) cudaGraphExecDestroy(j->chunk);
     if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
-    if (j->amem) cudaFree(j->amem);
-    cudaFree(j->dmem);
-    c->beads.release(j->b0, j->n);
+    CUDA_TRY(cudaStreamWaitEvent(c->io, j->ev, 0));
+    if (j->amem) CUDA_TRY(cudaFreeAsync(j->amem, c->io));
+    CUDA_TRY(cudaFreeAsync(j->dmem, c->io));
+    CUDA_TRY(cudaEventRecord(j->ev, c->io));
     c->slots[j->slot] = nullptr;
-    c->free_slots.push_back(j->slot);
+    c->deferred.push_back({j->ev, j->b0, j->n, j->slot});
     delete j;
     return SOPB_OK;
 }
@@ -990,58 +1096,114 @@ void group_jobs(const sopb_context* c, sopb_job* const* jobs, int32_t njobs, std
     for (auto& kv : cls) out.push_back(kv.second);
     std::sort(out.begin(), out.end(), [](const LaunchClass& a, const LaunchClass& b) { return a.max_n > b.max_n; });
 }
+int run_ordered(sopb_context* c, sopb_job* const* jobs, int32_t njobs, const int64_t* nsteps, cudaStream_t st);
 }  // namespace
 
-extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, int64_t nsteps) {
-    if (!c || (njobs > 0 && !jobs) || njobs < 0 || nsteps < 0) return SOPB_ERR_INVALID;
-    if (njobs == 0 || nsteps == 0) return SOPB_OK;
+extern "C" int sopb_run_ragged(sopb_context* c, sopb_job* const* jobs, int32_t njobs, const int64_t* nsteps,
+                               void* stream) {
+    if (!c || (njobs > 0 && (!jobs || !nsteps)) || njobs < 0) return SOPB_ERR_INVALID;
+    if (njobs == 0) return SOPB_OK;
     for (int32_t k = 0; k < njobs; ++k)
-        if (!jobs[k] || jobs[k]->ctx != c) return SOPB_ERR_INVALID;
+        if (!jobs[k] || jobs[k]->ctx != c || nsteps[k] < 0) return SOPB_ERR_INVALID;
     CUDA_TRY(cudaSetDevice(c->device));
+    const cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+    // a job that last ran on another stream: this run starts after that work
+    for (int32_t k = 0; k < njobs; ++k) {
+        sopb_job* j = jobs[k];
+        if (j->st != st) {
+            CUDA_TRY(cudaStreamWaitEvent(st, j->ev, 0));
+            j->st = st;
+        }
+    }
+    // jobs with no steps take no part
+    std::vector<sopb_job*> act;
+    std::vector<int64_t> n;
+    for (int32_t k = 0; k < njobs; ++k)
+        if (nsteps[k] > 0) {
+            act.push_back(jobs[k]);
+            n.push_back(nsteps[k]);
+        }
+    int rc = act.empty() ? SOPB_OK : run_ordered(c, act.data(), (int32_t)act.size(), n.data(), st);
+    // the jobs' last work is this run
+    for (int32_t k = 0; k < njobs; ++k) CUDA_TRY(cudaEventRecord(jobs[k]->ev, st));
+    return rc;
+}
+
+extern "C" int sopb_run_on(sopb_context* c, sopb_job* const* jobs, int32_t njobs, int64_t nsteps, void* stream) {
+    if (nsteps < 0 || njobs < 0) return SOPB_ERR_INVALID;
+    std::vector<int64_t> n((size_t)std::max(njobs, 0), nsteps);
+    return sopb_run_ragged(c, jobs, njobs, n.data(), stream);
+}
+
+namespace {
+int run_ordered(sopb_context* c, sopb_job* const* jobs, int32_t njobs, const int64_t* nsteps, cudaStream_t st) {
     std::vector<sopb_job*> resident, grid;
-    for (int32_t k = 0; k < njobs; ++k) (jobs[k]->h.grid ? grid : resident).push_back(jobs[k]);
+    std::vector<int64_t> gsteps;
+    std::map<const sopb_job*, int64_t> steps_of;
+    for (int32_t k = 0; k < njobs; ++k) {
+        if (jobs[k]->h.grid) {
+            grid.push_back(jobs[k]);
+            gsteps.push_back(nsteps[k]);
+        } else {
+            resident.push_back(jobs[k]);
+            steps_of[jobs[k]] = nsteps[k];
+        }
+    }
     // resident jobs: one launch per class; the class table goes up first
     std::vector<LaunchClass> cls;
     std::vector<size_t> off;
+    int32_t* d_ids = nullptr;
+    int64_t* d_steps = nullptr;
     int rc;
     if (!resident.empty()) {
         group_jobs(c, resident.data(), (int32_t)resident.size(), cls);
         std::vector<int32_t> ids;
+        std::vector<int64_t> steps;
         for (auto& L : cls) {
             off.push_back(ids.size());
             ids.insert(ids.end(), L.ids.begin(), L.ids.end());
+            for (int32_t slot : L.ids) steps.push_back(steps_of[c->slots[slot]]);
         }
-        if ((rc = ensure_ids(c, (int64_t)ids.size()))) return rc;
-        CUDA_TRY(cudaMemcpyAsync(c->d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, c->stream));
+        if ((rc = ensure_ids(c, st, (int64_t)ids.size(), &d_ids, &d_steps))) return rc;
+        // (a copy from pageable memory is staged before the call returns)
+        CUDA_TRY(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(d_steps, steps.data(), steps.size() * 8, cudaMemcpyHostToDevice, st));
+        if (grid.empty() && cls.size() == 1)
+            return launch_resident(cls[0].block, (int)cls[0].ids.size(), cls[0].smem, st, c->d_jobs, d_ids, d_steps);
     }
-    // one class or one grid job alone: straight on the context stream
-    if (grid.empty() && cls.size() == 1)
-        return launch_resident(cls[0].block, (int)cls[0].ids.size(), cls[0].smem, c->stream, c->d_jobs, c->d_ids, nsteps);
-    if (resident.empty() && grid.size() == 1) return grid_run(grid[0], c->stream, nsteps);
+    // one grid job alone: straight on the stream
+    if (resident.empty() && grid.size() == 1) return grid_run(grid[0], st, gsteps[0]);
     // otherwise fork: classes on the side streams, grid jobs (each a chain
     // of small launches) round-robin on their own streams, then join
-    CUDA_TRY(cudaEventRecord(c->ev_fork, c->stream));
+    sopb_context::Fork* f = nullptr;
+    if ((rc = fork_set(c, st, &f))) return rc;
+    CUDA_TRY(cudaEventRecord(f->fork, st));
     for (size_t k = 0; k < cls.size(); ++k) {
-        cudaStream_t s = c->side[k % kSideStreams];
-        CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
-        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs, c->d_ids + off[k],
-                             nsteps);
+        cudaStream_t s = f->side[k % kSideStreams];
+        CUDA_TRY(cudaStreamWaitEvent(s, f->fork, 0));
+        rc = launch_resident(cls[k].block, (int)cls[k].ids.size(), cls[k].smem, s, c->d_jobs, d_ids + off[k],
+                             d_steps + off[k]);
         if (rc) return rc;
     }
     for (size_t g = 0; g < grid.size(); ++g) {
-        cudaStream_t s = c->gside[g % kGridStreams];
-        if (g < (size_t)kGridStreams) CUDA_TRY(cudaStreamWaitEvent(s, c->ev_fork, 0));
-        if ((rc = grid_run(grid[g], s, nsteps))) return rc;
+        cudaStream_t s = f->gside[g % kGridStreams];
+        if (g < (size_t)kGridStreams) CUDA_TRY(cudaStreamWaitEvent(s, f->fork, 0));
+        if ((rc = grid_run(grid[g], s, gsteps[g]))) return rc;
     }
     for (int k = 0; k < kSideStreams && k < (int)cls.size(); ++k) {
-        CUDA_TRY(cudaEventRecord(c->ev_join[k], c->side[k]));
-        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_join[k], 0));
+        CUDA_TRY(cudaEventRecord(f->join[k], f->side[k]));
+        CUDA_TRY(cudaStreamWaitEvent(st, f->join[k], 0));
     }
     for (int k = 0; k < kGridStreams && k < (int)grid.size(); ++k) {
-        CUDA_TRY(cudaEventRecord(c->gev_join[k], c->gside[k]));
-        CUDA_TRY(cudaStreamWaitEvent(c->stream, c->gev_join[k], 0));
+        CUDA_TRY(cudaEventRecord(f->gjoin[k], f->gside[k]));
+        CUDA_TRY(cudaStreamWaitEvent(st, f->gjoin[k], 0));
     }
     return SOPB_OK;
+}
+}  // namespace
+
+extern "C" int sopb_run(sopb_context* c, sopb_job* const* jobs, int32_t njobs, int64_t nsteps) {
+    return sopb_run_on(c, jobs, njobs, nsteps, nullptr);
 }
 
 extern "C" int sopb_job_status(sopb_job* j) {
@@ -1076,33 +1238,35 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
     if (!j || !out) return SOPB_ERR_INVALID;
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
+    SOPB_TRY(io_begin(j));
     const size_t n = j->n;
     switch (what) {
     case SOPB_COORDS:
-        CUDA_TRY(cudaMemcpyAsync(out, c->x + j->b0, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(out, c->x + j->b0, n * 16, cudaMemcpyDeviceToHost, c->io));
         break;
     case SOPB_SEEDS:
-        CUDA_TRY(cudaMemcpyAsync(out, c->seeds + j->b0, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(out, c->seeds + j->b0, n * 16, cudaMemcpyDeviceToHost, c->io));
         break;
     case SOPB_TEMP:
-        CUDA_TRY(cudaMemcpyAsync(out, c->T + j->b0, n * 4, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(out, c->T + j->b0, n * 4, cudaMemcpyDeviceToHost, c->io));
         break;
     case SOPB_TIPFORCES:
-        CUDA_TRY(cudaMemcpyAsync(out, c->tipF + j->b0, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(out, c->tipF + j->b0, n * 16, cudaMemcpyDeviceToHost, c->io));
         break;
     case SOPB_FORCES: {
         if ((int64_t)n > c->scratch4_cap) {
-            if (c->d_scratch4) cudaFreeAsync(c->d_scratch4, c->stream);
-            CUDA_TRY(cudaMallocAsync((void**)&c->d_scratch4, n * 16, c->stream));
+            if (c->d_scratch4) cudaFreeAsync(c->d_scratch4, c->io);
+            CUDA_TRY(cudaMallocAsync((void**)&c->d_scratch4, n * 16, c->io));
             c->scratch4_cap = (int64_t)n;
         }
-        int rc = ensure_ids(c, 1);
+        int32_t* d_ids = nullptr;
+        int rc = ensure_ids(c, c->io, 1, &d_ids);
         if (rc) return rc;
         const int32_t id = j->slot;
-        CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
-        rc = launch_forces(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, c->d_scratch4);
+        CUDA_TRY(cudaMemcpyAsync(d_ids, &id, 4, cudaMemcpyHostToDevice, c->io));
+        rc = launch_forces(j->h.block, 1, c->io, c->d_jobs, d_ids, c->d_scratch4);
         if (rc) return rc;
-        CUDA_TRY(cudaMemcpyAsync(out, c->d_scratch4, n * 16, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaMemcpyAsync(out, c->d_scratch4, n * 16, cudaMemcpyDeviceToHost, c->io));
         break;
     }
     case SOPB_PULLSTATE: {
@@ -1128,7 +1292,7 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         if (!j->h.hi || !j->h.hi_exact || !j->aux.tensor) return SOPB_ERR_INVALID;
         const size_t m = 3 * (size_t)n;
         CUDA_TRY(cudaMemcpy2DAsync(out, m * 4, j->aux.tensor, (size_t)j->aux.ld * 4, m * 4, m,
-                                   cudaMemcpyDeviceToHost, c->stream));
+                                   cudaMemcpyDeviceToHost, c->io));
         break;
     }
     case SOPB_TIPSTATE: {
@@ -1146,7 +1310,7 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
     }
     default: return SOPB_ERR_INVALID;
     }
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    SOPB_TRY(io_end(j, false));
     return SOPB_OK;
 }
 
@@ -1154,15 +1318,16 @@ extern "C" int sopb_job_write(sopb_job* j, int32_t what, const void* in) {
     if (!j || !in) return SOPB_ERR_INVALID;
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
+    SOPB_TRY(io_begin(j));
     const size_t n = j->n;
     switch (what) {
-    case SOPB_COORDS: CUDA_TRY(cudaMemcpyAsync(c->x + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->stream)); break;
-    case SOPB_SEEDS: CUDA_TRY(cudaMemcpyAsync(c->seeds + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->stream)); break;
-    case SOPB_TEMP: CUDA_TRY(cudaMemcpyAsync(c->T + j->b0, in, n * 4, cudaMemcpyHostToDevice, c->stream)); break;
-    case SOPB_TIPFORCES: CUDA_TRY(cudaMemcpyAsync(c->tipF + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->stream)); break;
+    case SOPB_COORDS: CUDA_TRY(cudaMemcpyAsync(c->x + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->io)); break;
+    case SOPB_SEEDS: CUDA_TRY(cudaMemcpyAsync(c->seeds + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->io)); break;
+    case SOPB_TEMP: CUDA_TRY(cudaMemcpyAsync(c->T + j->b0, in, n * 4, cudaMemcpyHostToDevice, c->io)); break;
+    case SOPB_TIPFORCES: CUDA_TRY(cudaMemcpyAsync(c->tipF + j->b0, in, n * 16, cudaMemcpyHostToDevice, c->io)); break;
     default: return SOPB_ERR_INVALID;
     }
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    SOPB_TRY(io_end(j, true));
     return SOPB_OK;
 }
 
@@ -1170,12 +1335,13 @@ extern "C" int sopb_job_pairlist(sopb_job* j, int32_t possible, int32_t* counts,
     if (!j || !counts || !rows || cap <= 0) return SOPB_ERR_INVALID;
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
+    SOPB_TRY(io_begin(j));
     const int32_t n = j->n;
     if (j->h.mask && possible) {
         const int32_t W = j->h.W;
         std::vector<uint32_t> msk((size_t)n * W);
-        CUDA_TRY(cudaMemcpyAsync(msk.data(), j->h.pp_mask, msk.size() * 4, cudaMemcpyDeviceToHost, c->stream));
-        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        CUDA_TRY(cudaMemcpyAsync(msk.data(), j->h.pp_mask, msk.size() * 4, cudaMemcpyDeviceToHost, c->io));
+        SOPB_TRY(io_end(j, false));
         for (int32_t i = 0; i < n; ++i) {
             int32_t k = 0;
             for (int32_t q = 0; q < n; ++q)
@@ -1190,9 +1356,9 @@ extern "C" int sopb_job_pairlist(sopb_job* j, int32_t possible, int32_t* counts,
     }
     const int32_t lcap = possible ? j->h.cap_pp : j->h.cap_pl;
     std::vector<int32_t> cnt(n), lst((size_t)n * lcap);
-    CUDA_TRY(cudaMemcpyAsync(cnt.data(), possible ? j->h.pp_cnt : j->h.pl_cnt, (size_t)n * 4, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(lst.data(), possible ? j->h.pp_j : j->h.pl_j, lst.size() * 4, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaMemcpyAsync(cnt.data(), possible ? j->h.pp_cnt : j->h.pl_cnt, (size_t)n * 4, cudaMemcpyDeviceToHost, c->io));
+    CUDA_TRY(cudaMemcpyAsync(lst.data(), possible ? j->h.pp_j : j->h.pl_j, lst.size() * 4, cudaMemcpyDeviceToHost, c->io));
+    SOPB_TRY(io_end(j, false));
     for (int32_t i = 0; i < n; ++i) {
         counts[i] = cnt[i];
         for (int32_t k = 0; k < cap; ++k) rows[(size_t)i * cap + k] = (k < cnt[i] && k < lcap) ? lst[(size_t)i * lcap + k] : -1;
@@ -1204,26 +1370,28 @@ extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t ver
     if (!j) return SOPB_ERR_INVALID;
     sopb_context* c = j->ctx;
     CUDA_TRY(cudaSetDevice(c->device));
+    SOPB_TRY(io_begin(j));
     if (j->h.grid) {
         JobDev* Jp = &c->d_jobs[j->slot];
         int rc = SOPB_OK;
-        if (possible) rc = grid_possible(j, Jp, c->stream, 1);
+        if (possible) rc = grid_possible(j, Jp, c->io, 1);
         if (rc) return rc;
         if (verlet) {
             const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
-            k_g_verlet<<<wb, kGridBlock, 0, c->stream>>>(Jp, 1);
+            k_g_verlet<<<wb, kGridBlock, 0, c->io>>>(Jp, 1);
             CUDA_TRY(cudaGetLastError());
         }
-        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        SOPB_TRY(io_end(j, true));
         return SOPB_OK;
     }
-    int rc = ensure_ids(c, 1);
+    int32_t* d_ids = nullptr;
+    int rc = ensure_ids(c, c->io, 1, &d_ids);
     if (rc) return rc;
     const int32_t id = j->slot;
-    CUDA_TRY(cudaMemcpyAsync(c->d_ids, &id, 4, cudaMemcpyHostToDevice, c->stream));
-    rc = launch_rebuild(j->h.block, 1, c->stream, c->d_jobs, c->d_ids, possible, verlet);
+    CUDA_TRY(cudaMemcpyAsync(d_ids, &id, 4, cudaMemcpyHostToDevice, c->io));
+    rc = launch_rebuild(j->h.block, 1, c->io, c->d_jobs, d_ids, possible, verlet);
     if (rc) return rc;
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    SOPB_TRY(io_end(j, true));
     return SOPB_OK;
 }
 
@@ -1233,6 +1401,14 @@ namespace {
 int bulk_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, void* host, bool up) {
     if (!c || (njobs && !jobs) || !host) return SOPB_ERR_INVALID;
     CUDA_TRY(cudaSetDevice(c->device));
+    // the copies go on the context stream, after each job's last work
+    for (int32_t k = 0; k < njobs; ++k) {
+        sopb_job* j = jobs[k];
+        if (j->st != c->stream) {
+            CUDA_TRY(cudaStreamWaitEvent(c->stream, j->ev, 0));
+            j->st = c->stream;
+        }
+    }
     bool contiguous = true;
     for (int32_t k = 1; k < njobs; ++k)
         if (jobs[k]->b0 != jobs[k - 1]->b0 + jobs[k - 1]->n) contiguous = false;
@@ -1250,6 +1426,8 @@ int bulk_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, void* hos
             h += b;
         }
     }
+    if (up)   // the jobs' next work comes after the upload
+        for (int32_t k = 0; k < njobs; ++k) CUDA_TRY(cudaEventRecord(jobs[k]->ev, c->stream));
     return SOPB_OK;
 }
 }  // namespace

@@ -372,7 +372,8 @@ __host__ __device__ inline size_t resident_smem_bytes(const JobDev& J) {
 // Register cap of 64 per thread: 1024 threads of resident CTAs per SM.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
-k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int64_t nsteps) {
+k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, const int64_t* __restrict__ steps) {
+    const int64_t nsteps = steps[blockIdx.x];   // each job its own number of steps
     JobDev* Jp = &jobs[ids[blockIdx.x]];
     __shared__ JobDev Js;
     load_job<BLOCK>(Js, Jp);

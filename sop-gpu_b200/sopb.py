@@ -91,6 +91,8 @@ def lib() -> C.CDLL:
             "sopb_job_create": ([vp, vp, vp], C.c_int),
             "sopb_job_destroy": ([vp], C.c_int),
             "sopb_run": ([vp, vp, i32, i64], C.c_int),
+            "sopb_run_on": ([vp, vp, i32, i64, vp], C.c_int),
+            "sopb_run_ragged": ([vp, vp, i32, vp, vp], C.c_int),
             "sopb_job_status": ([vp], C.c_int),
             "sopb_job_step": ([vp, vp], C.c_int),
             "sopb_job_size": ([vp, vp], C.c_int),
@@ -286,9 +288,21 @@ class Context:
         arr = (C.c_void_p * len(jobs))(*[j.handle for j in jobs])
         return arr
 
-    def run(self, jobs: Sequence[Job], nsteps: int) -> None:
+    def run(self, jobs: Sequence[Job], nsteps, stream: Optional[int] = None) -> None:
+        """Advances `jobs` by `nsteps` steps (one count for all, or one per
+        job), asynchronously, on the context stream or on `stream` (a
+        cudaStream_t handle, e.g. a torch stream's cuda_stream)."""
         arr = self._handles(jobs)
-        check(lib().sopb_run(self.handle, arr, len(jobs), int(nsteps)), "run")
+        if not np.isscalar(nsteps):
+            n = np.ascontiguousarray(nsteps, np.int64)
+            if n.shape != (len(jobs),):
+                raise ValueError("one step count per job")
+            check(lib().sopb_run_ragged(self.handle, arr, len(jobs), n.ctypes.data, stream), "run_ragged")
+            return
+        if stream is None:
+            check(lib().sopb_run(self.handle, arr, len(jobs), int(nsteps)), "run")
+        else:
+            check(lib().sopb_run_on(self.handle, arr, len(jobs), int(nsteps), stream), "run_on")
 
     def sync(self) -> None:
         check(lib().sopb_context_sync(self.handle), "sync")

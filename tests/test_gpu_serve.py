@@ -36,3 +36,24 @@ def test_admission_by_footprint(gpu_ctx):
     assert srv.peak_used <= budget
     s = sopb_serve.summarize(res, max(r.finished for r in res))
     assert s["ok"] == len(reqs) and s["p99_s"] >= s["p50_s"] > 0
+
+
+def test_ragged_run_equals_separate_runs(gpu_ctx):
+    # one call, a step count per job (resident and grid-path jobs): each job
+    # ends where its own run of that length ends
+    from helpers import spec
+    specs = [spec(120, 3, "clamp"), spec(333, 4, "ramp"), spec(90, 5, "free"),
+             spec(200, 6, "clamp", hi_on=1, hi_a=1.9, hi_epsilon_freq=10, hi_capricious=0)]
+    steps = [37, 120, 0, 64]
+    ref = []
+    for sp, n in zip(specs, steps):
+        j = gpu_ctx.job(sp)
+        gpu_ctx.run([j], n)
+        ref.append((j.read(sopb.COORDS), j.step()))
+        j.destroy()
+    jobs = [gpu_ctx.job(sp) for sp in specs]
+    gpu_ctx.run(jobs, steps)
+    for j, (x, st) in zip(jobs, ref):
+        assert j.step() == st
+        assert np.array_equal(j.read(sopb.COORDS), x)
+        j.destroy()

@@ -18,7 +18,7 @@ Policy = Tuple[int, float, int]   # (lanes per bead, beads per lane group, max C
 
 DEFAULT_CANDIDATES: List[Policy] = [
     (lpb, bpg, maxb)
-    for lpb, bpg, maxb in itertools.product((8, 16, 32), (2.0, 4.0, 8.0), (512, 1024))
+    for lpb, bpg, maxb in itertools.product((4, 8, 16), (1.0, 2.0, 4.0), (1024,))
 ]
 
 

@@ -110,9 +110,13 @@ def test_forces_match_oracle(gpu_ctx, lpb, mode):
     g.destroy()
 
 
-@pytest.mark.parametrize("mode", ["free", "ramp", "clamp", "indent"])
-def test_one_step_matches_oracle(gpu_ctx, mode):
-    g, o = pair(gpu_ctx, spec(200, 13, mode))
+@pytest.mark.parametrize("mode,lpb", [("free", 0), ("ramp", 0), ("clamp", 0), ("indent", 0),
+                                      ("free", 4), ("free", 8), ("free", 16)])
+def test_one_step_matches_oracle(gpu_ctx, mode, lpb):
+    # one step through the resident kernel and its shared-memory list cache
+    # for several lane-group widths: a lost or doubled close pair would move
+    # beads by ~1e-3 A
+    g, o = pair(gpu_ctx, spec(200, 13, mode, lanes_per_bead=lpb))
     gpu_ctx.run([g], 1)
     o.advance(1)
     xg, xo = g.read(sopb.COORDS), o.read(sopb.COORDS)

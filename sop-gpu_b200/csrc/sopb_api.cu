@@ -142,6 +142,8 @@ struct sopb_job {
     cudaGraphExec_t chunk = nullptr;   // one stride chunk: updaters + stride steps
     cudaGraphExec_t chunk_r = nullptr; // the same with the Cholesky refresh at its first step
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
+    cudaStream_t la = nullptr;         // exact HI: the factorisation's second stream
+    cudaEvent_t la_fork = nullptr, la_join = nullptr;
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
 };
 
@@ -397,6 +399,7 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
         return rc;
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholTrsmSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_apply_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kCholMaxBeads * 12));
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
     *out = c;
@@ -412,6 +415,11 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
         if (j) {
             if (j->chunk) cudaGraphExecDestroy(j->chunk);
             if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
+            if (j->la) {
+                cudaStreamDestroy(j->la);
+                cudaEventDestroy(j->la_fork);
+                cudaEventDestroy(j->la_join);
+            }
             if (j->amem) cudaFree(j->amem);
             cudaFree(j->dmem);
             cudaEventDestroy(j->ev);
@@ -598,6 +606,11 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
         a.ci4 = (float4*)(b + o_ci);
         a.eps = (float*)(b + o_eps);
         if (p.hi_exact) a.tensor = (float*)(b + o_ten);
+        if (blocked) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&j->la, cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&j->la_fork, cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&j->la_join, cudaEventDisableTiming));
+        }
     }
     a.cell_geo = (float*)(b + o_geo);
     if (a.use_cells) {
@@ -637,19 +650,33 @@ int grid_possible(sopb_job* j, JobDev* Jp, cudaStream_t st, int force) {
 
 // Updaters of a stride boundary (each gated on the device step), then
 // `steps` Langevin steps, then the step counter moves by `steps`.
-// Exact HI of a job above 128 beads: assemble D and factorise it in place.
+// Exact HI of a job above 128 beads: assemble D and factorise it in place,
+// the panel kernels one panel ahead on the job's look-ahead stream pair.
 int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     GridAux& a = j->aux;
     const int n = j->n, m = 3 * n, sms = j->ctx->sm_count;
-    k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Jp, a);
-    for (int k = 0; k < m; k += kCholNB) {
+    auto panel = [&](int k) {
         k_chol_potrf<<<1, kPotrfThreads, 0, st>>>(Jp, a, k);
-        const int t0 = k + kCholNB;
-        if (t0 >= m) break;
-        const int rows = m - t0;
-        k_chol_trsm<<<std::min((rows + 8 * kTrsmRows - 1) / (8 * kTrsmRows), 2 * sms), 256, kCholTrsmSmem, st>>>(Jp, a, k);
-        const int t = (rows + kCholTile - 1) / kCholTile;
-        k_chol_syrk<<<t * (t + 1) / 2, 256, 0, st>>>(Jp, a, k);
+        const int rows = m - (k + kCholNB);
+        if (rows > 0)
+            k_chol_trsm<<<std::min((rows + 8 * kTrsmRows - 1) / (8 * kTrsmRows), 2 * sms), 256, kCholTrsmSmem, st>>>(
+                Jp, a, k);
+    };
+    k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Jp, a);
+    panel(0);
+    for (int k = 0; k + kCholNB < m; k += kCholNB) {
+        const int t0 = k + kCholNB, rows = m - t0;
+        const int t = (rows + kTcTile - 1) / kTcTile;
+        // the first tile column (the next panels) on the critical path
+        k_chol_syrk_tc<<<t, kTcThreads, kTcSmem, st>>>(Jp, a, k, 1);
+        if (t > 1) {
+            CUDA_TRY(cudaEventRecord(j->la_fork, st));
+            CUDA_TRY(cudaStreamWaitEvent(j->la, j->la_fork, 0));
+            k_chol_syrk_tc<<<t * (t - 1) / 2, kTcThreads, kTcSmem, j->la>>>(Jp, a, k, 2);
+            CUDA_TRY(cudaEventRecord(j->la_join, j->la));
+        }
+        panel(t0);
+        if (t > 1) CUDA_TRY(cudaStreamWaitEvent(st, j->la_join, 0));
     }
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
@@ -1048,6 +1075,11 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     // last work on its stream, the bead range and slot once it has finished
     if (j->chunk) cudaGraphExecDestroy(j->chunk);
     if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
+    if (j->la) {   // released by the runtime once its work is done
+        cudaStreamDestroy(j->la);
+        cudaEventDestroy(j->la_fork);
+        cudaEventDestroy(j->la_join);
+    }
     CUDA_TRY(cudaStreamWaitEvent(c->io, j->ev, 0));
     if (j->amem) CUDA_TRY(cudaFreeAsync(j->amem, c->io));
     CUDA_TRY(cudaFreeAsync(j->dmem, c->io));

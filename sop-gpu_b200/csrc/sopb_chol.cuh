@@ -10,10 +10,14 @@
 // panels:
 //   k_chol_potrf   the 64 x 64 diagonal block, one CTA, entries in registers;
 //   k_chol_trsm    the panel below it, L_ik = A_ik L_kk^-T, a warp per row;
-//   k_chol_syrk    the trailing lower triangle, A_ij -= L_ik L_jk^T, in
-//                  128 x 128 output tiles with 8 x 8 FP32 register tiles.
-// The trailing update does nearly all of the (3n)^3/3 flops; the panel
-// kernels sit on the critical path, one panel after the other.
+//   k_chol_syrk_tc the trailing lower triangle, A_ij -= L_ik L_jk^T, in
+//                  128 x 128 output tiles on the tensor cores (tcgen05,
+//                  TF32 split in hi and lo parts for FP32 accuracy).
+// The trailing update does nearly all of the (3n)^3/3 flops.  The panel
+// kernels sit on the critical path, one panel after the other; they run
+// ahead on a second stream: once the first tile column of the update (which
+// holds the next panel) is done, the next panel is factorised and solved
+// while the rest of the update proceeds.
 // The factor is refreshed every `hi_refresh` steps (an updater; 1 = every
 // step, as the reference).  Every step applies it: (L g)_i by a warp per bead
 // over the bead's three rows, D F by the TEA-style tiles, then the move
@@ -173,82 +177,6 @@ k_chol_trsm(JobDev* __restrict__ Jp, GridAux aux, int k) {
     }
 }
 
-// Trailing update of the lower triangle right of the panel:
-// A[i][j] -= sum_c P[i][c] P[j][c] over the panel's 64 columns, 128 x 128 output
-// tiles (lower tiles only, blockIdx.x enumerates them row by row), 256
-// threads with 8 x 8 outputs each, K staged 8 columns at a time.
-__global__ void __launch_bounds__(256, 2)
-k_chol_syrk(JobDev* __restrict__ Jp, GridAux aux, int k) {
-    __shared__ __align__(16) float As[2][kCholKC][kCholTile + 4];
-    __shared__ __align__(16) float Bs[2][kCholKC][kCholTile + 4];
-    if (Jp->status) return;
-    const int m = 3 * Jp->n, ld = aux.ld, nb = min(kCholNB, m - k), t0 = k + nb;
-    // tile (I, J), I >= J, from the linear index
-    const int b = blockIdx.x;
-    int I = (int)((sqrtf(8.f * (float)b + 1.f) - 1.f) * 0.5f);
-    while ((I + 1) * (I + 2) / 2 <= b) ++I;
-    while (I * (I + 1) / 2 > b) --I;
-    const int Jt = b - I * (I + 1) / 2;
-    const int r0 = t0 + I * kCholTile, c0 = t0 + Jt * kCholTile;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const float* P = aux.tensor + k;
-    // staging: thread loads row (tid >> 1) of the tile, 4 columns at (tid & 1) * 4
-    const int lr = tid >> 1, lc = (tid & 1) * 4;
-    auto fetch = [&](int row0, int kc) -> float4 {
-        const int r = row0 + lr;
-        if (r < m && kc + lc < nb) return *reinterpret_cast<const float4*>(P + (size_t)r * ld + kc + lc);
-        return make_float4(0.f, 0.f, 0.f, 0.f);
-    };
-    float acc[8][8];
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-#pragma unroll
-        for (int v = 0; v < 8; ++v) acc[u][v] = 0.f;
-    float4 pa = fetch(r0, 0), pb = fetch(c0, 0);
-    int buf = 0;
-    for (int kc = 0; kc < nb; kc += kCholKC) {
-        As[buf][lc + 0][lr] = pa.x; As[buf][lc + 1][lr] = pa.y; As[buf][lc + 2][lr] = pa.z; As[buf][lc + 3][lr] = pa.w;
-        Bs[buf][lc + 0][lr] = pb.x; Bs[buf][lc + 1][lr] = pb.y; Bs[buf][lc + 2][lr] = pb.z; Bs[buf][lc + 3][lr] = pb.w;
-        __syncthreads();
-        if (kc + kCholKC < nb) {
-            pa = fetch(r0, kc + kCholKC);
-            pb = fetch(c0, kc + kCholKC);
-        }
-#pragma unroll
-        for (int kk = 0; kk < kCholKC; ++kk) {
-            const float4 a0 = *reinterpret_cast<const float4*>(&As[buf][kk][ty * 4]);
-            const float4 a1 = *reinterpret_cast<const float4*>(&As[buf][kk][64 + ty * 4]);
-            const float4 b0 = *reinterpret_cast<const float4*>(&Bs[buf][kk][tx * 4]);
-            const float4 b1 = *reinterpret_cast<const float4*>(&Bs[buf][kk][64 + tx * 4]);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-#pragma unroll
-                for (int v = 0; v < 8; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
-        }
-        buf ^= 1;
-    }
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-        const int r = r0 + (u < 4 ? ty * 4 + u : 64 + ty * 4 + u - 4);
-        if (r >= m) continue;
-        float* crow = aux.tensor + (size_t)r * ld;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int c = c0 + h * 64 + tx * 4;
-            if (c + 3 < m && c + 3 <= r) {
-                float4 v = *reinterpret_cast<float4*>(crow + c);
-                v.x -= acc[u][4 * h + 0]; v.y -= acc[u][4 * h + 1]; v.z -= acc[u][4 * h + 2]; v.w -= acc[u][4 * h + 3];
-                *reinterpret_cast<float4*>(crow + c) = v;
-            } else {
-                for (int w = 0; w < 4; ++w)
-                    if (c + w < m && c + w <= r) crow[c + w] -= acc[u][4 * h + w];
-            }
-        }
-    }
-}
-
 // D F tiles: partial sums over one slice of j of D_ij F_j, j != i
 // (integrateCholesky_D's product, bdhitea_kernel.cu:130-148).
 __global__ void __launch_bounds__(kHiTile)
@@ -328,6 +256,226 @@ k_chol_apply_rows(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
         }
     }
     (void)m;
+}
+
+}  // namespace sopb
+
+namespace sopb {
+
+// ---- trailing update on the tensor cores (tcgen05, TF32 x3) -----------------
+// A_ij -= P_i P_j^T for one 128 x 128 lower tile, K = the 64 panel columns,
+// on the 5th-generation tensor cores: each FP32 panel value p is split into
+// TF32 p_hi = rn(p) and p_lo = rn(p - p_hi), and P_i P_j^T is accumulated in
+// TMEM as hi.hi + hi.lo + lo.hi (the lo.lo term is below FP32 rounding), so
+// the product keeps FP32 accuracy.  256 threads stage the two 128 x 64
+// operands (hi and lo) into shared memory in the canonical K-major layout
+// without swizzle (8-row x 16-byte core matrices, the 16 K-chunks of a row
+// group 128 B apart, row groups 2048 B apart); one elected thread issues the
+// 24 MMAs (M = N = 128, K = 8 each) and commits them to an mbarrier; the
+// warps read the accumulator from TMEM (warp w: lanes 32 (w mod 4), columns
+// 64 (w / 4) onwards) into shared memory.  The C tile is loaded into
+// registers at the start (16 coalesced float4 loads per thread, in flight
+// while the operands are staged and multiplied) and written back once.
+constexpr int kTcTile = 128;
+constexpr int kTcThreads = 256;
+constexpr int kTcOperandBytes = kTcTile * kCholNB * 4;          // 32 KB
+constexpr int kTcStageLd = kTcTile + 4;                          // accumulator rows in shared memory (float4 aligned)
+constexpr size_t kTcSmem = 4 * (size_t)kTcOperandBytes + 2048;   // + alignment, barrier, TMEM address
+constexpr uint32_t kTcWaitLimit = 1u << 24;
+static_assert(kTcTile * kTcStageLd * 4 <= 4 * kTcOperandBytes, "staged accumulator fits the operand buffers");
+
+__device__ __forceinline__ uint32_t tf32_rn(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t smem_addr) {
+    // start address >> 4 [0,14); leading byte offset 128 >> 4 [16,30);
+    // stride byte offset 2048 >> 4 [32,46); version 1 [46,48); no swizzle
+    return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(2048 >> 4) << 32) |
+           ((uint64_t)1 << 46);
+}
+
+// kind::tf32, D = F32, A = B = TF32, both K-major, N = 128, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+// `part`: 0 every lower tile, 1 the first tile column only (it holds the
+// next panels, which the panel kernels need first), 2 the other columns.
+__global__ void __launch_bounds__(kTcThreads, 1)
+k_chol_syrk_tc(JobDev* __restrict__ Jp, GridAux aux, int k, int part) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    if (Jp->status) return;
+    const int m = 3 * Jp->n, ld = aux.ld, t0 = k + kCholNB;
+    const int b = blockIdx.x;
+    int I, Jt;
+    if (part == 1) {
+        I = b;
+        Jt = 0;
+    } else {
+        I = (int)((sqrtf(8.f * (float)b + 1.f) - 1.f) * 0.5f);
+        while ((I + 1) * (I + 2) / 2 <= b) ++I;
+        while (I * (I + 1) / 2 > b) --I;
+        Jt = b - I * (I + 1) / 2;
+        if (part == 2) {   // lower tiles of the grid without its first column
+            ++I;
+            ++Jt;
+        }
+    }
+    const int r0 = t0 + I * kTcTile, c0 = t0 + Jt * kTcTile;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    // 1024-aligned operand buffers: A hi, A lo, B hi, B lo
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tc_smem);
+    const uint32_t pad = (1024u - (sbase & 1023u)) & 1023u;
+    unsigned char* buf = tc_smem + pad;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(buf + 4 * kTcOperandBytes + 16);
+    const uint32_t sbuf = sbase + pad;
+    const uint32_t s_mbar = sbuf + 4 * kTcOperandBytes;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbuf + 4 * kTcOperandBytes + 16),
+                     "r"(128));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_mbar), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+
+    // the C tile: thread (warp w, lane l) holds rows w + 8 i, columns 4 l .. 4 l + 3
+    float4 cv[kTcTile / 8];
+#pragma unroll
+    for (int i = 0; i < kTcTile / 8; ++i) {
+        const int gr = r0 + warp + 8 * i, gcol = c0 + 4 * lane;
+        // gcol and ld are multiples of 4: gcol < m keeps the float4 inside the row
+        cv[i] = (gr < m && gcol < m) ? *reinterpret_cast<const float4*>(aux.tensor + (size_t)gr * ld + gcol)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // stage the operands: lane = r + 8 cc covers 8 rows x 4 chunks of 16 B;
+    // all of a thread's loads are issued before the conversions
+    const float* P = aux.tensor + k;
+    const int r = lane & 7, cc = lane >> 3;
+    constexpr int kPer = 16 * 4 / (kTcThreads / 32);   // (row group, chunk quad) items per warp
+#pragma unroll
+    for (int op = 0; op < 2; ++op) {
+        const int row0 = op == 0 ? r0 : c0;
+        unsigned char* hi = buf + (2 * op) * kTcOperandBytes;
+        unsigned char* lo = hi + kTcOperandBytes;
+        float4 v[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int it = warp + u * (kTcThreads / 32);
+            const int g = it >> 2, q = it & 3;
+            const int gr = row0 + 8 * g + r;
+            v[u] = gr < m ? *reinterpret_cast<const float4*>(P + (size_t)gr * ld + 4 * (4 * q + cc))
+                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int it = warp + u * (kTcThreads / 32);
+            const int g = it >> 2, q = it & 3;
+            const uint32_t h0 = tf32_rn(v[u].x), h1 = tf32_rn(v[u].y), h2 = tf32_rn(v[u].z), h3 = tf32_rn(v[u].w);
+            const uint32_t l0 = tf32_rn(v[u].x - __uint_as_float(h0)), l1 = tf32_rn(v[u].y - __uint_as_float(h1)),
+                           l2 = tf32_rn(v[u].z - __uint_as_float(h2)), l3 = tf32_rn(v[u].w - __uint_as_float(h3));
+            const int off = g * 2048 + (4 * q + cc) * 128 + r * 16;
+            *reinterpret_cast<uint4*>(hi + off) = make_uint4(h0, h1, h2, h3);
+            *reinterpret_cast<uint4*>(lo + off) = make_uint4(l0, l1, l2, l3);
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0) {
+        const uint32_t a_hi = sbuf, a_lo = sbuf + kTcOperandBytes, b_hi = sbuf + 2 * kTcOperandBytes,
+                       b_lo = sbuf + 3 * kTcOperandBytes;
+        const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+        for (int s = 0; s < kCholNB / 8; ++s) {
+            const uint32_t step = 256u * (uint32_t)s;    // two 16-byte K chunks per K = 8
+            const uint64_t da[3] = {umma_desc_kmajor(a_hi + step), umma_desc_kmajor(a_hi + step),
+                                    umma_desc_kmajor(a_lo + step)};
+            const uint64_t db[3] = {umma_desc_kmajor(b_hi + step), umma_desc_kmajor(b_lo + step),
+                                    umma_desc_kmajor(b_hi + step)};
+            for (int t = 0; t < 3; ++t) {
+                const uint32_t acc = (s > 0 || t > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da[t]), "l"(db[t]), "r"(kTcIdesc), "r"(acc), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_mbar)
+                     : "memory");
+    }
+    // wait for the MMAs (bounded; on expiry the tile is skipped and the job
+    // reports SOPB_ERR_TIMEOUT)
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kTcWaitLimit && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(done)
+            : "r"(s_mbar), "r"(0u)
+            : "memory");
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // accumulator -> shared memory (the A operands are no longer read)
+    float* acc_s = reinterpret_cast<float*>(buf);
+    if (done) {
+        const int lrow = 32 * (warp & 3) + lane;       // TMEM lane = tile row
+        for (int ch = 0; ch < 2; ++ch) {
+            const int col = 64 * (warp >> 2) + 32 * ch;
+            uint32_t v[32];
+            const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 32; e += 4)
+                *reinterpret_cast<float4*>(acc_s + lrow * kTcStageLd + col + e) =
+                    make_float4(__uint_as_float(v[e]), __uint_as_float(v[e + 1]), __uint_as_float(v[e + 2]),
+                                __uint_as_float(v[e + 3]));
+        }
+    } else if (tid == 0) {
+        Jp->status = SOPB_ERR_TIMEOUT;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+    if (!done) return;
+    // C tile update from the registers, lower entries only
+    const int gc = c0 + 4 * lane;
+#pragma unroll
+    for (int i = 0; i < kTcTile / 8; ++i) {
+        const int R = warp + 8 * i, gr = r0 + R;
+        if (gr >= m) continue;
+        const float4 a = *reinterpret_cast<const float4*>(acc_s + R * kTcStageLd + 4 * lane);
+        float4 x = cv[i];
+        x.x -= a.x;
+        x.y -= a.y;
+        x.z -= a.z;
+        x.w -= a.w;
+        float* dst = aux.tensor + (size_t)gr * ld + gc;
+        if (gc + 3 <= gr && gc + 3 < m) {
+            *reinterpret_cast<float4*>(dst) = x;
+        } else {
+            const float xs[4] = {x.x, x.y, x.z, x.w};
+            for (int w = 0; w < 4; ++w)
+                if (gc + w <= gr && gc + w < m) dst[w] = xs[w];
+        }
+    }
 }
 
 }  // namespace sopb

@@ -62,6 +62,10 @@ struct RangeAlloc {
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
+// Skin of the resident jobs' near list (A): the Verlet rebuild filters the
+// possible pairs within pairlist_cutoff + skin instead of scanning them all.
+constexpr float kNearSkin = 4.0f;
+
 // Shape policy of the resident kernel (see launch_shape).
 struct ShapePolicy {
     int32_t lpb = 32;
@@ -797,6 +801,7 @@ extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
     b += align256(n * 4) * 2;                       // counts
     b += align256(n * cap_pp * 4) + align256(n * cap_pl * 4);
     b += n * (16 + 16 + 16 + 4 + 16 + 1);           // bead pools
+    b += align256(n * std::min<int64_t>(n - 1, 2 * cap_pl) * 2) + align256(n * 4) + align256(n * 16);   // near list
     *bytes = b;
     return SOPB_OK;
 }
@@ -843,6 +848,10 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.pp_thr = p.pairs_threshold;
     h.pl_t = sqrt_threshold(p.pairlist_cutoff);
     h.pp_t = sqrt_threshold(p.pairs_threshold);
+    // near list skin: valid while no bead moved more than half of it (less
+    // a margin far above the rounding of the distances)
+    h.nr_t = sqrt_threshold(p.pairlist_cutoff + kNearSkin);
+    h.drift2 = (0.5f * kNearSkin - 0.01f) * (0.5f * kNearSkin - 0.01f);
     h.h = p.timestep;
     h.zeta = p.zeta;
     h.hOverZeta = p.timestep / p.zeta;
@@ -989,7 +998,13 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     const size_t o_plcnt = o_ppcnt + align256((size_t)n * 4);
     const size_t o_ppj = o_plcnt + align256((size_t)n * 4);
     const size_t o_plj = o_ppj + (h.mask ? 0 : align256((size_t)n * h.cap_pp * 4));
-    const size_t total = o_plj + align256((size_t)n * h.cap_pl * 4);
+    // resident jobs: the near list (pairs within pairlist_cutoff + skin,
+    // u16) and the coordinates it was built at
+    h.cap_nr = h.mask ? std::max<int32_t>(1, std::min<int32_t>(n - 1, 2 * h.cap_pl)) : 0;
+    const size_t o_nrj = o_plj + align256((size_t)n * h.cap_pl * 4);
+    const size_t o_nrc = o_nrj + (h.mask ? align256((size_t)n * h.cap_nr * 2) : 0);
+    const size_t o_xref = o_nrc + (h.mask ? align256((size_t)n * 4) : 0);
+    const size_t total = o_xref + (h.mask ? align256((size_t)n * 16) : 0);
     sopb_job* j = new (std::nothrow) sopb_job();
     if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
     // stream-ordered allocation: a destroyed job's memory returns to the
@@ -1014,6 +1029,10 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.pl_cnt = (int32_t*)(base + o_plcnt);
     h.pp_j = h.mask ? nullptr : (int32_t*)(base + o_ppj);
     h.pl_j = (int32_t*)(base + o_plj);
+    h.nr_j = h.mask ? (uint16_t*)(base + o_nrj) : nullptr;
+    h.nr_cnt = h.mask ? (int32_t*)(base + o_nrc) : nullptr;
+    h.x_ref = h.mask ? (float4*)(base + o_xref) : nullptr;
+    h.nr_valid = 0;
     h.x = c->x + b0;
     h.xalt = c->xalt + b0;
     h.seeds = c->seeds + b0;

@@ -64,6 +64,13 @@ struct JobDev {
     int32_t* pl_j;        // [n * cap_pl]
     uint32_t* ex_mask;    // [n * W] bonded + native partners and self
     uint32_t* pp_mask;    // [n * W] possible pairs (MASK mode)
+    uint16_t* nr_j;       // [n * cap_nr] near list: possible pairs within pairlist_cutoff + skin
+    int32_t* nr_cnt;      // [n]
+    float4* x_ref;        // coordinates the near list was built at
+    int32_t cap_nr;       // near-list row capacity
+    int32_t nr_valid;     // 1: the near list holds every pair the next Verlet list can have
+    float nr_t;           // r^2 threshold of the near list
+    float drift2;         // squared displacement since x_ref that invalidates it
     // ---- force field ---------------------------------------------------------
     float ks, R2;         // FENE: kspring_cov, R_limit^2
     float c8, cut2;       // repulsive: -6 el a^6, pairs_cutoff^2

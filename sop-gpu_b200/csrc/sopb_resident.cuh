@@ -84,6 +84,7 @@ struct StepScalars {
     float V, dx;
     float fav[4];
     int32_t err;
+    int32_t nr_valid;   // the job's near list is usable (written back at the end)
 };
 
 // Cooperative copy of a job descriptor into shared memory (read by every
@@ -191,9 +192,12 @@ __device__ void build_possible(const JobDev& J, const float4* __restrict__ xs, i
 // with |r| < pairlist_cutoff, in increasing j (the reference's order), as
 // index rows.  A warp takes one bead: the possible-pairs words are held two
 // per lane (W <= 64), lane b tests candidate 32w+b and a ballot places the
-// hits.  A row longer than its capacity sets err.
+// hits.  The same scan writes the near list -- the possible pairs within
+// pairlist_cutoff + skin, also in increasing j -- for the cheaper rebuilds
+// that follow (build_verlet_near).  A Verlet row longer than its capacity
+// sets err; a near row longer than its capacity sets *near_over.
 template <int BLOCK>
-__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int& err) {
+__device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int& err, int* near_over) {
     static_assert(kMaxResidentBeads <= 64 * 32, "two mask words per lane");
     const int n = J.n, W = J.W, lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -203,11 +207,54 @@ __device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int
         const uint32_t m0 = lane < W ? pm[lane] : 0u;
         const uint32_t m1 = lane + 32 < W ? pm[lane + 32] : 0u;
         int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
-        int cnt = 0;
+        uint16_t* nrow = J.nr_j + (size_t)i * J.cap_nr;
+        int cnt = 0, ncnt = 0;
         for (int w = 0; w < W; ++w) {
             const uint32_t m = __shfl_sync(0xffffffffu, w < 32 ? m0 : m1, w & 31);
             const int q = 32 * w + lane;
-            const bool ok = ((m >> lane) & 1u) && q < n && within_cutoff(xi, xs[q], J.pl_t);
+            const bool cand = ((m >> lane) & 1u) && q < n;
+            const float r2 = cand ? dist2_rn(xi, xs[q]) : 0.f;
+            const bool ok = cand && r2 < J.pl_t, nok = cand && r2 < J.nr_t;
+            const uint32_t hit = __ballot_sync(0xffffffffu, ok), nhit = __ballot_sync(0xffffffffu, nok);
+            if (ok) {
+                const int pos = cnt + __popc(hit & below);
+                if (pos < J.cap_pl) row[pos] = q;
+            }
+            if (nok) {
+                const int pos = ncnt + __popc(nhit & below);
+                if (pos < J.cap_nr) nrow[pos] = (uint16_t)q;
+            }
+            cnt += __popc(hit);
+            ncnt += __popc(nhit);
+        }
+        if (lane == 0) {
+            if (cnt > J.cap_pl) err = SOPB_STATUS_CAPACITY;
+            J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
+            if (ncnt > J.cap_nr) atomicOr(near_over, 1);
+            J.nr_cnt[i] = ncnt < J.cap_nr ? ncnt : J.cap_nr;
+        }
+    }
+}
+
+// The Verlet list from the near list: while no bead moved more than half the
+// skin since the near list was built, every pair now closer than
+// pairlist_cutoff was closer than pairlist_cutoff + skin then, so filtering
+// the near rows (increasing j) with the same exact test gives the same rows
+// as the full scan.  A warp per bead, lanes over 32 near entries at a time.
+template <int BLOCK>
+__device__ void build_verlet_near(const JobDev& J, const float4* __restrict__ xs, int& err) {
+    const int n = J.n, lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    for (int i = threadIdx.x >> 5; i < n; i += BLOCK / 32) {
+        const float4 xi = xs[i];
+        const uint16_t* nrow = J.nr_j + (size_t)i * J.cap_nr;
+        const int ncnt = J.nr_cnt[i];
+        int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
+        int cnt = 0;
+        for (int kb = 0; kb < ncnt; kb += 32) {
+            const int k = kb + lane;
+            const int q = k < ncnt ? nrow[k] : 0;
+            const bool ok = k < ncnt && within_cutoff(xi, xs[q], J.pl_t);
             const uint32_t hit = __ballot_sync(0xffffffffu, ok);
             if (ok) {
                 const int pos = cnt + __popc(hit & below);
@@ -220,6 +267,35 @@ __device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int
             J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
         }
     }
+}
+
+// Verlet rebuild of a resident job: from the near list when it is valid and
+// no bead drifted more than half the skin from where it was built, else a
+// full scan that also rebuilds the near list at the current coordinates.
+template <int BLOCK>
+__device__ void rebuild_verlet(const JobDev& J, const float4* __restrict__ xs, int& valid, bool possible_changed,
+                               int& err) {
+    __shared__ int drift_bits, near_over;
+    const int tid = threadIdx.x, n = J.n;
+    if (tid == 0) {
+        drift_bits = 0;
+        near_over = 0;
+    }
+    __syncthreads();
+    if (valid && !possible_changed) {
+        float d2 = 0.f;
+        for (int i = tid; i < n; i += BLOCK) d2 = fmaxf(d2, dist2_rn(J.x_ref[i], xs[i]));
+        if (d2 > 0.f) atomicMax(&drift_bits, __float_as_int(d2));   // non-negative floats order as ints
+    }
+    __syncthreads();
+    if (valid && !possible_changed && __int_as_float(drift_bits) < J.drift2) {
+        build_verlet_near<BLOCK>(J, xs, err);
+        return;
+    }
+    build_verlet<BLOCK>(J, xs, err, &near_over);
+    for (int i = tid; i < n; i += BLOCK) J.x_ref[i] = xs[i];
+    __syncthreads();
+    valid = near_over ? 0 : 1;
 }
 
 // Deterministic CTA sum of a float3 (fixed tree for a given BLOCK).
@@ -353,7 +429,9 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
     const bool verlet = step % J.pairs_freq == 0;
     if (verlet) {
         if (pp) __syncthreads();
-        build_verlet<BLOCK>(J, xs, err);
+        int valid = sc.nr_valid;
+        rebuild_verlet<BLOCK>(J, xs, valid, pp, err);
+        if (tid == 0) sc.nr_valid = valid;
     }
     if (J.heating && tid == 0 && step % J.temp_freq == 0) {
         // TemperatureUpdater (src/Integrators/langevin.cu:129-135, 44-48)
@@ -430,6 +508,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
         sc.V = J.V; sc.dx = J.dx;
         for (int c = 0; c < 4; ++c) sc.fav[c] = J.fav[c];
         sc.err = 0;
+        sc.nr_valid = J.nr_valid;
     }
     __syncthreads();
     const int cap = J.lcache;
@@ -521,6 +600,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
         Jp->V = sc.V;
         Jp->dx = sc.dx;
         for (int c = 0; c < 4; ++c) Jp->fav[c] = sc.fav[c];
+        Jp->nr_valid = sc.nr_valid;
         if (sc.err) Jp->status = sc.err;
     }
 }
@@ -573,7 +653,13 @@ k_rebuild_lists(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, int 
     int err = 0;
     if (possible) build_possible<BLOCK>(J, J.x, err);
     __syncthreads();
-    if (verlet) build_verlet<BLOCK>(J, J.x, err);
+    if (verlet) {
+        int valid = 0;                      // a full scan, which also renews the near list
+        rebuild_verlet<BLOCK>(J, J.x, valid, true, err);
+        if (threadIdx.x == 0) Jp->nr_valid = valid;
+    } else if (possible && threadIdx.x == 0) {
+        Jp->nr_valid = 0;                   // the near list no longer matches the possible pairs
+    }
     if (err) atomicMax(&errs, err);
     __syncthreads();
     if (threadIdx.x == 0 && errs) Jp->status = errs;

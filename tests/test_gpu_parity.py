@@ -96,6 +96,29 @@ def test_lists_bit_exact_within_ulps_of_the_cutoff(gpu_ctx, cut):
     g.destroy()
 
 
+@pytest.mark.parametrize("n,shift", [(200, 0.0), (450, 0.0), (200, 2.5)])
+def test_verlet_rebuild_from_near_list_is_exact(gpu_ctx, n, shift):
+    # rebuilds after the first filter the near list (pairs within the
+    # cutoff plus a skin); the rows must equal a full scan of the same
+    # coordinates, and a displacement beyond half the skin must force the
+    # full scan again
+    sp = spec(n, 31, "clamp")
+    g = gpu_ctx.job(sp)
+    gpu_ctx.run([g], 30)                      # rebuilds at 0 (full), 10, 20
+    x = g.read(sopb.COORDS)
+    if shift:
+        x[n // 2:, 0] += shift                   # half of the beads jump
+        g.write(sopb.COORDS, x)
+    gpu_ctx.run([g], 1)                       # rebuild at step 30 from x
+    o = O.OracleJob(sp)
+    o.write(sopb.COORDS, x)
+    o.rebuild(True, True)
+    cg, rg = g.pairlist(False)
+    co, ro = o.pairlist(False)
+    assert np.array_equal(cg, co) and np.array_equal(rg, ro)
+    g.destroy()
+
+
 @pytest.mark.parametrize("lpb", [1, 2, 4, 8, 32])
 @pytest.mark.parametrize("mode", ["free", "indent"])
 def test_forces_match_oracle(gpu_ctx, lpb, mode):

@@ -231,6 +231,20 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def reduce_over_ranks(dist, bead_steps, seconds, device):
+    """Whole-job totals of a replicas-only run: every rank's bead-steps summed
+    and the slowest rank's time (each rank owns its own batch, so the job
+    ends when the last rank does).  `dist` is None on one process."""
+    if dist is None:
+        return float(bead_steps), float(seconds)
+    import torch
+    t = torch.tensor([float(bead_steps), float(seconds)], dtype=torch.float64, device=device)
+    s = t.clone()
+    dist.all_reduce(s[:1], op=dist.ReduceOp.SUM)
+    dist.all_reduce(t[1:], op=dist.ReduceOp.MAX)
+    return float(s[0].item()), float(t[1].item())
+
+
 def run_gpu(args):
     import torch
     import sopb
@@ -299,13 +313,10 @@ def run_gpu(args):
     if dist:
         dist.barrier()
     ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = sum(ms)
-    if dist:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
     bead_steps = beads * chunk * args.steps
-    value = world * bead_steps / (total_ms / 1e3)
+    all_bead_steps, total_s = reduce_over_ranks(dist, bead_steps, sum(ms) / 1e3, dev)
+    total_ms = total_s * 1e3
+    value = all_bead_steps / total_s
     launches = len(classes) * args.steps
 
     # e2e through the C ABI with host buffers
@@ -321,12 +332,8 @@ def run_gpu(args):
         one()
         ctx.download_coords(jobs, host_np)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * bead_steps / e2e_s
+    _, e2e_s = reduce_over_ranks(dist, bead_steps, time.perf_counter() - t0, dev)
+    e2e = all_bead_steps / e2e_s
     for j in jobs:
         if j.status() != 0:
             raise RuntimeError("job failed: status %d" % j.status())

@@ -129,7 +129,8 @@ typedef struct sopb_params {
     int32_t lanes_per_bead;    /* 0 = autotuned                                */
     int32_t cell_list;         /* possible pairs by cell list: 0 auto, 1 on, 2 off */
     int32_t grid_path;         /* 0 auto (resident kernel when it fits), 1 grid */
-    int32_t reserved[5];
+    float R_limit_bond;        /* 8: a native contact within it counts intact   */
+    int32_t reserved[4];
 } sopb_params;
 
 /*
@@ -170,9 +171,15 @@ enum {
     SOPB_PULLSTATE = 5,/* float[12]  extForce[3] cant[3] cant0[3] vec[3]      */
     SOPB_TIPSTATE = 6, /* float[16]  tip[3] chip[3] micaR[3] V dx fav[4] pad  */
     SOPB_HISTATE = 7,  /* float[4]   TEA beta', epsilon (computeTEAeps), 0, 0 */
-    SOPB_HIFACTOR = 8  /* float[9n^2] exact HI: the (3n)^2 tensor, row-major, */
+    SOPB_HIFACTOR = 8, /* float[9n^2] exact HI: the (3n)^2 tensor, row-major, */
                        /*            its lower triangle the Cholesky factor L */
                        /*            of D at the last refresh (read only)     */
+    SOPB_OBSERVABLES = 9 /* double[8] the .dat columns of the output manager,  */
+                       /* computed on the device at the current coordinates: */
+                       /* T (averaged over beads and the nav window), FENE,  */
+                       /* native and repulsive energies, their total, intact */
+                       /* native contacts, Rg, TEA epsilon (0 without TEA)   */
+                       /* (src/Updaters/output_manager.cu:73-222) (read only) */
 };
 
 /* ---- host utilities ---------------------------------------------------- */

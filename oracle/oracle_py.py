@@ -49,6 +49,7 @@ def lib() -> C.CDLL:
             "orc_job_write": ([vp, i32, vp], None),
             "orc_job_rebuild": ([vp, i32, i32], None),
             "orc_job_pairlist": ([vp, i32, vp, vp, i32], None),
+            "orc_job_observables": ([vp, vp], None),
             "orc_rpy_tensor": ([i32, vp, C.c_float, vp], None),
             "orc_cholesky_ref": ([i32, vp], None),
             "orc_ref_b_matrix": ([i32, vp, vp], None),
@@ -133,6 +134,12 @@ class OracleJob:
         rows = np.zeros((self.n, cap), np.int32)
         lib().orc_job_pairlist(self.h, int(possible), counts.ctypes.data, rows.ctypes.data, cap)
         return counts, rows
+
+    def observables(self) -> np.ndarray:
+        """T, E_fene, E_native, E_pairs, E_total, native contacts, Rg, TEA eps."""
+        out = np.zeros(8, np.float64)
+        lib().orc_job_observables(self.h, out.ctypes.data)
+        return out
 
     def close(self) -> None:
         if self.h:

@@ -1116,3 +1116,73 @@ void orc_job_pairlist(const orc_job* j, int32_t possible, int32_t* counts, int32
             rows[(size_t)i * cap + k] = (k < cnt[i] && k < lcap) ? lst[(size_t)i * lcap + k] : -1;
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Observables (src/Updaters/output_manager.cu:73-222)                       */
+/* ------------------------------------------------------------------------ */
+void orc_job_observables(const orc_job* j, double* out) {
+    const int32_t n = j->n;
+    const float R_limit = sqrtf(j->R2);
+    const float rlb = j->p.R_limit_bond > 0.0f ? j->p.R_limit_bond : 8.0f;
+    double efene = 0.0, enat = 0.0, epair = 0.0, tsum = 0.0, rg = 0.0;
+    int contacts = 0;
+    for (int32_t i = 0; i < n; i++) {
+        const float* xi = F4(j->x, i);
+        /* covalentEnergy_kernel (covalent_kernel.cu:57-78) */
+        float pot = 0.0f;
+        for (int32_t k = 0; k < j->cov_cnt[i]; k++) {
+            const size_t s = (size_t)i * j->cap_cov + k;
+            const float* xj = F4(j->x, j->cov_j[s]);
+            float dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+            float d = sqrtf(dx * dx + dy * dy + dz * dz) - j->cov_r0[s];
+            pot -= 0.5f * j->ks * j->R2 * logf(1.0f - d * d / j->R2);
+        }
+        efene += pot;
+        /* nativeEnergy_kernel (native_kernel.cu:57-82) */
+        pot = 0.0f;
+        for (int32_t k = 0; k < j->nat_cnt[i]; k++) {
+            const size_t s = (size_t)i * j->cap_nat + k;
+            const int32_t q = j->nat_j[s];
+            const float* xj = F4(j->x, q);
+            float dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+            float r2 = dx * dx + dy * dy + dz * dz;
+            float w = j->nat_r02[s] / r2, p6 = w * w * w;
+            pot += (-j->nat_m12[s] * j->nat_r02[s] / 12.0f) * (p6 * p6 - 2.0f * p6);
+            /* computeNativeCounts (output_manager.cu:166-186): each contact once */
+            if (q > i) {
+                float dr = sqrtf(r2);
+                if (dr < rlb || fabsf(sqrtf(j->nat_r02[s]) - dr) <= R_limit) contacts++;
+            }
+        }
+        enat += pot;
+        /* pairsEnergy_kernel (pairs_kernel.cu:69-91) */
+        pot = 0.0f;
+        for (int32_t k = 0; k < j->pl_cnt[i]; k++) {
+            const float* xj = F4(j->x, j->pl_j[(size_t)i * j->cap_pl + k]);
+            float dx = xj[0] - xi[0], dy = xj[1] - xi[1], dz = xj[2] - xi[2];
+            float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 < j->cut2) {
+                float w = j->a2 / r2;
+                pot += j->p.el * w * w * w;
+            }
+        }
+        epair += pot;
+        tsum += j->T[i];
+        /* computeRg_kernel (output_manager_kernel.cu:14-31) */
+        float g = 0.0f;
+        for (int32_t q = 0; q < i; q++) {
+            const float* xq = F4(j->x, q);
+            float dx = xq[0] - xi[0], dy = xq[1] - xi[1], dz = xq[2] - xi[2];
+            g += dx * dx + dy * dy + dz * dz;
+        }
+        rg += g;
+    }
+    out[0] = tsum / ((double)n * (double)j->p.nav);
+    out[1] = efene * 0.5;
+    out[2] = enat * 0.5;
+    out[3] = epair * 0.5;
+    out[4] = out[1] + out[2] + out[3];
+    out[5] = contacts;
+    out[6] = sqrt(rg / ((double)n * (double)n));
+    out[7] = (j->p.hi_on && !j->p.hi_exact) ? (double)j->epsilon : 0.0;
+}

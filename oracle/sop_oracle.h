@@ -50,6 +50,11 @@ void orc_job_read(const orc_job* job, int32_t what, void* out);
 void orc_job_write(orc_job* job, int32_t what, const void* in);
 void orc_job_rebuild(orc_job* job, int32_t possible, int32_t verlet);
 void orc_job_pairlist(const orc_job* job, int32_t possible, int32_t* counts, int32_t* rows, int32_t cap);
+/* The output manager's .dat quantities at the current coordinates
+ * (src/Updaters/output_manager.cu:73-222, the energy kernels and
+ * SOPPotential::sumEnergies): T, E_fene, E_native, E_pairs, E_total,
+ * intact native contacts, Rg, TEA epsilon (0 without TEA). */
+void orc_job_observables(const orc_job* job, double* out8);
 
 /* Exact-HI helpers (src/Integrators/bdhitea_kernel.cu:89-190). */
 /* Normalised RPY tensor D (3n x 3n, row-major) at coords xyz[3n]. */

@@ -17,6 +17,7 @@
 #include "sopb_grid.cuh"
 #include "sopb_hi.cuh"
 #include "sopb_chol.cuh"
+#include "sopb_obs.cuh"
 
 using namespace sopb;
 
@@ -851,6 +852,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     // near list skin: valid while no bead moved more than half of it (less
     // a margin far above the rounding of the distances)
     h.nr_t = sqrt_threshold(p.pairlist_cutoff + kNearSkin);
+    h.rlb = p.R_limit_bond > 0.0f ? p.R_limit_bond : 8.0f;
     h.drift2 = (0.5f * kNearSkin - 0.01f) * (0.5f * kNearSkin - 0.01f);
     h.h = p.timestep;
     h.zeta = p.zeta;
@@ -1344,6 +1346,19 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         const size_t m = 3 * (size_t)n;
         CUDA_TRY(cudaMemcpy2DAsync(out, m * 4, j->aux.tensor, (size_t)j->aux.ld * 4, m * 4, m,
                                    cudaMemcpyDeviceToHost, c->io));
+        break;
+    }
+    case SOPB_OBSERVABLES: {
+        // per-CTA partials and the 8 results, stream-ordered scratch on io
+        const int nb = (int)std::min<int64_t>(((int64_t)n + kObsBlock - 1) / kObsBlock, (int64_t)c->sm_count * 4);
+        double* d = nullptr;
+        CUDA_TRY(cudaMallocAsync((void**)&d, ((size_t)nb * kObsTerms + 8) * sizeof(double), c->io));
+        JobDev* Jp = &c->d_jobs[j->slot];
+        k_obs_partial<<<nb, kObsBlock, 0, c->io>>>(Jp, d);
+        k_obs_final<<<1, 32, 0, c->io>>>(Jp, d, nb, d + (size_t)nb * kObsTerms);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(out, d + (size_t)nb * kObsTerms, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->io));
+        CUDA_TRY(cudaFreeAsync(d, c->io));
         break;
     }
     case SOPB_TIPSTATE: {

@@ -71,6 +71,7 @@ struct JobDev {
     int32_t nr_valid;     // 1: the near list holds every pair the next Verlet list can have
     float nr_t;           // r^2 threshold of the near list
     float drift2;         // squared displacement since x_ref that invalidates it
+    float rlb;            // R_limit_bond: native contacts closer than it count intact
     // ---- force field ---------------------------------------------------------
     float ks, R2;         // FENE: kspring_cov, R_limit^2
     float c8, cut2;       // repulsive: -6 el a^6, pairs_cutoff^2

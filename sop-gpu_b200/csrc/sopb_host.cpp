@@ -34,6 +34,7 @@ extern "C" void sopb_default_params(sopb_params* p) {
     p->temperature = 0.6f;
     p->kspring_cov = 20.0f;
     p->R_limit = 2.0f;
+    p->R_limit_bond = 8.0f;
     p->a = 3.8f;
     p->el = 1.0f;
     p->pairs_cutoff = 20.0f;

@@ -334,6 +334,7 @@ void Simulation::initFF() {
     p.temperature = g.real("temperature", p.temperature);
     p.kspring_cov = g.real("kspring_cov", p.kspring_cov);
     p.R_limit = g.real("R_limit", p.R_limit);
+    p.R_limit_bond = g.real("R_limit_bond", p.R_limit_bond);
     p.a = g.real("a", p.a);
     p.el = g.real("el", p.el);
     p.pairs_cutoff = g.real("pairs_cutoff", p.pairs_cutoff);

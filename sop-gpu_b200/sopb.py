@@ -19,7 +19,8 @@ LIB_PATH = os.path.join(HERE, "libsopb.so")
 OK, ERR_INVALID, ERR_CAPACITY, ERR_NONFINITE, ERR_CUDA, ERR_TIMEOUT, ERR_NOMEM, ERR_UNSUPPORTED, ERR_HI, ERR_NODEVICE = range(10)
 PULL_END_TO_END, PULL_VECTOR = 0, 1
 HI_B_CHOLESKY, HI_B_REFCOMPAT = 0, 1
-COORDS, SEEDS, TEMP, FORCES, TIPFORCES, PULLSTATE, TIPSTATE, HISTATE, HIFACTOR = range(9)
+COORDS, SEEDS, TEMP, FORCES, TIPFORCES, PULLSTATE, TIPSTATE, HISTATE, HIFACTOR, OBSERVABLES = range(10)
+OBSERVABLE_NAMES = ("T", "E_fene", "E_native", "E_pairs", "E_total", "native_contacts", "Rg", "tea_eps")
 
 F3 = C.c_float * 3
 
@@ -51,8 +52,8 @@ class Params(C.Structure):
         ("hi_on", C.c_int32), ("hi_exact", C.c_int32), ("hi_a", C.c_float), ("hi_epsilon_freq", C.c_int32),
         ("hi_capricious", C.c_int32), ("hi_unlisted", C.c_int32), ("hi_epsmax", C.c_float),
         ("hi_b_mode", C.c_int32), ("hi_refresh", C.c_int32), ("lanes_per_bead", C.c_int32),
-        ("cell_list", C.c_int32), ("grid_path", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("cell_list", C.c_int32), ("grid_path", C.c_int32), ("R_limit_bond", C.c_float),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -222,7 +223,7 @@ class Job:
         shapes = {COORDS: ((self.n, 4), np.float32), SEEDS: ((self.n, 4), np.uint32), TEMP: ((self.n,), np.float32),
                   FORCES: ((self.n, 4), np.float32), TIPFORCES: ((self.n, 4), np.float32),
                   PULLSTATE: ((12,), np.float32), TIPSTATE: ((16,), np.float32), HISTATE: ((4,), np.float32),
-                  HIFACTOR: ((3 * self.n, 3 * self.n), np.float32)}
+                  HIFACTOR: ((3 * self.n, 3 * self.n), np.float32), OBSERVABLES: ((8,), np.float64)}
         shape, dt = shapes[what]
         out = np.zeros(shape, dt)
         check(lib().sopb_job_read(self.handle, what, out.ctypes.data), "job_read")

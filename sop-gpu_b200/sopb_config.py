@@ -146,7 +146,7 @@ def job_config(cfg: Config) -> JobConfig:
     else:
         ntr, firstrun = 1, run
     p.timestep = g.get_float("timestep")
-    for k in ("zeta", "temperature", "kspring_cov", "R_limit", "a", "el", "pairs_cutoff", "pairlist_cutoff",
+    for k in ("zeta", "temperature", "kspring_cov", "R_limit", "R_limit_bond", "a", "el", "pairs_cutoff", "pairlist_cutoff",
               "pairs_threshold", "k_trans", "hi_a", "hi_epsmax"):
         setattr(p, k, g.get_float(k, getattr(p, k)))
     for k in ("pairs_freq", "possiblepairs_freq", "max_pairs", "max_possiblePairs", "nav"):

@@ -130,7 +130,9 @@ typedef struct sopb_params {
     int32_t cell_list;         /* possible pairs by cell list: 0 auto, 1 on, 2 off */
     int32_t grid_path;         /* 0 auto (resident kernel when it fits), 1 grid */
     float R_limit_bond;        /* 8: a native contact within it counts intact   */
-    int32_t reserved[4];
+    int32_t log_rows;          /* event-log ring of a pulling (deltax != 0) or  */
+                               /* indentation job, rows; a power of two, 0 = 1024 */
+    int32_t reserved[3];
 } sopb_params;
 
 /*
@@ -288,6 +290,37 @@ int sopb_job_pairlist(sopb_job* job, int32_t possible, int32_t* counts, int32_t*
 /* Rebuilds the possible-pairs list and/or the pairlist of a job now
  * (PossiblepairList::update / PairList::update without the step gate). */
 int sopb_job_rebuild_lists(sopb_job* job, int32_t possible, int32_t verlet);
+
+/* ---- event log --------------------------------------------------------
+ * The reference's pulling and indentation updaters print one line per
+ * update from the host (src/Potentials/pulling.cu:167-190,
+ * src/Potentials/indentation.cu:440-534).  Here those updaters run inside
+ * the step kernel, which appends the values to a per-job ring on the
+ * device; the caller drains it at its output times.
+ *
+ * SOPB_LOG_PULL, at every step % pullFreq == 0 of a force-ramp job:
+ *   v[0] |x[pulledEnd] - x[fixedEnd]|, v[1] that vector . pull vector,
+ *   v[2] extForce . pull vector, v[3..5] extForce (the force applied from
+ *   this step on).
+ * SOPB_LOG_TIP, at every step % nav == 0 of an indentation job, after the
+ *   tip's own step: v[0..2] the tip force averaged over nav, v[3] its norm,
+ *   v[4] |chip - tip| before the tip moved, v[5] dx, v[6..8] the tip after
+ *   the move, v[9..11] the cantilever base (chip).
+ */
+typedef struct sopb_log_row {
+    int32_t kind;                      /* SOPB_LOG_PULL or SOPB_LOG_TIP        */
+    int32_t pad;
+    int64_t step;
+    float v[12];
+} sopb_log_row;
+enum { SOPB_LOG_PULL = 1, SOPB_LOG_TIP = 2 };
+
+/* Copies the rows appended since the last drain, oldest first, at most
+ * max_rows of them, and sets *nrows.  Rows left over stay for the next
+ * call.  Returns SOPB_ERR_CAPACITY (the rows still come back) when the
+ * ring wrapped before the drain and the oldest rows were lost.  No
+ * reference counterpart. */
+int sopb_job_log(sopb_job* job, sopb_log_row* rows, int32_t max_rows, int32_t* nrows);
 
 /* Bulk transfer of the coordinates of many jobs with one copy each way:
  * host_xyzw holds sum(n_j) float4 in the order of `jobs`. */

@@ -50,6 +50,7 @@ def lib() -> C.CDLL:
             "orc_job_rebuild": ([vp, i32, i32], None),
             "orc_job_pairlist": ([vp, i32, vp, vp, i32], None),
             "orc_job_observables": ([vp, vp], None),
+            "orc_job_log": ([vp, vp, i32], i32),
             "orc_rpy_tensor": ([i32, vp, C.c_float, vp], None),
             "orc_cholesky_ref": ([i32, vp], None),
             "orc_ref_b_matrix": ([i32, vp, vp], None),
@@ -140,6 +141,12 @@ class OracleJob:
         out = np.zeros(8, np.float64)
         lib().orc_job_observables(self.h, out.ctypes.data)
         return out
+
+    def log(self, max_rows: int = 1 << 16) -> np.ndarray:
+        """Drains the pulling / indentation event log (sopb.LOG_ROW rows)."""
+        out = np.zeros(max_rows, sopb.LOG_ROW)
+        got = lib().orc_job_log(self.h, out.ctypes.data, max_rows)
+        return out[:got]
 
     def close(self) -> None:
         if self.h:

@@ -172,6 +172,9 @@ struct orc_job {
     float* tensor;
     int32_t status;
     int32_t refresh_due;   /* exact HI: refactorise D at the next step */
+    /* the per-update lines of the pulling and indentation updaters */
+    sopb_log_row* log;
+    int32_t log_len, log_cap;
 };
 
 static int32_t compute_stride(const sopb_params* p) {
@@ -342,7 +345,8 @@ void orc_job_destroy(orc_job* j) {
     if (!j) return;
     void* ptrs[] = {j->cov_cnt, j->cov_j, j->cov_r0, j->nat_cnt, j->nat_j, j->nat_r02, j->nat_m12,
                     j->nat_r0d, j->nat_ehd, j->pp_cnt, j->pp_j, j->pl_cnt, j->pl_j, j->x, j->f, j->T,
-                    j->extF, j->tipF, j->seeds, j->pulled, j->rf, j->mf, j->xc, j->ci4, j->eps, j->tensor};
+                    j->extF, j->tipF, j->seeds, j->pulled, j->rf, j->mf, j->xc, j->ci4, j->eps, j->tensor,
+                    j->log};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
     free(j);
 }
@@ -578,6 +582,27 @@ void orc_job_rebuild(orc_job* j, int32_t possible, int32_t verlet) {
 /* ------------------------------------------------------------------------ */
 /* Updaters                                                                  */
 /* ------------------------------------------------------------------------ */
+static void log_append(orc_job* j, int32_t kind, const float* v) {
+    if (j->log_len == j->log_cap) {
+        j->log_cap = j->log_cap ? 2 * j->log_cap : 64;
+        j->log = (sopb_log_row*)realloc(j->log, (size_t)j->log_cap * sizeof(sopb_log_row));
+    }
+    sopb_log_row* r = &j->log[j->log_len++];
+    memset(r, 0, sizeof(*r));
+    r->kind = kind;
+    r->step = j->step;
+    memcpy(r->v, v, 12 * sizeof(float));
+}
+
+/* Drains the rows appended since the last call (oldest first). */
+int32_t orc_job_log(orc_job* j, sopb_log_row* rows, int32_t max_rows) {
+    int32_t take = j->log_len < max_rows ? j->log_len : max_rows;
+    memcpy(rows, j->log, (size_t)take * sizeof(sopb_log_row));
+    memmove(j->log, j->log + take, (size_t)(j->log_len - take) * sizeof(sopb_log_row));
+    j->log_len -= take;
+    return take;
+}
+
 /* PullingUpdater::update -> PullingPotential::updateForces
  * (src/Potentials/pulling.cu:152-165, 198-214) */
 static void pulling_update(orc_job* j) {
@@ -587,6 +612,19 @@ static void pulling_update(orc_job* j) {
     const float* xe = F4(j->x, p->pulledEnd);
     for (int c = 0; c < 3; c++) j->extForce[c] = p->k_trans * (j->cant[c] - xe[c]);
     for (int c = 0; c < 3; c++) j->cant[c] = j->cant0[c] + xt * j->pullvec[c];
+    if (j->step % freq == 0) {
+        /* savePullingData (src/Potentials/pulling.cu:167-190) */
+        const float* xf = F4(j->x, p->fixedEnd);
+        float e[3] = {xe[0] - xf[0], xe[1] - xf[1], xe[2] - xf[2]};
+        float v[12] = {0};
+        v[0] = sqrtf(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        v[1] = e[0] * j->pullvec[0] + e[1] * j->pullvec[1] + e[2] * j->pullvec[2];
+        v[2] = j->extForce[0] * j->pullvec[0] + j->extForce[1] * j->pullvec[1] + j->extForce[2] * j->pullvec[2];
+        v[3] = j->extForce[0];
+        v[4] = j->extForce[1];
+        v[5] = j->extForce[2];
+        log_append(j, SOPB_LOG_PULL, v);
+    }
     for (int32_t k = 0; k < j->npulled; k++) {
         float* e = F4(j->extF, j->pulled[k]);
         e[0] = j->extForce[0];
@@ -629,6 +667,9 @@ static void indentation_update(orc_job* j) {
         for (int c = 0; c < 3; c++) j->tip[c] += mult * df[c];
     }
     memcpy(j->fav, f, 16);
+    const float v[12] = {f[0], f[1], f[2], f[3], sqrtf(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), j->dx,
+                         j->tip[0], j->tip[1], j->tip[2], j->chip[0], j->chip[1], j->chip[2]};
+    log_append(j, SOPB_LOG_TIP, v);
 }
 
 /* RPY block normalised by D_ii (src/Integrators/bdhitea_kernel.cu:67-87);

@@ -55,6 +55,8 @@ void orc_job_pairlist(const orc_job* job, int32_t possible, int32_t* counts, int
  * SOPPotential::sumEnergies): T, E_fene, E_native, E_pairs, E_total,
  * intact native contacts, Rg, TEA epsilon (0 without TEA). */
 void orc_job_observables(const orc_job* job, double* out8);
+/* Drains the pulling / indentation event log (sopb_log_row rows). */
+int32_t orc_job_log(orc_job* job, sopb_log_row* rows, int32_t max_rows);
 
 /* Exact-HI helpers (src/Integrators/bdhitea_kernel.cu:89-190). */
 /* Normalised RPY tensor D (3n x 3n, row-major) at coords xyz[3n]. */

@@ -150,6 +150,7 @@ struct sopb_job {
     cudaStream_t la = nullptr;         // exact HI: the factorisation's second stream
     cudaEvent_t la_fork = nullptr, la_join = nullptr;
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
+    uint32_t log_tail = 0;             // event-log rows drained so far
 };
 
 #define CUDA_TRY(call)                                                                         \
@@ -493,6 +494,7 @@ int validate_desc(const sopb_job_desc* d) {
     if (p.timestep <= 0.0f || p.zeta <= 0.0f) return SOPB_ERR_INVALID;
     if (p.nav <= 0 || p.pairs_freq <= 0 || p.possiblepairs_freq <= 0) return SOPB_ERR_INVALID;
     if (p.heating && p.tempFreq <= 0) return SOPB_ERR_INVALID;
+    if (p.log_rows < 0 || p.log_rows > (1 << 24) || (p.log_rows & (p.log_rows - 1))) return SOPB_ERR_INVALID;
     if (d->nbonds < 0 || d->nnatives < 0 || d->nfixed < 0 || d->npulled < 0) return SOPB_ERR_INVALID;
     if ((d->nbonds && (!d->bonds || !d->bonds_r0)) || (d->nnatives && (!d->natives || !d->natives_r0 || !d->natives_eh)))
         return SOPB_ERR_INVALID;
@@ -803,6 +805,9 @@ extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
     b += align256(n * cap_pp * 4) + align256(n * cap_pl * 4);
     b += n * (16 + 16 + 16 + 4 + 16 + 1);           // bead pools
     b += align256(n * std::min<int64_t>(n - 1, 2 * cap_pl) * 2) + align256(n * 4) + align256(n * 16);   // near list
+    const sopb_params& p = d->params;
+    if ((p.pulling && p.deltax != 0.0f) || p.indentation)
+        b += align256((size_t)(p.log_rows > 0 ? p.log_rows : 1024) * 64);                        // event log
     *bytes = b;
     return SOPB_OK;
 }
@@ -875,6 +880,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
         h.deltax = p.deltax;
         h.k_trans = p.k_trans;
         h.pulledEnd = p.pulledEnd;
+        h.fixedEnd = p.fixedEnd;
         const float4 xe = x[p.pulledEnd], xf = x[p.fixedEnd];
         if (p.pull_direction == SOPB_PULL_VECTOR) {
             for (int c2 = 0; c2 < 3; ++c2) h.pullvec[c2] = p.pullVector[c2];
@@ -1006,7 +1012,10 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     const size_t o_nrj = o_plj + align256((size_t)n * h.cap_pl * 4);
     const size_t o_nrc = o_nrj + (h.mask ? align256((size_t)n * h.cap_nr * 2) : 0);
     const size_t o_xref = o_nrc + (h.mask ? align256((size_t)n * 4) : 0);
-    const size_t total = o_xref + (h.mask ? align256((size_t)n * 16) : 0);
+    const size_t o_log = o_xref + (h.mask ? align256((size_t)n * 16) : 0);
+    // event-log ring of the jobs whose updaters print per-update lines
+    h.log_cap = (h.ramp || h.indent) ? (p.log_rows > 0 ? p.log_rows : 1024) : 0;
+    const size_t total = o_log + align256((size_t)h.log_cap * 64);
     sopb_job* j = new (std::nothrow) sopb_job();
     if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
     // stream-ordered allocation: a destroyed job's memory returns to the
@@ -1034,6 +1043,8 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.nr_j = h.mask ? (uint16_t*)(base + o_nrj) : nullptr;
     h.nr_cnt = h.mask ? (int32_t*)(base + o_nrc) : nullptr;
     h.x_ref = h.mask ? (float4*)(base + o_xref) : nullptr;
+    h.log = h.log_cap ? (float*)(base + o_log) : nullptr;
+    h.log_head = 0;
     h.nr_valid = 0;
     h.x = c->x + b0;
     h.xalt = c->xalt + b0;
@@ -1378,6 +1389,34 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
     }
     SOPB_TRY(io_end(j, false));
     return SOPB_OK;
+}
+
+extern "C" int sopb_job_log(sopb_job* j, sopb_log_row* rows, int32_t max_rows, int32_t* nrows) {
+    if (!j || !nrows || max_rows < 0 || (max_rows > 0 && !rows)) return SOPB_ERR_INVALID;
+    *nrows = 0;
+    sopb_context* c = j->ctx;
+    CUDA_TRY(cudaSetDevice(c->device));
+    SOPB_TRY(read_slot(j));
+    const uint32_t cap = (uint32_t)j->h.log_cap;
+    if (cap == 0) return SOPB_OK;
+    const uint32_t head = j->h.log_head;
+    int rc = SOPB_OK;
+    if (head - j->log_tail > cap) {        // the ring wrapped: keep the newest cap rows
+        j->log_tail = head - cap;
+        rc = SOPB_ERR_CAPACITY;
+    }
+    const uint32_t take = std::min<uint32_t>(head - j->log_tail, (uint32_t)max_rows);
+    const uint32_t r0 = j->log_tail & (cap - 1);
+    const uint32_t first = std::min<uint32_t>(take, cap - r0);
+    const float* ring = j->h.log;
+    if (first)
+        CUDA_TRY(cudaMemcpyAsync(rows, ring + (size_t)r0 * 16, (size_t)first * 64, cudaMemcpyDeviceToHost, c->io));
+    if (take > first)
+        CUDA_TRY(cudaMemcpyAsync(rows + first, ring, (size_t)(take - first) * 64, cudaMemcpyDeviceToHost, c->io));
+    CUDA_TRY(cudaStreamSynchronize(c->io));
+    j->log_tail += take;
+    *nrows = (int32_t)take;
+    return rc;
 }
 
 extern "C" int sopb_job_write(sopb_job* j, int32_t what, const void* in) {

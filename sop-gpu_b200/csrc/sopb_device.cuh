@@ -51,6 +51,7 @@ struct JobDev {
     float4* tipF;         // per-bead tip force accumulator (indentation)
     uint8_t* flags;       // FLAG_*
     float4* xalt;         // second coordinate buffer (grid path ping-pong)
+    float* log;           // [log_cap * 16] event-log ring (sopb_log_row), or null
     // ---- maps ----------------------------------------------------------------
     int32_t* cov_off;     // [n+1]
     int32_t* cov_j;
@@ -83,7 +84,7 @@ struct JobDev {
     int32_t minimization, heating;
     float initialT, deltaT;
     // ---- pulling ---------------------------------------------------------------
-    int32_t pulling, ramp, pulledEnd, pad0;
+    int32_t pulling, ramp, pulledEnd, fixedEnd;
     float deltax, k_trans;
     float pullvec[3], cant0[3], cant[3], pullF[3];
     // ---- indentation (continuous surface) ------------------------------------
@@ -98,7 +99,9 @@ struct JobDev {
     float epsilon;        // last per-job epsilon (for output)
     // ---- status ---------------------------------------------------------------
     int32_t status;
-    int32_t pad2[3];
+    int32_t log_cap;      // rows of the event-log ring (a power of two), 0 = none
+    uint32_t log_head;    // rows appended so far
+    int32_t pad2;
 };
 
 // ---------------------------------------------------------------------------

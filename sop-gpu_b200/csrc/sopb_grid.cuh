@@ -158,6 +158,7 @@ __global__ void k_g_scalar_updaters(JobDev* __restrict__ Jp, GridAux aux) {
     sc.V = J.V;
     sc.dx = J.dx;
     for (int c = 0; c < 4; ++c) sc.fav[c] = J.fav[c];
+    sc.log_head = J.log_head;
     if (J.indent) {
         if (step == J.retraction_step) sc.V = -sc.V;
         if (step % J.nav == 0) {
@@ -172,6 +173,7 @@ __global__ void k_g_scalar_updaters(JobDev* __restrict__ Jp, GridAux aux) {
         const float xe3[3] = {xe.x, xe.y, xe.z};
         for (int c = 0; c < 3; ++c) sc.pullF[c] = __fmul_rn(J.k_trans, __fsub_rn(sc.cant[c], xe3[c]));
         for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
+        if (step % J.pull_freq == 0) log_pull(J, sc, xe, J.x[J.fixedEnd], step);
     }
     if (J.heating && step % J.temp_freq == 0) {
         const float temp = __fadd_rn(J.initialT, __fmul_rn((float)(step / J.temp_freq), J.deltaT));
@@ -185,6 +187,7 @@ __global__ void k_g_scalar_updaters(JobDev* __restrict__ Jp, GridAux aux) {
     J.V = sc.V;
     J.dx = sc.dx;
     for (int c = 0; c < 4; ++c) J.fav[c] = sc.fav[c];
+    J.log_head = sc.log_head;
 }
 
 // Temperature-accumulator reset at nav (output_manager.cu:125-127).

@@ -85,6 +85,7 @@ struct StepScalars {
     float fav[4];
     int32_t err;
     int32_t nr_valid;   // the job's near list is usable (written back at the end)
+    uint32_t log_head;  // event-log rows appended (written back at the end)
 };
 
 // Cooperative copy of a job descriptor into shared memory (read by every
@@ -315,6 +316,32 @@ __device__ float3 block_sum3(float3 v, float (*red)[4]) {
     return s;
 }
 
+// Appends one row to the job's event-log ring (sopb_log_row layout: kind,
+// pad, step, twelve floats); the host drains it with sopb_job_log.
+__device__ __forceinline__ void log_row(const JobDev& J, uint32_t& head, int32_t kind, int64_t step, const float* v) {
+    if (J.log_cap <= 0) return;
+    float* r = J.log + (size_t)(head & (uint32_t)(J.log_cap - 1)) * 16;
+    reinterpret_cast<int32_t*>(r)[0] = kind;
+    reinterpret_cast<int32_t*>(r)[1] = 0;
+    *reinterpret_cast<int64_t*>(r + 2) = step;
+    for (int k = 0; k < 12; ++k) r[4 + k] = v[k];
+    ++head;
+}
+
+// PullingPotential::savePullingData (src/Potentials/pulling.cu:167-190): the
+// end-to-end distance, its projection and the applied force along the pull
+// vector, from the coordinates of this step and the force just computed.
+// The reference evaluates it on the host (IEEE, no contraction).
+__device__ __noinline__ void log_pull(const JobDev& J, StepScalars& sc, float4 xp, float4 xf, int64_t step) {
+    const float e[3] = {__fsub_rn(xp.x, xf.x), __fsub_rn(xp.y, xf.y), __fsub_rn(xp.z, xf.z)};
+    auto dot3 = [](const float* a, const float* b) {
+        return __fadd_rn(__fadd_rn(__fmul_rn(a[0], b[0]), __fmul_rn(a[1], b[1])), __fmul_rn(a[2], b[2]));
+    };
+    const float v[12] = {__fsqrt_rn(dot3(e, e)), dot3(e, J.pullvec), dot3(sc.pullF, J.pullvec),
+                         sc.pullF[0], sc.pullF[1], sc.pullF[2], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    log_row(J, sc.log_head, SOPB_LOG_PULL, step, v);
+}
+
 // IndentationTipUpdater::update (src/Potentials/indentation.cu:414-550) for
 // the continuous surface, run by thread 0 after the CTA summed the tip force.
 // Host-side arithmetic of the reference is IEEE without contraction, hence
@@ -328,8 +355,10 @@ __device__ __noinline__ void tip_update(const JobDev& J, StepScalars& sc, float3
     } else {
         for (int c = 0; c < 3; ++c) sc.chip[c] = __fadd_rn(J.chip0[c], __fmul_rn(J.dir[c], sc.dx));
     }
-    float df[3];
-    for (int c = 0; c < 3; ++c) df[c] = __fadd_rn(-f[c], __fmul_rn(__fsub_rn(sc.chip[c], sc.ig.tip[c]), J.cantKs));
+    float df[3], dr[3];
+    for (int c = 0; c < 3; ++c) dr[c] = __fsub_rn(sc.chip[c], sc.ig.tip[c]);
+    const float drw = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dr[0], dr[0]), __fmul_rn(dr[1], dr[1])), __fmul_rn(dr[2], dr[2])));
+    for (int c = 0; c < 3; ++c) df[c] = __fadd_rn(-f[c], __fmul_rn(dr[c], J.cantKs));
     const float mult = __fdiv_rn(__fmul_rn(J.h, (float)J.nav), J.tipZeta);
     if (J.fixTrans) {
         float ct = __fadd_rn(__fadd_rn(__fmul_rn(__fmul_rn(mult, df[0]), J.dir[0]), __fmul_rn(__fmul_rn(mult, df[1]), J.dir[1])),
@@ -342,6 +371,9 @@ __device__ __noinline__ void tip_update(const JobDev& J, StepScalars& sc, float3
     sc.fav[1] = f[1];
     sc.fav[2] = f[2];
     sc.fav[3] = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(f[0], f[0]), __fmul_rn(f[1], f[1])), __fmul_rn(f[2], f[2])));
+    const float v[12] = {sc.fav[0], sc.fav[1], sc.fav[2], sc.fav[3], drw, sc.dx,
+                         sc.ig.tip[0], sc.ig.tip[1], sc.ig.tip[2], sc.chip[0], sc.chip[1], sc.chip[2]};
+    log_row(J, sc.log_head, SOPB_LOG_TIP, step, v);
 }
 
 // Shared-memory cache of the Verlet rows as compact CSR: offsets by a CTA
@@ -421,6 +453,7 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
         const float xe3[3] = {xe.x, xe.y, xe.z};
         for (int c = 0; c < 3; ++c) sc.pullF[c] = __fmul_rn(J.k_trans, __fsub_rn(sc.cant[c], xe3[c]));
         for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
+        if (step % J.pull_freq == 0) log_pull(J, sc, xe, xs[J.fixedEnd], step);
     }
     const bool pp = step % J.pp_freq == 0;
     if (pp) build_possible<BLOCK>(J, xs, err);
@@ -509,6 +542,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
         for (int c = 0; c < 4; ++c) sc.fav[c] = J.fav[c];
         sc.err = 0;
         sc.nr_valid = J.nr_valid;
+        sc.log_head = J.log_head;
     }
     __syncthreads();
     const int cap = J.lcache;
@@ -601,6 +635,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
         Jp->dx = sc.dx;
         for (int c = 0; c < 4; ++c) Jp->fav[c] = sc.fav[c];
         Jp->nr_valid = sc.nr_valid;
+        Jp->log_head = sc.log_head;
         if (sc.err) Jp->status = sc.err;
     }
 }

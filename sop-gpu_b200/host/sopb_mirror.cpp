@@ -132,21 +132,10 @@ void Config::float3(const std::string& key, float out[3], const float def[3]) co
 // ---------------------------------------------------------------------------
 // .top (src/IO/topio.cpp:36-80, 204-240) and PDB (src/IO/pdbio.cpp:80-152)
 // ---------------------------------------------------------------------------
-namespace {
-struct AtomRec {
-    std::string name, resName;
-    char chain = 'A';
-    int resid = 0;
-    double occupancy = 0.0, beta = 0.0;
-};
-std::vector<AtomRec> g_atoms;   // [ atoms ] of the loaded topology, for the final PDB
-}  // namespace
-
 Topology Topology::load(const std::string& path) {
     std::ifstream f(path);
     if (!f) throw Error(SOPB_ERR_INVALID, "cannot open topology " + path);
     Topology t;
-    g_atoms.clear();
     std::string line;
     enum { NONE, ATOMS, BONDS, NATIVES, PAIRS } sec = NONE;
     int lineno = 0;
@@ -174,7 +163,9 @@ Topology Topology::load(const std::string& path) {
         if (tok.empty()) continue;
         switch (sec) {
         case ATOMS: {
-            AtomRec a;
+            Atom a;
+            a.resid = t.natoms + 1;
+            a.occupancy = 1.0;
             if (tok.size() >= 8) {
                 a.resid = std::atoi(tok[2].c_str());
                 a.resName = tok[3];
@@ -183,7 +174,7 @@ Topology Topology::load(const std::string& path) {
                 a.occupancy = std::atof(tok[6].c_str());
                 a.beta = std::atof(tok[7].c_str());
             }
-            g_atoms.push_back(a);
+            t.atoms.push_back(a);
             t.natoms++;
             break;
         }
@@ -226,19 +217,31 @@ std::vector<float> read_coords(const std::string& path, int expect) {
     return xyz;
 }
 
-// savePDB (src/IO/pdbio.cpp:194-221) with PDBAtom::fprint's format (:265-280)
-void save_pdb(const std::string& path, const std::vector<float>& xyzw, int n) {
+// savePDB (src/IO/pdbio.cpp:194-221) with PDBAtom::fprint's format
+// (:265-280): atom ids in hexadecimal from 100000 atoms on; CONECT lines
+// group consecutive bonds that share their first bead.
+void save_pdb(const std::string& path, const std::vector<Atom>& atoms, const std::vector<Atom>& extra,
+              const std::vector<int32_t>& bonds) {
     FILE* f = std::fopen(path.c_str(), "w");
     if (!f) throw Error(SOPB_ERR_INVALID, "cannot write " + path);
-    const bool hex = n >= 100000;
-    for (int i = 0; i < n; ++i) {
-        AtomRec a = i < (int)g_atoms.size() ? g_atoms[i] : AtomRec{"CA", "ALA", 'A', i + 1, 1.0, 0.0};
-        std::fprintf(f, hex ? "ATOM  %5x %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n"
-                            : "ATOM  %5d %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n",
-                     i + 1, a.name.c_str(), ' ', a.resName.c_str(), a.chain, a.resid, (double)xyzw[4 * i],
-                     (double)xyzw[4 * i + 1], (double)xyzw[4 * i + 2], a.occupancy, a.beta);
+    const bool hex = atoms.size() + extra.size() >= 100000;
+    int id = 0;
+    for (const std::vector<Atom>* set : {&atoms, &extra})
+        for (const Atom& a : *set)
+            std::fprintf(f, hex ? "ATOM  %5x %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n"
+                                : "ATOM  %5d %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n",
+                         ++id, a.name.c_str(), ' ', a.resName.c_str(), a.chain, a.resid, (double)a.x, (double)a.y,
+                         (double)a.z, a.occupancy, a.beta);
+    int last = -1;
+    for (size_t b = 0; b + 1 < bonds.size(); b += 2) {
+        if (bonds[b] != last) {
+            if (last != -1) std::fputc('\n', f);
+            std::fprintf(f, "CONECT%5d", bonds[b] + 1);
+            last = bonds[b];
+        }
+        std::fprintf(f, "%5d", bonds[b + 1] + 1);
     }
-    std::fprintf(f, "END");
+    std::fprintf(f, "\nEND");
     std::fclose(f);
 }
 
@@ -436,6 +439,7 @@ void Simulation::initFF() {
     } else {
         integrator.reset(new NamedIntegrator("Langevin", p.timestep));
     }
+    p.log_rows = 4096;   // event-log ring of the pulling / indentation lines
     // runGPU's stride (src/gsop.cu:117-122)
     stride = p.nav;
     for (auto& u : updaters) stride = std::min(stride, u->frequency);
@@ -452,19 +456,6 @@ void Simulation::run(int64_t nsteps) {
         const int st = sopb_job_status(jobs[r]);
         if (st != SOPB_OK)
             throw Error(st, "run " + std::to_string(r + firstrun) + ": " + sopb_status_string(st));
-    }
-}
-
-// runGPU (src/gsop.cu:111-163): (numsteps/stride + 1) * stride steps, then
-// the final coordinates of every run.
-void Simulation::runGPU() {
-    run((numsteps / stride + 1) * stride);
-    const int n = top.natoms;
-    std::vector<float> x(4 * (size_t)n);
-    const std::string mask = cfg.str("finalcoord", cfg.str("name", "unnamed") + "_<run>_final.pdb");
-    for (size_t r = 0; r < jobs.size(); ++r) {
-        check(sopb_job_read(jobs[r], SOPB_COORDS, x.data()), "coords");
-        save_pdb(replace_all(mask, "<run>", std::to_string((int)r + firstrun)), x, n);
     }
 }
 

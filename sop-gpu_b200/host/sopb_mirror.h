@@ -51,8 +51,16 @@ private:
 };
 
 // ---- topology and coordinates (src/IO/topio.cpp, src/IO/pdbio.cpp) --------
+struct Atom {                      // one PDB ATOM record (PDBAtom)
+    std::string name = "CA", resName = "ALA";
+    char chain = 'A';
+    int resid = 0;
+    double occupancy = 0.0, beta = 0.0;
+    float x = 0.0f, y = 0.0f, z = 0.0f;
+};
 struct Topology {
     int natoms = 0;
+    std::vector<Atom> atoms;           // [ atoms ] section, in file order
     std::vector<int32_t> bonds;        // (i, j) pairs
     std::vector<float> bonds_r0;
     std::vector<int32_t> natives;
@@ -61,7 +69,18 @@ struct Topology {
     static Topology load(const std::string& path);
 };
 std::vector<float> read_coords(const std::string& path, int expect);         // xyz[3n]
-void save_pdb(const std::string& path, const std::vector<float>& xyzw, int n);  // final coordinates
+// savePDB (src/IO/pdbio.cpp:194-221): the atoms, then `extra` (the tip and
+// surface beads of an indentation run), then CONECT records of the bonds.
+void save_pdb(const std::string& path, const std::vector<Atom>& atoms, const std::vector<Atom>& extra,
+              const std::vector<int32_t>& bonds);
+
+// ---- DCD trajectories (src/IO/dcdio.cpp:56-194) ------------------------------
+// CHARMM/NAMD binary layout: an 84-byte header record, two 80-character
+// title lines, the atom count, then per frame the X, Y and Z blocks, each
+// framed by its byte length.  No unit cell.
+void dcd_write_header(const std::string& path, int natoms, int nsavc, float delta);
+void dcd_append_frame(const std::string& path, const std::vector<float>& X, const std::vector<float>& Y,
+                      const std::vector<float>& Z);
 
 // ---- plugin surface (src/gsop.h:69-105) -------------------------------------
 class Simulation;
@@ -105,7 +124,10 @@ public:
     ~Simulation();
     void initFF();                         // plugins in the reference's creation order
     void run(int64_t nsteps);              // sopb_run over every run of the job
-    void runGPU();                         // the reference's loop length, then final PDBs
+    // the reference's loop: (numsteps/stride + 1) * stride steps with the
+    // output updaters (.dat, DCD, restart PDB, pulling and indentation lines)
+    // at their steps, then the final PDB of every run
+    void runGPU();
     SOPPotential* potentialByName(const std::string& n) const;
     SOPUpdater* updaterByName(const std::string& n) const;
 

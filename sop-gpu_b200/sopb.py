@@ -21,6 +21,9 @@ PULL_END_TO_END, PULL_VECTOR = 0, 1
 HI_B_CHOLESKY, HI_B_REFCOMPAT = 0, 1
 COORDS, SEEDS, TEMP, FORCES, TIPFORCES, PULLSTATE, TIPSTATE, HISTATE, HIFACTOR, OBSERVABLES = range(10)
 OBSERVABLE_NAMES = ("T", "E_fene", "E_native", "E_pairs", "E_total", "native_contacts", "Rg", "tea_eps")
+# event-log rows (sopb_log_row): pulling lines every pullFreq, tip lines every nav
+LOG_PULL, LOG_TIP = 1, 2
+LOG_ROW = np.dtype([("kind", "<i4"), ("pad", "<i4"), ("step", "<i8"), ("v", "<f4", (12,))])
 
 F3 = C.c_float * 3
 
@@ -53,7 +56,7 @@ class Params(C.Structure):
         ("hi_capricious", C.c_int32), ("hi_unlisted", C.c_int32), ("hi_epsmax", C.c_float),
         ("hi_b_mode", C.c_int32), ("hi_refresh", C.c_int32), ("lanes_per_bead", C.c_int32),
         ("cell_list", C.c_int32), ("grid_path", C.c_int32), ("R_limit_bond", C.c_float),
-        ("reserved", C.c_int32 * 4),
+        ("log_rows", C.c_int32), ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -102,6 +105,7 @@ def lib() -> C.CDLL:
             "sopb_job_write": ([vp, i32, vp], C.c_int),
             "sopb_job_pairlist": ([vp, i32, vp, vp, i32], C.c_int),
             "sopb_job_rebuild_lists": ([vp, i32, i32], C.c_int),
+            "sopb_job_log": ([vp, vp, i32, vp], C.c_int),
             "sopb_jobs_upload_coords": ([vp, vp, i32, vp], C.c_int),
             "sopb_jobs_download_coords": ([vp, vp, i32, vp], C.c_int),
             "sopb_tea_coefficients_noalloc": ([vp, i32, C.c_float, vp, vp, vp], C.c_int),
@@ -260,6 +264,14 @@ class Job:
 
     def rebuild(self, possible: bool = True, verlet: bool = True) -> None:
         check(lib().sopb_job_rebuild_lists(self.handle, int(possible), int(verlet)), "rebuild")
+
+    def log(self, max_rows: int = 1 << 16) -> np.ndarray:
+        """Drains the event log: rows of LOG_ROW, oldest first.  Raises when
+        the ring wrapped since the last drain (rows were lost)."""
+        out = np.zeros(max_rows, LOG_ROW)
+        got = C.c_int32(0)
+        check(lib().sopb_job_log(self.handle, out.ctypes.data, max_rows, C.byref(got)), "job_log")
+        return out[: got.value]
 
     def destroy(self) -> None:
         if self.handle:

@@ -2,10 +2,15 @@
 SOP-GPU source tree by oracle/build_ref.sh) on every case of ref_cases.py on
 a B200 and packs the dumps into ref_gpu_<case>.npz.
 
-    python tests/golden/make_ref_gpu_golden.py <outdir>
+    python tests/golden/make_ref_gpu_golden.py <outdir> [case ...]
+    python tests/golden/make_ref_gpu_golden.py --pack <outdir> [case ...]
 
 The .npz files are then committed next to this script.  Pair rows are
-trimmed to the largest count (the reference pads them with -1).
+trimmed to the largest count (the reference pads them with -1).  The files
+the reference's output updaters wrote during the run (.dat, DCD, restart
+PDB, pulling and indentation lines) go into the same archive as byte arrays
+under "file:<basename>".  --pack repacks an earlier run's directory without
+running the reference again.
 """
 import os
 import subprocess
@@ -22,17 +27,22 @@ REF_GPU = os.path.join(REPO, "oracle", "_ref", "ref_gpu")
 
 
 def main():
-    out = os.path.abspath(sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/refgold")
-    names = sys.argv[2:] or list(ref_cases.CASES)
+    args = sys.argv[1:]
+    pack_only = bool(args) and args[0] == "--pack"
+    if pack_only:
+        args = args[1:]
+    out = os.path.abspath(args[0] if args else "gpurun_out/refgold")
+    names = args[1:] or list(ref_cases.CASES)
     for name in names:
         c = ref_cases.CASES[name]
         d = os.path.join(out, name)
-        cfg = ref_cases.write_inputs(name, d)
         dumpdir = os.path.join(d, "dump")
-        os.makedirs(dumpdir, exist_ok=True)
-        cmd = [REF_GPU, os.path.basename(cfg), dumpdir, str(c["total"])] + [str(s) for s in c["dumps"]]
-        with open(os.path.join(d, "ref_gpu.log"), "w") as log:
-            subprocess.check_call(cmd, cwd=d, stdout=log, stderr=subprocess.STDOUT)
+        if not pack_only:
+            cfg = ref_cases.write_inputs(name, d)
+            os.makedirs(dumpdir, exist_ok=True)
+            cmd = [REF_GPU, os.path.basename(cfg), dumpdir, str(c["total"])] + [str(s) for s in c["dumps"]]
+            with open(os.path.join(d, "ref_gpu.log"), "w") as log:
+                subprocess.check_call(cmd, cwd=d, stdout=log, stderr=subprocess.STDOUT)
         meta = dict(l.split() for l in open(os.path.join(dumpdir, "meta.txt")))
         N = int(meta["aminoCount"])
         mp = int(meta["max_pairs"])
@@ -49,6 +59,9 @@ def main():
             arrays["pairs_%d" % s] = rows[:, : max(1, int(cnt.max()))].copy()
             if os.path.exists(f("tip")):
                 arrays["tip_%d" % s] = np.fromfile(f("tip"), np.float32)
+        for fname in ref_cases.output_files(d, name):
+            with open(os.path.join(d, fname), "rb") as fh:
+                arrays["file:" + fname] = np.frombuffer(fh.read(), np.uint8)
         np.savez_compressed(os.path.join(out, "ref_gpu_%s.npz" % name), **arrays)
         print("case %s: %d beads, stride %s" % (name, N, meta["stride"]))
 

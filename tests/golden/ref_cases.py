@@ -46,6 +46,30 @@ CASES = {
         "indentationDirection": "0.0 1.0 0.0", "indentationSurfaceN": "0.0 -1.0 0.0", "indentationTipZeta": "500",
         "indentationSurfA": "1.0", "indentationSurfB": "-2.0", "indentationSurfSigma": "3.0",
         "indentationSurfEl": "0.2", "indentationFixTrans": "yes", "indentationOutput": "<name>_indent.dat"}),
+    # output files every few strides: .dat (with Rg), DCD, restart PDB and
+    # pulling lines for two runs
+    "pullout": dict(n=200, sys_seed=11, runs=2, total=100, dumps=[100], files=True, cfg={
+        "runnum": "2", "firstrun": "1", "seed": "1119726", "nav": "100", "max_pairs": "256",
+        "max_possiblePairs": "256", "pulling": "on", "deltax": "0.02", "k_trans": "0.05", "pullFreq": "10",
+        "fixed": "0", "pulled": "199", "fixedEnd": "0", "pulledEnd": "199", "pullDirection": "endToEnd",
+        "pullOutput": "<name>_<run>_pull.dat", "outputtiming": "20", "dcdfreq": "20", "restartfreq": "50",
+        "computeRg": "yes"}),
+    # indentation lines averaged over two tip updates, the tip and surface
+    # beads in the DCD and PDB files
+    "indentout": dict(n=200, sys_seed=13, runs=1, total=120, dumps=[120], files=True, cfg={
+        "run": "1", "seed": "31337", "nav": "20", "max_pairs": "256", "max_possiblePairs": "256",
+        "indentation": "on", "indentationTipR": "20.0", "indentationKs": "0.07", "indentationDeltaX": "0.05",
+        "indentationDirection": "0.0 1.0 0.0", "indentationSurfaceN": "0.0 -1.0 0.0", "indentationTipZeta": "500",
+        "indentationSurfA": "1.0", "indentationSurfB": "-2.0", "indentationSurfSigma": "3.0",
+        "indentationSurfEl": "0.2", "indentationFixTrans": "yes", "indentationOutput": "<name>_indent.dat",
+        "indentationOutputFreq": "40", "outputtiming": "20", "dcdfreq": "40", "restartfreq": "60",
+        "indentationShowTipSurf": "yes", "indentationSurfaceSize": "5", "indentationSurfaceStep": "10.0",
+        "indentationCantLength": "50.0", "indentationSurfConnectFile": "<name>_mica.vmd"}),
+    # the TEA epsilon column
+    "teaout": dict(n=100, sys_seed=23, runs=1, total=30, dumps=[30], files=True, cfg={
+        "run": "1", "seed": "777", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
+        "hi_on": "yes", "hi_a": "1.9", "hi_unlisted": "yes", "hi_capricious": "no", "hi_epsilon_freq": "10",
+        "outputtiming": "10", "dcdfreq": "10"}),
     "heat": dict(n=100, sys_seed=6, runs=1, total=45, dumps=[45], cfg={
         "run": "1", "seed": "5", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
         "heating": "on", "initialT": "0.1", "deltaT": "0.2", "tempFreq": "10"}),
@@ -80,6 +104,19 @@ def config_text(name):
         cfg["indentationTip"] = tip
         cfg["indentationSurfaceR0"] = "0.0 %.4f 0.0" % (x[:, 1].max() + 6.0)
     return "".join("%s\t%s\n" % (k, v) for k, v in cfg.items())
+
+
+# the files the reference's output updaters write for a case, by basename
+OUTPUT_SUFFIXES = (".dat", ".dcd", "_restart", "_final.pdb", ".vmd")
+
+
+def output_files(d, name):
+    """Output files of a case found in directory d (not the input PDBs)."""
+    out = []
+    for f in sorted(os.listdir(d)):
+        if f.startswith(name) and f.endswith(OUTPUT_SUFFIXES):
+            out.append(f)
+    return out
 
 
 def write_inputs(name, d):

@@ -220,7 +220,8 @@ def run_cli(name, d):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", golden_cases())
 def test_cli_files_match_reference(tmp_path, name):
-    subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "sop-gpu_b200")])
+    if not os.path.exists(CLI):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "sop-gpu_b200")])
     d = str(tmp_path)
     g = run_cli(name, d)
     ref_names = sorted(k[5:] for k in g.files if k.startswith("file:"))

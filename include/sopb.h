@@ -130,9 +130,25 @@ typedef struct sopb_params {
     int32_t cell_list;         /* possible pairs by cell list: 0 auto, 1 on, 2 off */
     int32_t grid_path;         /* 0 auto (resident kernel when it fits), 1 grid */
     float R_limit_bond;        /* 8: a native contact within it counts intact   */
-    int32_t log_rows;          /* event-log ring of a pulling (deltax != 0) or  */
-                               /* indentation job, rows; a power of two, 0 = 1024 */
-    int32_t reserved[3];
+    int32_t log_rows;          /* event-log ring of a pulling (deltax != 0),    */
+                               /* indentation or pulling-plane job, rows; a   */
+                               /* power of two, 0 = 1024                      */
+    /* Potentials/indentation.h:39-47 (discrete surface) */
+    int32_t indentationDiscreteSurf; /* surface as a square of beads           */
+    int32_t indentationSurfaceSize;  /* 51: beads per side                     */
+    float indentationSurfaceStep;    /* 1.4: bead spacing                      */
+    float indentationPairsCutoff;    /* 40: surface-bead list cutoff           */
+    /* Potentials/pulling_plane.h:12-27 */
+    int32_t pullingPlane;
+    float pullingPlaneDeltax;        /* cantilever displacement per update     */
+    float pullingPlaneKs;            /* 0.05: bead-plane spring                */
+    float pullingPlaneKsCant;        /* 0.05: plane-cantilever spring          */
+    float pullingPlaneZeta;          /* 200: plane friction                    */
+    float pullingPlaneDir[3];        /* plane normal (normalised on use)       */
+    float pullingPlanePos[3];        /* a point of both planes at step 0       */
+    int32_t pullingPlaneUpdateFreq;  /* defaults to nav                        */
+    int32_t pullingPlaneOutputFreq;  /* defaults to nav                        */
+    int32_t reserved2[4];
 } sopb_params;
 
 /*
@@ -157,6 +173,10 @@ typedef struct sopb_job_desc {
     int32_t seed;                      /* used when seeds == NULL             */
     int32_t reserved;
     sopb_params params;
+    int32_t nplane_fixed;
+    const int32_t* plane_fixed;        /* pulling plane 'plane_fixed' beads   */
+    int32_t nplane_pulled;
+    const int32_t* plane_pulled;       /* pulling plane 'plane_pulled' beads  */
 } sopb_job_desc;
 
 typedef struct sopb_context sopb_context;
@@ -306,6 +326,12 @@ int sopb_job_rebuild_lists(sopb_job* job, int32_t possible, int32_t verlet);
  *   tip's own step: v[0..2] the tip force averaged over nav, v[3] its norm,
  *   v[4] |chip - tip| before the tip moved, v[5] dx, v[6..8] the tip after
  *   the move, v[9..11] the cantilever base (chip).
+ * SOPB_LOG_PLANE, at every step % pullingPlaneOutputFreq == 0 of a
+ *   pulling-plane job, after the plane's own step
+ *   (src/Potentials/pulling_plane.cu:183-258): v[0] the plane displacement,
+ *   v[1] the cantilever displacement, v[2] the cantilever force on the
+ *   plane, v[3] the beads' force on the plane, v[4] the distance between
+ *   the centroids of the fixed and the pulled beads.
  */
 typedef struct sopb_log_row {
     int32_t kind;                      /* SOPB_LOG_PULL or SOPB_LOG_TIP        */
@@ -313,7 +339,7 @@ typedef struct sopb_log_row {
     int64_t step;
     float v[12];
 } sopb_log_row;
-enum { SOPB_LOG_PULL = 1, SOPB_LOG_TIP = 2 };
+enum { SOPB_LOG_PULL = 1, SOPB_LOG_TIP = 2, SOPB_LOG_PLANE = 3 };
 
 /* Copies the rows appended since the last drain, oldest first, at most
  * max_rows of them, and sets *nrows.  Rows left over stay for the next

@@ -175,6 +175,14 @@ struct orc_job {
     /* the per-update lines of the pulling and indentation updaters */
     sopb_log_row* log;
     int32_t log_len, log_cap;
+    /* discrete surface (indentation.cu:137-201, 311-362) */
+    int32_t nsurf;
+    float *surf0, *surf;     /* surface beads at dx = 0 and now, xyz */
+    int32_t *mica_cnt, *mica_j, cap_mica;
+    /* pulling plane (pulling_plane.cu:35-266) */
+    uint8_t* plane_mask;     /* 1 fixed plane, 2 pulled plane */
+    float *plane_r0, *plane_f;
+    float plane_n[3], plane_p0[3], plane_displ, plane_cant;
 };
 
 static int32_t compute_stride(const sopb_params* p) {
@@ -187,6 +195,7 @@ static int32_t compute_stride(const sopb_params* p) {
     if (p->heating) MINF(p->tempFreq);
     if (p->hi_on && !p->hi_exact) MINF(p->hi_epsilon_freq);
     if (p->hi_on && p->hi_exact && p->hi_refresh > 1) MINF(p->hi_refresh);   /* factor refresh updater */
+    if (p->pullingPlane) MINF(p->pullingPlaneUpdateFreq > 0 ? p->pullingPlaneUpdateFreq : p->nav);
 #undef MINF
     return s;
 }
@@ -329,6 +338,52 @@ orc_job* orc_job_create(const sopb_job_desc* d) {
         for (int c = 0; c < 3; c++) j->dir[c] /= nrm;
         nrm = sqrtf(j->micaN[0] * j->micaN[0] + j->micaN[1] * j->micaN[1] + j->micaN[2] * j->micaN[2]);
         for (int c = 0; c < 3; c++) j->micaN[c] /= nrm;
+        if (p->indentationDiscreteSurf) {
+            /* the square of surface beads of IndentationAminoUpdater
+             * (indentation.cu:311-362), from the configured, unnormalised
+             * surface normal */
+            const int32_t S = p->indentationSurfaceSize;
+            const float* nn = p->indentationSurfaceN;
+            const float* r0 = p->indentationSurfaceR0;
+            float r1[3];
+            if (nn[0] == 0) { r1[0] = 1.0f; r1[1] = 0; r1[2] = 0; }
+            else if (nn[1] == 0) { r1[0] = 0; r1[1] = 1.0f; r1[2] = 0; }
+            else if (nn[2] == 0) { r1[0] = 0; r1[1] = 0; r1[2] = 1.0f; }
+            else { r1[0] = 0; r1[1] = 1.0f; r1[2] = -(nn[1] / nn[2]) * r1[1]; }
+            float norm = sqrtf(r1[0] * r1[0] + r1[1] * r1[1] + r1[2] * r1[2]);
+            for (int c = 0; c < 3; c++) r1[c] /= norm;
+            float r2[3] = {nn[1] * r1[2] - nn[2] * r1[1], nn[2] * r1[0] - nn[0] * r1[2], nn[0] * r1[1] - nn[1] * r1[0]};
+            j->nsurf = S * S;
+            j->surf0 = (float*)malloc(3 * sizeof(float) * (size_t)j->nsurf);
+            j->surf = (float*)malloc(3 * sizeof(float) * (size_t)j->nsurf);
+            const float displ = p->indentationSurfaceStep;
+            for (int32_t a = 0; a < S; a++)
+                for (int32_t b = 0; b < S; b++) {
+                    const int32_t i1 = a - S / 2, i2 = b - S / 2;
+                    float* q = j->surf0 + 3 * (a * S + b);
+                    for (int c = 0; c < 3; c++) q[c] = r0[c] + i1 * displ * r1[c] + i2 * displ * r2[c];
+                }
+            memcpy(j->surf, j->surf0, 3 * sizeof(float) * (size_t)j->nsurf);
+            j->cap_mica = j->nsurf;
+            j->mica_cnt = (int32_t*)calloc(n, sizeof(int32_t));
+            j->mica_j = (int32_t*)malloc(sizeof(int32_t) * (size_t)n * j->cap_mica);
+        }
+    }
+    /* pulling plane (pulling_plane.cu:35-135) */
+    if (p->pullingPlane) {
+        float v[3] = {p->pullingPlaneDir[0], p->pullingPlaneDir[1], p->pullingPlaneDir[2]};
+        const float t = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        for (int c = 0; c < 3; c++) { j->plane_n[c] = v[c] / t; j->plane_p0[c] = p->pullingPlanePos[c]; }
+        j->plane_mask = (uint8_t*)calloc(n, 1);
+        j->plane_r0 = (float*)calloc(n, sizeof(float));
+        j->plane_f = (float*)calloc(n, sizeof(float));
+        for (int32_t i = 0; i < n; i++) {
+            const float* xi = F4(j->x, i);
+            float dr[3] = {xi[0] - j->plane_p0[0], xi[1] - j->plane_p0[1], xi[2] - j->plane_p0[2]};
+            j->plane_r0[i] = dr[0] * j->plane_n[0] + dr[1] * j->plane_n[1] + dr[2] * j->plane_n[2];
+        }
+        for (int32_t k = 0; k < d->nplane_pulled; k++) j->plane_mask[d->plane_pulled[k]] = 2;
+        for (int32_t k = 0; k < d->nplane_fixed; k++) j->plane_mask[d->plane_fixed[k]] = 1;
     }
     if (p->hi_on) {
         j->rf = (float*)calloc(4 * (size_t)n, sizeof(float));
@@ -346,7 +401,7 @@ void orc_job_destroy(orc_job* j) {
     void* ptrs[] = {j->cov_cnt, j->cov_j, j->cov_r0, j->nat_cnt, j->nat_j, j->nat_r02, j->nat_m12,
                     j->nat_r0d, j->nat_ehd, j->pp_cnt, j->pp_j, j->pl_cnt, j->pl_j, j->x, j->f, j->T,
                     j->extF, j->tipF, j->seeds, j->pulled, j->rf, j->mf, j->xc, j->ci4, j->eps, j->tensor,
-                    j->log};
+                    j->log, j->surf0, j->surf, j->mica_cnt, j->mica_j, j->plane_mask, j->plane_r0, j->plane_f};
     for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); k++) free(ptrs[k]);
     free(j);
 }
@@ -421,6 +476,24 @@ static inline void indentation_bead(orc_job* j, int32_t i, float* f) {
     fin[0] += df[0];
     fin[1] += df[1];
     fin[2] += df[2];
+    if (j->p.indentationDiscreteSurf) {
+        /* indentationDiscreteSurf_kernel (indentation_kernel.cu:130-180):
+         * the beads of the surface in the bead's list, no cutoff */
+        f[0] += df[0];
+        f[1] += df[1];
+        f[2] += df[2];
+        for (int32_t k = 0; k < j->mica_cnt[i]; k++) {
+            const float* q = j->surf + 3 * j->mica_j[(size_t)i * j->cap_mica + k];
+            float e[3] = {xi[0] - q[0], xi[1] - q[1], xi[2] - q[2]};
+            float w2 = 1.0f / (e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+            float s6 = w2 * w2 * w2;
+            float c = (j->surfAp * s6 + j->surfBp) * s6 * w2;
+            f[0] += e[0] * c;
+            f[1] += e[1] * c;
+            f[2] += e[2] * c;
+        }
+        return;
+    }
     float mx = xi[0] - j->micaR[0], my = xi[1] - j->micaR[1], mz = xi[2] - j->micaR[2];
     float d = mx * j->micaN[0] + my * j->micaN[1] + mz * j->micaN[2];
     d = 1.0f / d;
@@ -433,20 +506,41 @@ static inline void indentation_bead(orc_job* j, int32_t i, float* f) {
     f[2] += j->micaN[2] * w + df[2];
 }
 
+/* pullingPlane_kernel (src/Potentials/pulling_plane_kernel.cu:25-52): a
+ * spring along the plane normal to the fixed plane or the moving one. */
+static inline void plane_bead(orc_job* j, int32_t i, float* f) {
+    const int mask = j->plane_mask[i];
+    if (!mask) return;
+    const float* xi = F4(j->x, i);
+    float pc[3] = {j->plane_p0[0], j->plane_p0[1], j->plane_p0[2]};
+    if (mask == 2)
+        for (int c = 0; c < 3; c++) pc[c] += j->plane_displ * j->plane_n[c];
+    float dr = (xi[0] - pc[0]) * j->plane_n[0] + (xi[1] - pc[1]) * j->plane_n[1] + (xi[2] - pc[2]) * j->plane_n[2];
+    float df = -j->p.pullingPlaneKs * (dr - j->plane_r0[i]);
+    for (int c = 0; c < 3; c++) f[c] += df * j->plane_n[c];
+    j->plane_f[i] = df;
+}
+
 /* All potentials of one bead in registration order (gsop.cu:80-85). */
 static inline void potentials_bead(orc_job* j, int32_t i, float* f) {
     covalent_bead(j, i, f);
     native_bead(j, i, f);
     pairs_bead(j, i, f);
     if (j->p.indentation) indentation_bead(j, i, f);
+    if (j->p.pullingPlane) plane_bead(j, i, f);
 }
 
 void orc_job_forces(orc_job* j, float* out4, double* out4d, double* abs4d) {
     const int32_t n = j->n;
     float* save = NULL;
+    float* save_plane = NULL;
     if (j->p.indentation) { /* do not disturb the tip-force accumulator */
         save = (float*)malloc(16 * (size_t)n);
         memcpy(save, j->tipF, 16 * (size_t)n);
+    }
+    if (j->p.pullingPlane) {
+        save_plane = (float*)malloc(4 * (size_t)n);
+        memcpy(save_plane, j->plane_f, 4 * (size_t)n);
     }
     for (int32_t i = 0; i < n; i++) {
         if (out4) {
@@ -498,21 +592,50 @@ void orc_job_forces(orc_job* j, float* out4, double* out4d, double* abs4d) {
                 double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
                 double rho = r - j->tipR, r6 = 1.0 / (rho * rho * rho * rho * rho * rho);
                 double w = ((double)j->tipAp * r6 + j->tipBp) * r6 / (r * rho);
-                double m[3] = {(double)xi[0] - j->micaR[0], (double)xi[1] - j->micaR[1], (double)xi[2] - j->micaR[2]};
-                double dd = m[0] * j->micaN[0] + m[1] * j->micaN[1] + m[2] * j->micaN[2];
-                double s6 = 1.0 / (dd * dd * dd * dd * dd * dd);
-                double ws = ((double)j->surfAp * s6 + j->surfBp) * s6 / (dd * dd);
                 /* r - R_tip and the surface distance cancel: scale by the
                  * magnitudes that are subtracted */
                 double stip = fabs(w) * 7.0 * (r + j->tipR) / fabs(rho);
-                double mabs = fabs((double)xi[0] * j->micaN[0]) + fabs((double)xi[1] * j->micaN[1]) + fabs((double)xi[2] * j->micaN[2])
-                            + fabs((double)j->micaR[0] * j->micaN[0]) + fabs((double)j->micaR[1] * j->micaN[1]) + fabs((double)j->micaR[2] * j->micaN[2]);
-                double ssurf = fabs(ws) * 8.0 * mabs / fabs(dd);
-                for (int c = 0; c < 3; c++) {
-                    double t = w * d[c] + ws * j->micaN[c];
-                    fd[c] += t;
-                    fa[c] += stip * fabs(d[c]) + ssurf * fabs(j->micaN[c]);
+                if (j->p.indentationDiscreteSurf) {
+                    for (int c = 0; c < 3; c++) { fd[c] += w * d[c]; fa[c] += stip * fabs(d[c]); }
+                    for (int32_t k = 0; k < j->mica_cnt[i]; k++) {
+                        const float* q = j->surf + 3 * j->mica_j[(size_t)i * j->cap_mica + k];
+                        double e[3] = {(double)xi[0] - q[0], (double)xi[1] - q[1], (double)xi[2] - q[2]};
+                        double w2 = 1.0 / (e[0] * e[0] + e[1] * e[1] + e[2] * e[2]), s6 = w2 * w2 * w2;
+                        double cw = ((double)j->surfAp * s6 + j->surfBp) * s6 * w2;
+                        /* the difference cancels |x| + |q|; the A/B terms may cancel too */
+                        double sc = (fabs((double)j->surfAp * s6) + fabs((double)j->surfBp)) * s6 * w2 * 16.0;
+                        for (int c = 0; c < 3; c++) {
+                            fd[c] += cw * e[c];
+                            fa[c] += sc * (fabs((double)xi[c]) + fabs((double)q[c]));
+                        }
+                    }
+                } else {
+                    double m[3] = {(double)xi[0] - j->micaR[0], (double)xi[1] - j->micaR[1], (double)xi[2] - j->micaR[2]};
+                    double dd = m[0] * j->micaN[0] + m[1] * j->micaN[1] + m[2] * j->micaN[2];
+                    double s6 = 1.0 / (dd * dd * dd * dd * dd * dd);
+                    double ws = ((double)j->surfAp * s6 + j->surfBp) * s6 / (dd * dd);
+                    double mabs = fabs((double)xi[0] * j->micaN[0]) + fabs((double)xi[1] * j->micaN[1]) + fabs((double)xi[2] * j->micaN[2])
+                                + fabs((double)j->micaR[0] * j->micaN[0]) + fabs((double)j->micaR[1] * j->micaN[1]) + fabs((double)j->micaR[2] * j->micaN[2]);
+                    double ssurf = fabs(ws) * 8.0 * mabs / fabs(dd);
+                    for (int c = 0; c < 3; c++) {
+                        double t = w * d[c] + ws * j->micaN[c];
+                        fd[c] += t;
+                        fa[c] += stip * fabs(d[c]) + ssurf * fabs(j->micaN[c]);
+                    }
                 }
+            }
+            if (j->p.pullingPlane && j->plane_mask[i]) {
+                double pc[3] = {j->plane_p0[0], j->plane_p0[1], j->plane_p0[2]};
+                if (j->plane_mask[i] == 2)
+                    for (int c = 0; c < 3; c++) pc[c] += (double)j->plane_displ * j->plane_n[c];
+                double dr = ((double)xi[0] - pc[0]) * j->plane_n[0] + ((double)xi[1] - pc[1]) * j->plane_n[1] +
+                            ((double)xi[2] - pc[2]) * j->plane_n[2];
+                double df = -(double)j->p.pullingPlaneKs * (dr - j->plane_r0[i]);
+                /* dr - r0 cancels the plane distances */
+                double mag = 0;
+                for (int c = 0; c < 3; c++) mag += (fabs((double)xi[c]) + fabs(pc[c])) * fabs(j->plane_n[c]);
+                double sc = fabs((double)j->p.pullingPlaneKs) * (mag + fabs((double)j->plane_r0[i])) * 4.0;
+                for (int c = 0; c < 3; c++) { fd[c] += df * j->plane_n[c]; fa[c] += sc * fabs(j->plane_n[c]); }
             }
             if (out4d) { for (int c = 0; c < 3; c++) out4d[4 * i + c] = fd[c]; out4d[4 * i + 3] = 0; }
             if (abs4d) { for (int c = 0; c < 3; c++) abs4d[4 * i + c] = fa[c]; abs4d[4 * i + 3] = 0; }
@@ -521,6 +644,10 @@ void orc_job_forces(orc_job* j, float* out4, double* out4d, double* abs4d) {
     if (save) {
         memcpy(j->tipF, save, 16 * (size_t)n);
         free(save);
+    }
+    if (save_plane) {
+        memcpy(j->plane_f, save_plane, 4 * (size_t)n);
+        free(save_plane);
     }
 }
 
@@ -634,6 +761,23 @@ static void pulling_update(orc_job* j) {
     }
 }
 
+/* generateMicaList_kernel (src/Potentials/indentation_kernel.cu:182-201):
+ * the surface beads within indentationPairsCutoff of each bead, in surface
+ * order. */
+static void mica_list(orc_job* j) {
+    const float cut2 = j->p.indentationPairsCutoff * j->p.indentationPairsCutoff;
+    for (int32_t i = 0; i < j->n; i++) {
+        const float* xi = F4(j->x, i);
+        int32_t cnt = 0;
+        for (int32_t q = 0; q < j->nsurf; q++) {
+            const float* s = j->surf + 3 * q;
+            float e[3] = {xi[0] - s[0], xi[1] - s[1], xi[2] - s[2]};
+            if (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] < cut2) j->mica_j[(size_t)i * j->cap_mica + cnt++] = q;
+        }
+        j->mica_cnt[i] = cnt;
+    }
+}
+
 /* IndentationTipUpdater::update (src/Potentials/indentation.cu:414-550),
  * continuous surface. */
 static void indentation_update(orc_job* j) {
@@ -652,10 +796,16 @@ static void indentation_update(orc_job* j) {
     f[3] = sqrtf(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
     j->dx = (float)(j->step / p->nav) * j->V;
     if (p->indentationMoveSurface) {
-        for (int c = 0; c < 3; c++) j->micaR[c] = j->micaR0[c] + j->dir[c] * j->dx;
+        if (p->indentationDiscreteSurf) {
+            for (int32_t q = 0; q < j->nsurf; q++)
+                for (int c = 0; c < 3; c++) j->surf[3 * q + c] = j->surf0[3 * q + c] + j->dir[c] * j->dx;
+        } else {
+            for (int c = 0; c < 3; c++) j->micaR[c] = j->micaR0[c] + j->dir[c] * j->dx;
+        }
     } else {
         for (int c = 0; c < 3; c++) j->chip[c] = j->chip0[c] + j->dir[c] * j->dx;
     }
+    if (p->indentationDiscreteSurf) mica_list(j);
     float dr[3] = {j->chip[0] - j->tip[0], j->chip[1] - j->tip[1], j->chip[2] - j->tip[2]};
     float df[3];
     for (int c = 0; c < 3; c++) df[c] = -f[c] + dr[c] * j->cantKs;
@@ -670,6 +820,41 @@ static void indentation_update(orc_job* j) {
     const float v[12] = {f[0], f[1], f[2], f[3], sqrtf(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]), j->dx,
                          j->tip[0], j->tip[1], j->tip[2], j->chip[0], j->chip[1], j->chip[2]};
     log_append(j, SOPB_LOG_TIP, v);
+}
+
+/* PullingPlaneUpdater::update (src/Potentials/pulling_plane.cu:183-258),
+ * every stride: the cantilever moves by deltax per update period, the plane
+ * follows it by one overdamped step of update-period length against the
+ * beads' pull, summed in bead order from the last forces. */
+static void plane_update(orc_job* j) {
+    const sopb_params* p = &j->p;
+    const int32_t freq = p->pullingPlaneUpdateFreq > 0 ? p->pullingPlaneUpdateFreq : p->nav;
+    const int32_t ofreq = p->pullingPlaneOutputFreq > 0 ? p->pullingPlaneOutputFreq : p->nav;
+    const float xt = p->pullingPlaneDeltax * (float)j->step / (float)freq;
+    j->plane_cant = xt;
+    float ext = 0.0f;
+    for (int32_t i = 0; i < j->n; i++)
+        if (j->plane_mask[i] == 2) ext += j->plane_f[i];
+    const float cant = (xt - j->plane_displ) * p->pullingPlaneKsCant;
+    j->plane_displ += ((float)freq * p->timestep / p->pullingPlaneZeta) * (cant - ext);
+    if (j->step % ofreq == 0) {
+        float cf[3] = {0, 0, 0}, cp[3] = {0, 0, 0};
+        int32_t nf = 0, np = 0;
+        for (int32_t i = 0; i < j->n; i++) {
+            const float* xi = F4(j->x, i);
+            if (j->plane_mask[i] == 1) { for (int c = 0; c < 3; c++) cf[c] += xi[c]; nf++; }
+            if (j->plane_mask[i] == 2) { for (int c = 0; c < 3; c++) cp[c] += xi[c]; np++; }
+        }
+        for (int c = 0; c < 3; c++) { cf[c] /= (float)nf; cp[c] /= (float)np; }
+        float dx = cp[0] - cf[0], dy = cp[1] - cf[1], dz = cp[2] - cf[2];
+        float v[12] = {0};
+        v[0] = j->plane_displ;
+        v[1] = j->plane_cant;
+        v[2] = cant;
+        v[3] = ext;
+        v[4] = sqrtf(dx * dx + dy * dy + dz * dz);
+        log_append(j, SOPB_LOG_PLANE, v);
+    }
 }
 
 /* RPY block normalised by D_ii (src/Integrators/bdhitea_kernel.cu:67-87);
@@ -747,6 +932,7 @@ static void run_updaters(orc_job* j) {
     const sopb_params* p = &j->p;
     if (p->indentation) indentation_update(j);
     if (p->pulling && p->deltax != 0.0f) pulling_update(j);
+    if (p->pullingPlane) plane_update(j);
     if (j->step % p->possiblepairs_freq == 0) possiblepairs(j);
     if (j->step % p->nav == 0) memset(j->T, 0, j->n * sizeof(float)); /* output_manager.cu:125-127 */
     if (j->step % p->pairs_freq == 0) pairlist(j);

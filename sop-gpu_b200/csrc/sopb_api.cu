@@ -353,6 +353,7 @@ int32_t compute_stride(const sopb_params& p) {
     if (p.heating) mn(p.tempFreq);
     if (p.hi_on && !p.hi_exact) mn(p.hi_epsilon_freq);
     if (p.hi_on && p.hi_exact && p.hi_refresh > 1) mn(p.hi_refresh);   // the factor refresh is an updater
+    if (p.pullingPlane) mn(p.pullingPlaneUpdateFreq > 0 ? p.pullingPlaneUpdateFreq : p.nav);
     return s;
 }
 
@@ -510,6 +511,21 @@ int validate_desc(const sopb_job_desc* d) {
             if (d->fixed[k] < 0 || d->fixed[k] >= n) return SOPB_ERR_INVALID;
         for (int32_t k = 0; k < d->npulled; ++k)
             if (d->pulled[k] < 0 || d->pulled[k] >= n) return SOPB_ERR_INVALID;
+    }
+    if (p.pullingPlane) {
+        // PullingPlanePotential ctor checks (src/Potentials/pulling_plane.cu:60-74)
+        if (p.pullingPlaneDeltax == 0.0f || f3norm(p.pullingPlaneDir) == 0.0f || p.pullingPlaneZeta == 0.0f)
+            return SOPB_ERR_INVALID;
+        if (d->nplane_fixed < 0 || d->nplane_pulled < 0) return SOPB_ERR_INVALID;
+        if ((d->nplane_fixed && !d->plane_fixed) || (d->nplane_pulled && !d->plane_pulled)) return SOPB_ERR_INVALID;
+        for (int32_t k = 0; k < d->nplane_fixed; ++k)
+            if (d->plane_fixed[k] < 0 || d->plane_fixed[k] >= n) return SOPB_ERR_INVALID;
+        for (int32_t k = 0; k < d->nplane_pulled; ++k)
+            if (d->plane_pulled[k] < 0 || d->plane_pulled[k] >= n) return SOPB_ERR_INVALID;
+    }
+    if (p.indentation && p.indentationDiscreteSurf) {
+        if (p.indentationSurfaceSize <= 0 || p.indentationSurfaceSize > 1024 || p.indentationPairsCutoff <= 0.0f)
+            return SOPB_ERR_INVALID;
     }
     if (p.indentation) {
         if (p.indentationTipZeta == 0.0f) return SOPB_ERR_INVALID;
@@ -697,6 +713,12 @@ int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, bool ref
     if (updaters) {
         k_g_tip_partial<<<nb, kGridBlock, 0, st>>>(Jp, a);
         k_g_scalar_updaters<<<1, 32, 0, st>>>(Jp, a);
+        if (j->h.indent && j->h.discrete) {
+            const int sb = (int)std::min<int64_t>((j->h.nsurf + kGridBlock - 1) / kGridBlock, (int64_t)c->sm_count);
+            k_g_surf_move<<<sb, kGridBlock, 0, st>>>(Jp);
+            const int mb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
+            k_g_mica<<<mb, kGridBlock, 0, st>>>(Jp);
+        }
         k_g_treset<<<nb, kGridBlock, 0, st>>>(Jp);
         int rc = grid_possible(j, Jp, st, 0);
         if (rc) return rc;
@@ -806,8 +828,13 @@ extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
     b += n * (16 + 16 + 16 + 4 + 16 + 1);           // bead pools
     b += align256(n * std::min<int64_t>(n - 1, 2 * cap_pl) * 2) + align256(n * 4) + align256(n * 16);   // near list
     const sopb_params& p = d->params;
-    if ((p.pulling && p.deltax != 0.0f) || p.indentation)
+    if ((p.pulling && p.deltax != 0.0f) || p.indentation || p.pullingPlane)
         b += align256((size_t)(p.log_rows > 0 ? p.log_rows : 1024) * 64);                        // event log
+    if (p.indentation && p.indentationDiscreteSurf) {
+        const int64_t ns = (int64_t)p.indentationSurfaceSize * p.indentationSurfaceSize;
+        b += 2 * align256(ns * 16) + align256(n * ((ns + 31) / 32) * 4);                          // surface, lists
+    }
+    if (p.pullingPlane) b += align256(n) + 2 * align256(n * 4) + align256(n * 4 + 4);            // plane
     *bytes = b;
     return SOPB_OK;
 }
@@ -926,6 +953,70 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
         nd = f3norm(h.micaN);
         for (int c2 = 0; c2 < 3; ++c2) h.micaN[c2] /= nd;
     }
+    // discrete surface: the square of surface beads IndentationAminoUpdater
+    // builds from the configured (unnormalised) surface normal
+    // (indentation.cu:311-362); lists are rebuilt at every tip update
+    std::vector<float4> surf0;
+    if (p.indentation && p.indentationDiscreteSurf) {
+        const int32_t S = p.indentationSurfaceSize;
+        const float* nn = p.indentationSurfaceN;
+        const float* r0 = p.indentationSurfaceR0;
+        float r1[3];
+        if (nn[0] == 0.0f) { r1[0] = 1.0f; r1[1] = 0.0f; r1[2] = 0.0f; }
+        else if (nn[1] == 0.0f) { r1[0] = 0.0f; r1[1] = 1.0f; r1[2] = 0.0f; }
+        else if (nn[2] == 0.0f) { r1[0] = 0.0f; r1[1] = 0.0f; r1[2] = 1.0f; }
+        else { r1[0] = 0.0f; r1[1] = 1.0f; r1[2] = -(nn[1] / nn[2]) * r1[1]; }
+        const float nr = std::sqrt(r1[0] * r1[0] + r1[1] * r1[1] + r1[2] * r1[2]);
+        for (float& v : r1) v /= nr;
+        const float r2[3] = {nn[1] * r1[2] - nn[2] * r1[1], nn[2] * r1[0] - nn[0] * r1[2], nn[0] * r1[1] - nn[1] * r1[0]};
+        const float displ = p.indentationSurfaceStep;
+        for (int32_t a = 0; a < S; ++a)
+            for (int32_t b = 0; b < S; ++b) {
+                const int32_t i1 = a - S / 2, i2 = b - S / 2;
+                float q[3];
+                for (int c2 = 0; c2 < 3; ++c2) q[c2] = r0[c2] + i1 * displ * r1[c2] + i2 * displ * r2[c2];
+                surf0.push_back(make_float4(q[0], q[1], q[2], 0.0f));
+            }
+        h.discrete = 1;
+        h.nsurf = S * S;
+        h.Wm = (h.nsurf + 31) / 32;
+        h.mica_cut2 = p.indentationPairsCutoff * p.indentationPairsCutoff;
+    }
+    // pulling plane (PullingPlanePotential ctor, pulling_plane.cu:35-135):
+    // the masks (pulled, then fixed over them), each bead's distance from
+    // the plane at step 0, and the masked beads in bead order
+    std::vector<uint8_t> plane_mask;
+    std::vector<float> plane_r0;
+    std::vector<int32_t> plane_idx;
+    if (p.pullingPlane) {
+        h.plane = 1;
+        const float t = std::sqrt(p.pullingPlaneDir[0] * p.pullingPlaneDir[0] + p.pullingPlaneDir[1] * p.pullingPlaneDir[1] +
+                                  p.pullingPlaneDir[2] * p.pullingPlaneDir[2]);
+        for (int c2 = 0; c2 < 3; ++c2) {
+            h.plane_n[c2] = p.pullingPlaneDir[c2] / t;
+            h.plane_p0[c2] = p.pullingPlanePos[c2];
+        }
+        h.plane_ks = p.pullingPlaneKs;
+        h.plane_kscant = p.pullingPlaneKsCant;
+        h.plane_zeta = p.pullingPlaneZeta;
+        h.plane_deltax = p.pullingPlaneDeltax;
+        h.plane_freq = p.pullingPlaneUpdateFreq > 0 ? p.pullingPlaneUpdateFreq : p.nav;
+        h.plane_ofreq = p.pullingPlaneOutputFreq > 0 ? p.pullingPlaneOutputFreq : p.nav;
+        plane_mask.assign(n, 0);
+        plane_r0.resize(n);
+        for (int32_t i = 0; i < n; ++i) {
+            const float dr[3] = {x[i].x - h.plane_p0[0], x[i].y - h.plane_p0[1], x[i].z - h.plane_p0[2]};
+            plane_r0[i] = dr[0] * h.plane_n[0] + dr[1] * h.plane_n[1] + dr[2] * h.plane_n[2];
+        }
+        for (int32_t k = 0; k < d->nplane_pulled; ++k) plane_mask[d->plane_pulled[k]] = 2;
+        for (int32_t k = 0; k < d->nplane_fixed; ++k) plane_mask[d->plane_fixed[k]] = 1;
+        for (int want = 1; want <= 2; ++want)
+            for (int32_t i = 0; i < n; ++i)
+                if (plane_mask[i] == want) plane_idx.push_back(i);
+        h.nplane_fixed = 0;
+        for (int32_t i = 0; i < n; ++i) h.nplane_fixed += plane_mask[i] == 1;
+        h.nplane_pulled = (int32_t)plane_idx.size() - h.nplane_fixed;
+    }
     std::vector<uint32_t> seeds(4 * (size_t)n);
     if (d->seeds) std::memcpy(seeds.data(), d->seeds, seeds.size() * 4);
     else sopb_generate_seeds(d->seed, n, seeds.data());
@@ -1014,8 +1105,15 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     const size_t o_xref = o_nrc + (h.mask ? align256((size_t)n * 4) : 0);
     const size_t o_log = o_xref + (h.mask ? align256((size_t)n * 16) : 0);
     // event-log ring of the jobs whose updaters print per-update lines
-    h.log_cap = (h.ramp || h.indent) ? (p.log_rows > 0 ? p.log_rows : 1024) : 0;
-    const size_t total = o_log + align256((size_t)h.log_cap * 64);
+    h.log_cap = (h.ramp || h.indent || h.plane) ? (p.log_rows > 0 ? p.log_rows : 1024) : 0;
+    const size_t o_surf = o_log + align256((size_t)h.log_cap * 64);
+    const size_t o_surf0 = o_surf + align256((size_t)h.nsurf * 16);
+    const size_t o_mica = o_surf0 + align256((size_t)h.nsurf * 16);
+    const size_t o_pmask = o_mica + align256((size_t)n * h.Wm * 4);
+    const size_t o_pr0 = o_pmask + (h.plane ? align256((size_t)n) : 0);
+    const size_t o_pf = o_pr0 + (h.plane ? align256((size_t)n * 4) : 0);
+    const size_t o_pidx = o_pf + (h.plane ? align256((size_t)n * 4) : 0);
+    const size_t total = o_pidx + (h.plane ? align256(plane_idx.size() * 4 + 4) : 0);
     sopb_job* j = new (std::nothrow) sopb_job();
     if (!j) { c->beads.release(b0, n); return SOPB_ERR_NOMEM; }
     // stream-ordered allocation: a destroyed job's memory returns to the
@@ -1045,6 +1143,13 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.x_ref = h.mask ? (float4*)(base + o_xref) : nullptr;
     h.log = h.log_cap ? (float*)(base + o_log) : nullptr;
     h.log_head = 0;
+    h.surf = h.nsurf ? (float4*)(base + o_surf) : nullptr;
+    h.surf0 = h.nsurf ? (float4*)(base + o_surf0) : nullptr;
+    h.mica = h.nsurf ? (uint32_t*)(base + o_mica) : nullptr;
+    h.plane_mask = h.plane ? (uint8_t*)(base + o_pmask) : nullptr;
+    h.plane_r0 = h.plane ? (float*)(base + o_pr0) : nullptr;
+    h.plane_f = h.plane ? (float*)(base + o_pf) : nullptr;
+    h.plane_idx = h.plane ? (int32_t*)(base + o_pidx) : nullptr;
     h.nr_valid = 0;
     h.x = c->x + b0;
     h.xalt = c->xalt + b0;
@@ -1070,6 +1175,18 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     CUDA_TRY(cudaMemcpyAsync(h.flags, flags.data(), (size_t)n, cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemsetAsync(h.T, 0, (size_t)n * 4, st));
     CUDA_TRY(cudaMemsetAsync(h.tipF, 0, (size_t)n * 16, st));
+    if (h.nsurf) {
+        CUDA_TRY(cudaMemcpyAsync(h.surf, surf0.data(), (size_t)h.nsurf * 16, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(h.surf0, surf0.data(), (size_t)h.nsurf * 16, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemsetAsync(h.mica, 0, (size_t)n * h.Wm * 4, st));   // lists built at the first tip update
+    }
+    if (h.plane) {
+        CUDA_TRY(cudaMemcpyAsync(h.plane_mask, plane_mask.data(), (size_t)n, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(h.plane_r0, plane_r0.data(), (size_t)n * 4, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemsetAsync(h.plane_f, 0, (size_t)n * 4, st));
+        if (!plane_idx.empty())
+            CUDA_TRY(cudaMemcpyAsync(h.plane_idx, plane_idx.data(), plane_idx.size() * 4, cudaMemcpyHostToDevice, st));
+    }
     j->b0 = b0;   // the grid buffers are views of the job's bead range
     j->n = n;
     if (h.grid) {

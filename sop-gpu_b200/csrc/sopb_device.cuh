@@ -52,6 +52,14 @@ struct JobDev {
     uint8_t* flags;       // FLAG_*
     float4* xalt;         // second coordinate buffer (grid path ping-pong)
     float* log;           // [log_cap * 16] event-log ring (sopb_log_row), or null
+    // ---- discrete surface and pulling plane (views into the job's memory) ------
+    float4* surf;         // [nsurf] surface beads now
+    float4* surf0;        // [nsurf] surface beads at dx = 0
+    uint32_t* mica;       // [n * Wm] surface beads within the list cutoff, bitmask rows
+    uint8_t* plane_mask;  // [n] 1: spring to the fixed plane, 2: to the pulled plane
+    float* plane_r0;      // [n] distance from the plane at step 0
+    float* plane_f;       // [n] last spring force along the normal
+    int32_t* plane_idx;   // beads of the fixed plane, then of the pulled one, ascending
     // ---- maps ----------------------------------------------------------------
     int32_t* cov_off;     // [n+1]
     int32_t* cov_j;
@@ -92,6 +100,14 @@ struct JobDev {
     float tip[3], chip[3], chip0[3], dir[3], micaR[3], micaR0[3], micaN[3];
     float tipR, tipAp, tipBp, surfAp, surfBp, cantKs, V, dx, tipZeta;
     float fav[4];
+    int32_t discrete;     // 1: the surface is a square of beads with per-bead lists
+    int32_t nsurf, Wm;    // surface beads, words per bitmask row
+    float mica_cut2;      // indentationPairsCutoff^2
+    // ---- pulling plane (pulling_plane.cu) ----------------------------------------
+    int32_t plane, plane_freq, plane_ofreq, nplane_fixed, nplane_pulled, pad3;
+    float plane_n[3], plane_p0[3];
+    float plane_ks, plane_kscant, plane_zeta, plane_deltax;
+    float plane_displ, plane_cant;   // plane and cantilever displacement
     // ---- hydrodynamics (TEA / exact) ----------------------------------------------
     int32_t hi, hi_exact, hi_unlisted, hi_capricious, hi_bmode, hi_refresh;
     float hi_a, hi_epsmax;
@@ -197,6 +213,59 @@ struct IndentGeom {
     float tip[3], micaR[3], micaN[3];
     float tipR, tipAp, tipBp, surfAp, surfBp;
 };
+// The tip alone (the first half of indentationDiscreteSurf_kernel,
+// indentation_kernel.cu:130-157).
+__device__ __forceinline__ void tip_term(float4 xi, const IndentGeom& g, float3& f, float3& tipf) {
+    float dx = xi.x - g.tip[0], dy = xi.y - g.tip[1], dz = xi.z - g.tip[2];
+    float dw = __fsqrt_rn(dx * dx + dy * dy + dz * dz);
+    float r2 = __frcp_rn(dw - g.tipR);
+    r2 = r2 * r2;
+    float r6 = r2 * r2 * r2;
+    float w = g.tipAp * r6 + g.tipBp;
+    w = w * r6 / (dw * (dw - g.tipR));
+    tipf = make_float3(dx * w, dy * w, dz * w);
+    f.x += tipf.x;
+    f.y += tipf.y;
+    f.z += tipf.z;
+}
+
+// The surface beads of bead i's list, strided over the group's lanes
+// (indentationDiscreteSurf_kernel's list loop, indentation_kernel.cu:159-177;
+// no cutoff inside the list).
+__device__ __forceinline__ void mica_partial(const JobDev& J, int i, float4 xi, int l, int lpb, float3& f) {
+    const uint32_t* row = J.mica + (size_t)i * J.Wm;
+    for (int w = l; w < J.Wm; w += lpb) {
+        uint32_t bits = row[w];
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const float4 q = J.surf[32 * w + b];
+            const float ex = xi.x - q.x, ey = xi.y - q.y, ez = xi.z - q.z;
+            const float w2 = 1.0f / (ex * ex + ey * ey + ez * ez);
+            const float s6 = w2 * w2 * w2;
+            const float c = (J.surfAp * s6 + J.surfBp) * s6 * w2;
+            f.x += ex * c;
+            f.y += ey * c;
+            f.z += ez * c;
+        }
+    }
+}
+
+// pullingPlane_kernel (src/Potentials/pulling_plane_kernel.cu:25-52): a
+// spring along the normal to the fixed plane (mask 1) or to the plane
+// displaced by `displ` (mask 2).  Returns the spring force.
+__device__ __forceinline__ float plane_term(const JobDev& J, float displ, int mask, float4 xi, float r0, float3& f) {
+    float pc[3] = {J.plane_p0[0], J.plane_p0[1], J.plane_p0[2]};
+    if (mask == 2)
+        for (int c = 0; c < 3; ++c) pc[c] += displ * J.plane_n[c];
+    const float dr = (xi.x - pc[0]) * J.plane_n[0] + (xi.y - pc[1]) * J.plane_n[1] + (xi.z - pc[2]) * J.plane_n[2];
+    const float df = -J.plane_ks * (dr - r0);
+    f.x += df * J.plane_n[0];
+    f.y += df * J.plane_n[1];
+    f.z += df * J.plane_n[2];
+    return df;
+}
+
 __device__ __forceinline__ void indentation_term(float4 xi, const IndentGeom& g, float3& f, float3& tipf) {
     float dx = xi.x - g.tip[0], dy = xi.y - g.tip[1], dz = xi.z - g.tip[2];
     float dw = __fsqrt_rn(dx * dx + dy * dy + dz * dz);

@@ -77,15 +77,21 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
         if (act) {
             bonded_partial(J, global_bonded(J), J.x, i, xi, l, lpb, f);
             pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
+            if (J.discrete) mica_partial(J, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {
             if (J.indent) {
                 float3 tf;
-                indentation_term(xi, ig, f, tf);
+                if (J.discrete) tip_term(xi, ig, f, tf);
+                else indentation_term(xi, ig, f, tf);
                 float4 t = J.tipF[i];
                 t.x += tf.x; t.y += tf.y; t.z += tf.z;
                 J.tipF[i] = t;
+            }
+            if (J.plane) {
+                const int mask = J.plane_mask[i];
+                if (mask) J.plane_f[i] = plane_term(J, J.plane_displ, mask, xi, J.plane_r0[i], f);
             }
             aux.F[i] = make_float4(f.x, f.y, f.z, 0.f);
         }
@@ -159,6 +165,8 @@ __global__ void k_g_scalar_updaters(JobDev* __restrict__ Jp, GridAux aux) {
     sc.dx = J.dx;
     for (int c = 0; c < 4; ++c) sc.fav[c] = J.fav[c];
     sc.log_head = J.log_head;
+    sc.plane_displ = J.plane_displ;
+    sc.plane_cant = J.plane_cant;
     if (J.indent) {
         if (step == J.retraction_step) sc.V = -sc.V;
         if (step % J.nav == 0) {
@@ -175,6 +183,7 @@ __global__ void k_g_scalar_updaters(JobDev* __restrict__ Jp, GridAux aux) {
         for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
         if (step % J.pull_freq == 0) log_pull(J, sc, xe, J.x[J.fixedEnd], step);
     }
+    if (J.plane) plane_update(J, sc, J.x, step);
     if (J.heating && step % J.temp_freq == 0) {
         const float temp = __fadd_rn(J.initialT, __fmul_rn((float)(step / J.temp_freq), J.deltaT));
         sc.var = __fsqrt_rn(__fdiv_rn(__fmul_rn(__fmul_rn(2.0f, temp), J.zeta), J.h));
@@ -188,6 +197,44 @@ __global__ void k_g_scalar_updaters(JobDev* __restrict__ Jp, GridAux aux) {
     J.dx = sc.dx;
     for (int c = 0; c < 4; ++c) J.fav[c] = sc.fav[c];
     J.log_head = sc.log_head;
+    J.plane_displ = sc.plane_displ;
+    J.plane_cant = sc.plane_cant;
+}
+
+// Discrete surface at a tip update (after k_g_scalar_updaters moved dx):
+// the surface beads follow dx when the surface moves (indentation.cu:446-455).
+__global__ void __launch_bounds__(kGridBlock)
+k_g_surf_move(JobDev* __restrict__ Jp) {
+    const int64_t step = job_step(Jp);
+    const JobDev& J = *Jp;
+    if (!J.indent || !J.discrete || !J.moveSurface || J.status || step % J.stride != 0 || step % J.nav != 0) return;
+    const float dx = J.dx;
+    for (int q = blockIdx.x * kGridBlock + threadIdx.x; q < J.nsurf; q += gridDim.x * kGridBlock) {
+        const float4 s0 = J.surf0[q];
+        J.surf[q] = make_float4(__fadd_rn(s0.x, __fmul_rn(J.dir[0], dx)), __fadd_rn(s0.y, __fmul_rn(J.dir[1], dx)),
+                                __fadd_rn(s0.z, __fmul_rn(J.dir[2], dx)), 0.f);
+    }
+}
+
+// Every bead's surface-bead list (generateMicaList_kernel,
+// indentation_kernel.cu:182-201) as a bitmask row, a warp per bead.
+__global__ void __launch_bounds__(kGridBlock)
+k_g_mica(JobDev* __restrict__ Jp) {
+    const int64_t step = job_step(Jp);
+    const JobDev& J = *Jp;
+    if (!J.indent || !J.discrete || J.status || step % J.stride != 0 || step % J.nav != 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (kGridBlock / 32);
+    for (int i = blockIdx.x * (kGridBlock / 32) + (threadIdx.x >> 5); i < J.n; i += warps) {
+        const float4 xi = J.x[i];
+        uint32_t* row = J.mica + (size_t)i * J.Wm;
+        for (int wd = 0; wd < J.Wm; ++wd) {
+            const int q = 32 * wd + lane;
+            const bool in = q < J.nsurf && dist2_rn(xi, J.surf[q]) < J.mica_cut2;
+            const uint32_t m = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) row[wd] = m;
+        }
+    }
 }
 
 // Temperature-accumulator reset at nav (output_manager.cu:125-127).

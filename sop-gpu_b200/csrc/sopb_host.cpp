@@ -26,8 +26,8 @@ extern "C" const char* sopb_status_string(int status) {
 // Defaults of the PARAMETER() declarations: src/Integrators/langevin.h:12-23,
 // src/Potentials/covalent.h:12-14, pairs.h:12-15, native.h:11-12,
 // src/Updaters/pairlist.h:12-14, possiblepairlist.h:12-13, src/gsop.h:34,
-// src/Potentials/pulling.h:15-26, indentation.h:12-38,
-// src/Integrators/bdhitea.h:15-21.
+// src/Potentials/pulling.h:15-26, indentation.h:12-47, pulling_plane.h:12-27,
+// src/Integrators/bdhitea.h:15-21.  Frequencies that default to nav are 0.
 extern "C" void sopb_default_params(sopb_params* p) {
     std::memset(p, 0, sizeof(*p));
     p->zeta = 50.0f;
@@ -57,6 +57,12 @@ extern "C" void sopb_default_params(sopb_params* p) {
     p->indentationSurfB = 1.0f;
     p->indentationTipZeta = 5000.0f;
     p->indentationRetractionStep = -1;
+    p->indentationSurfaceSize = 51;
+    p->indentationSurfaceStep = 1.4f;
+    p->indentationPairsCutoff = 40.0f;
+    p->pullingPlaneKs = 0.05f;
+    p->pullingPlaneKsCant = 0.05f;
+    p->pullingPlaneZeta = 200.0f;
     p->hi_a = 1.8f;
     p->hi_capricious = 1;
     p->hi_unlisted = 1;

@@ -86,6 +86,7 @@ struct StepScalars {
     int32_t err;
     int32_t nr_valid;   // the job's near list is usable (written back at the end)
     uint32_t log_head;  // event-log rows appended (written back at the end)
+    float plane_displ, plane_cant;   // pulling plane (written back at the end)
 };
 
 // Cooperative copy of a job descriptor into shared memory (read by every
@@ -342,6 +343,72 @@ __device__ __noinline__ void log_pull(const JobDev& J, StepScalars& sc, float4 x
     log_row(J, sc.log_head, SOPB_LOG_PULL, step, v);
 }
 
+// PullingPlaneUpdater::update (src/Potentials/pulling_plane.cu:183-258), run
+// every stride by one thread: the cantilever moves by deltax per update
+// period; the plane takes one overdamped step of update-period length under
+// the cantilever spring and the beads' springs, summed in bead order from
+// the forces of the last step; every output period one log line with the
+// distance between the centroids of the fixed and the pulled beads.  Host
+// arithmetic in the reference: explicit _rn operations.
+__device__ __noinline__ void plane_update(const JobDev& J, StepScalars& sc, const float4* __restrict__ xs, int64_t step) {
+    const float xt = __fdiv_rn(__fmul_rn(J.plane_deltax, (float)step), (float)J.plane_freq);
+    sc.plane_cant = xt;
+    const int32_t* fixed = J.plane_idx;
+    const int32_t* pulled = J.plane_idx + J.nplane_fixed;
+    float ext = 0.0f;
+    for (int k = 0; k < J.nplane_pulled; ++k) ext = __fadd_rn(ext, J.plane_f[pulled[k]]);
+    const float cant = __fmul_rn(__fsub_rn(xt, sc.plane_displ), J.plane_kscant);
+    const float mult = __fdiv_rn(__fmul_rn((float)J.plane_freq, J.h), J.plane_zeta);
+    sc.plane_displ = __fadd_rn(sc.plane_displ, __fmul_rn(mult, __fsub_rn(cant, ext)));
+    if (step % J.plane_ofreq == 0) {
+        float cf[3] = {0.f, 0.f, 0.f}, cp[3] = {0.f, 0.f, 0.f};
+        for (int k = 0; k < J.nplane_fixed; ++k) {
+            const float4 q = xs[fixed[k]];
+            cf[0] = __fadd_rn(cf[0], q.x); cf[1] = __fadd_rn(cf[1], q.y); cf[2] = __fadd_rn(cf[2], q.z);
+        }
+        for (int k = 0; k < J.nplane_pulled; ++k) {
+            const float4 q = xs[pulled[k]];
+            cp[0] = __fadd_rn(cp[0], q.x); cp[1] = __fadd_rn(cp[1], q.y); cp[2] = __fadd_rn(cp[2], q.z);
+        }
+        float d[3];
+        for (int c = 0; c < 3; ++c)
+            d[c] = __fsub_rn(__fdiv_rn(cp[c], (float)J.nplane_pulled), __fdiv_rn(cf[c], (float)J.nplane_fixed));
+        const float e2e = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])), __fmul_rn(d[2], d[2])));
+        const float v[12] = {sc.plane_displ, xt, cant, ext, e2e, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        log_row(J, sc.log_head, SOPB_LOG_PLANE, step, v);
+    }
+}
+
+// Discrete surface at a tip update: the surface beads follow dx when the
+// surface moves (IndentationTipUpdater::update, indentation.cu:446-455), then
+// every bead's list of surface beads within the cutoff is rebuilt
+// (generateMicaList_kernel, indentation_kernel.cu:182-201) as a bitmask row,
+// a warp per bead and a ballot per 32 surface beads.
+template <int BLOCK>
+__device__ void build_mica(const JobDev& J, const float4* __restrict__ xs, float dx) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (J.moveSurface) {
+        for (int q = tid; q < J.nsurf; q += BLOCK) {
+            const float4 s0 = J.surf0[q];
+            J.surf[q] = make_float4(__fadd_rn(s0.x, __fmul_rn(J.dir[0], dx)), __fadd_rn(s0.y, __fmul_rn(J.dir[1], dx)),
+                                    __fadd_rn(s0.z, __fmul_rn(J.dir[2], dx)), 0.f);
+        }
+        __syncthreads();
+    }
+    for (int i = w; i < J.n; i += BLOCK / 32) {
+        const float4 xi = xs[i];
+        uint32_t* row = J.mica + (size_t)i * J.Wm;
+        for (int wd = 0; wd < J.Wm; ++wd) {
+            const int q = 32 * wd + lane;
+            bool in = false;
+            if (q < J.nsurf) in = dist2_rn(xi, J.surf[q]) < J.mica_cut2;
+            const uint32_t m = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) row[wd] = m;
+        }
+    }
+    __syncthreads();
+}
+
 // IndentationTipUpdater::update (src/Potentials/indentation.cu:414-550) for
 // the continuous surface, run by thread 0 after the CTA summed the tip force.
 // Host-side arithmetic of the reference is IEEE without contraction, hence
@@ -444,6 +511,10 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
             }
             const float3 s = block_sum3<BLOCK>(p, red);
             if (tid == 0) tip_update(J, sc, s, step);
+            if (J.discrete) {
+                __syncthreads();
+                build_mica<BLOCK>(J, xs, sc.dx);
+            }
         }
     }
     if (J.pulling && J.ramp && tid == 0) {
@@ -455,6 +526,7 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
         for (int c = 0; c < 3; ++c) sc.cant[c] = __fadd_rn(J.cant0[c], __fmul_rn(xt, J.pullvec[c]));
         if (step % J.pull_freq == 0) log_pull(J, sc, xe, xs[J.fixedEnd], step);
     }
+    if (J.plane && tid == 0) plane_update(J, sc, xs, step);
     const bool pp = step % J.pp_freq == 0;
     if (pp) build_possible<BLOCK>(J, xs, err);
     if (step % J.nav == 0)
@@ -543,6 +615,8 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
         sc.err = 0;
         sc.nr_valid = J.nr_valid;
         sc.log_head = J.log_head;
+        sc.plane_displ = J.plane_displ;
+        sc.plane_cant = J.plane_cant;
     }
     __syncthreads();
     const int cap = J.lcache;
@@ -573,15 +647,21 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
             if (i < n) {
                 bonded_partial(J, B, xs, i, xi, l, lpb, f);
                 pairs_partial(J, xs, off, nbr, cap, i, xi, l, lpb, f);
+                if (J.discrete) mica_partial(J, i, xi, l, lpb, f);
             }
             f = group_reduce(f, lpb);
             if (l == 0 && i < n) {
                 if (J.indent) {
                     float3 tf;
-                    indentation_term(xi, sc.ig, f, tf);
+                    if (J.discrete) tip_term(xi, sc.ig, f, tf);
+                    else indentation_term(xi, sc.ig, f, tf);
                     float4 t = J.tipF[i];
                     t.x += tf.x; t.y += tf.y; t.z += tf.z;
                     J.tipF[i] = t;
+                }
+                if (J.plane) {
+                    const int mask = J.plane_mask[i];
+                    if (mask) J.plane_f[i] = plane_term(J, sc.plane_displ, mask, xi, J.plane_r0[i], f);
                 }
                 F[i] = make_float4(f.x, f.y, f.z, 0.f);
             }
@@ -636,6 +716,8 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
         for (int c = 0; c < 4; ++c) Jp->fav[c] = sc.fav[c];
         Jp->nr_valid = sc.nr_valid;
         Jp->log_head = sc.log_head;
+        Jp->plane_displ = sc.plane_displ;
+        Jp->plane_cant = sc.plane_cant;
         if (sc.err) Jp->status = sc.err;
     }
 }
@@ -662,12 +744,18 @@ k_forces_only(const JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, 
         if (act) {
             bonded_partial(J, global_bonded(J), J.x, i, xi, l, lpb, f);
             pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
+            if (J.discrete) mica_partial(J, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {
             if (J.indent) {
                 float3 tf;
-                indentation_term(xi, ig, f, tf);
+                if (J.discrete) tip_term(xi, ig, f, tf);
+                else indentation_term(xi, ig, f, tf);
+            }
+            if (J.plane) {
+                const int mask = J.plane_mask[i];
+                if (mask) plane_term(J, J.plane_displ, mask, xi, J.plane_r0[i], f);
             }
             out[i] = make_float4(f.x, f.y, f.z, 0.f);
         }

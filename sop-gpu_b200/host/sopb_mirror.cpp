@@ -314,6 +314,10 @@ Simulation::Simulation(const Config& c, int device) : cfg(c) {
         d.fixed = fixed.data();
         d.npulled = (int32_t)pulled.size();
         d.pulled = pulled.data();
+        d.nplane_fixed = (int32_t)plane_fixed.size();
+        d.plane_fixed = plane_fixed.data();
+        d.nplane_pulled = (int32_t)plane_pulled.size();
+        d.plane_pulled = plane_pulled.data();
         d.seeds = seeds.data() + 4 * (size_t)r * n;
         d.params = params;
         sopb_job* j = nullptr;
@@ -362,8 +366,14 @@ void Simulation::initFF() {
     // createIndentationPotential (indentation.cu:19-66): tip updater first
     if (g.boolean("indentation", false)) {
         if (ntr > 1) throw Error(SOPB_ERR_INVALID, "Many-runs-per-GPU mode is not supported by indentation potential.");
-        if (g.boolean("indentationDiscreteSurf", false)) throw Error(SOPB_ERR_UNSUPPORTED, "discrete-surface indentation");
         p.indentation = 1;
+        if (g.boolean("indentationDiscreteSurf", false)) {
+            // the surface as a square of beads (indentation.cu:137-201)
+            p.indentationDiscreteSurf = 1;
+            p.indentationSurfaceSize = (int32_t)g.integer("indentationSurfaceSize", 51);
+            p.indentationSurfaceStep = g.real("indentationSurfaceStep", 1.4f);
+            p.indentationPairsCutoff = g.real("indentationPairsCutoff", 40.0f);
+        }
         g.float3("indentationChip", p.indentationChip);
         g.float3("indentationTip", p.indentationTip, p.indentationChip);
         g.float3("indentationDirection", p.indentationDirection);
@@ -386,6 +396,10 @@ void Simulation::initFF() {
         p.indentationTipZeta = g.real("indentationTipZeta", 5000.0f);
         p.indentationRetractionStep = g.integer("indentationRetractionStep", -1);
         updaters.emplace_back(new NamedUpdater("Indentation", p.nav));
+        // the tip and surface beads of the output files; a discrete surface
+        // forces them (indentation.cu:24-32)
+        if (p.indentationDiscreteSurf || g.boolean("indentationShowTipSurf", false))
+            updaters.emplace_back(new NamedUpdater("AdditionalAminos", (int)g.integer("outputtiming", 10000)));
         potentials.emplace_back(new NamedPotential("Indentation"));
     }
     // createPullingPotential (pulling.cu:22-35)
@@ -415,6 +429,27 @@ void Simulation::initFF() {
         potentials.emplace_back(new NamedPotential("Pulling"));
         if (p.deltax != 0.0f) updaters.emplace_back(new NamedUpdater("Pulling", p.pullFreq));
     }
+    // createPullingPlanePotential (pulling_plane.cu:17-30)
+    if (g.boolean("pullingPlane", false)) {
+        p.pullingPlane = 1;
+        p.pullingPlaneDeltax = g.real("pullingPlaneDeltax", 0.0f);
+        if (p.pullingPlaneDeltax == 0.0f)
+            throw Error(SOPB_ERR_INVALID, "'pullingPlaneDeltax' parameter should be specified to initiate this->");
+        if (g.has("plane_fixed_beads") || g.has("plane_pulled_beads"))
+            throw Error(SOPB_ERR_INVALID,
+                        "'plane_fixed_beads' and 'plane_pulled_beads' parameters are deprecated. Use 'plane_fixed' and 'plane_pulled' instead");
+        p.pullingPlaneKs = g.real("pullingPlaneKs", p.pullingPlaneKs);
+        p.pullingPlaneKsCant = g.real("pullingPlaneKsCant", p.pullingPlaneKsCant);
+        p.pullingPlaneZeta = g.real("pullingPlaneZeta", p.pullingPlaneZeta);
+        for (int i : g.ints("plane_fixed")) plane_fixed.push_back(i);
+        for (int i : g.ints("plane_pulled")) plane_pulled.push_back(i);
+        g.float3("pullingPlaneDir", p.pullingPlaneDir);
+        g.float3("pullingPlanePos", p.pullingPlanePos);
+        p.pullingPlaneUpdateFreq = (int32_t)g.integer("pullingPlaneUpdateFreq", p.nav);
+        p.pullingPlaneOutputFreq = (int32_t)g.integer("pullingPlaneOutputFreq", p.nav);
+        potentials.emplace_back(new NamedPotential("Pulling Plane"));
+        updaters.emplace_back(new NamedUpdater("Pulling Plane", p.pullingPlaneUpdateFreq));
+    }
     updaters.emplace_back(new ListUpdater("Possiblepairlist", p.possiblepairs_freq, 1));
     updaters.emplace_back(new NamedUpdater("DAT output", (int)g.integer("outputtiming", 10000)));
     updaters.emplace_back(new ListUpdater("Pairlist", p.pairs_freq, 0));
@@ -433,13 +468,15 @@ void Simulation::initFF() {
             p.hi_unlisted = g.boolean("hi_unlisted", true);
             updaters.emplace_back(new NamedUpdater("BDHI-TEA updater", p.hi_epsilon_freq));
         }
+        p.hi_refresh = (int32_t)g.integer("hi_refresh", 1);
+        if (p.hi_exact && p.hi_refresh > 1) updaters.emplace_back(new NamedUpdater("Cholesky refresh", p.hi_refresh));
         const std::string bm = g.str("hi_b_mode", "cholesky");
         p.hi_b_mode = bm == "reference" ? SOPB_HI_B_REFCOMPAT : SOPB_HI_B_CHOLESKY;
         integrator.reset(new NamedIntegrator("BDHI-TEA", p.timestep));
     } else {
         integrator.reset(new NamedIntegrator("Langevin", p.timestep));
     }
-    p.log_rows = 4096;   // event-log ring of the pulling / indentation lines
+    p.log_rows = 4096;   // event-log ring of the pulling, indentation and plane lines
     // runGPU's stride (src/gsop.cu:117-122)
     stride = p.nav;
     for (auto& u : updaters) stride = std::min(stride, u->frequency);

@@ -138,6 +138,7 @@ public:
     int stride = 1;
     sopb_params params{};
     std::vector<int32_t> fixed, pulled;
+    std::vector<int32_t> plane_fixed, plane_pulled;   // pulling plane masks
     std::vector<std::vector<float>> coords;     // per run, xyz[3n]
     std::vector<uint32_t> seeds;                // all runs, one ran2 stream
     sopb_context* ctx = nullptr;

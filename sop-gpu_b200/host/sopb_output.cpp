@@ -137,9 +137,9 @@ private:
     const Config& cfg;
     const int n;
     int64_t dat_freq, dcd_freq, restart_freq, amino_freq = 0;
-    std::vector<std::string> dat_files, dcd_files, restart_files, pull_files;
+    std::vector<std::string> dat_files, dcd_files, restart_files, pull_files, plane_files;
     std::string indent_file;
-    bool rg, tea, pull_log, indent_log, show_tip;
+    bool rg, tea, pull_log, indent_log, show_tip, plane_log;
     int width, print_runs;
     std::vector<Atom> atoms, extra;
     std::deque<Frame> pending;
@@ -167,7 +167,10 @@ OutputManagers::OutputManagers(Simulation& s)
     print_runs = (int)g.integer("printruns", 10);
     pull_log = p.pulling && p.deltax != 0.0f;
     indent_log = p.indentation != 0;
-    show_tip = indent_log && g.boolean("indentationShowTipSurf", false);
+    // a discrete surface forces the tip and surface beads into the files
+    // (indentation.cu:24-32)
+    show_tip = indent_log && (p.indentationDiscreteSurf || g.boolean("indentationShowTipSurf", false));
+    plane_log = p.pullingPlane != 0;
     atoms = s.top.atoms;
     if (p.pulling) {
         // the beta column marks pulled (2) and fixed (1) beads
@@ -175,6 +178,12 @@ OutputManagers::OutputManagers(Simulation& s)
         for (Atom& a : atoms) a.beta = 0.0;
         for (int32_t i : s.pulled) atoms[i].beta = 2.0;
         for (int32_t i : s.fixed) atoms[i].beta = 1.0;
+    }
+    if (plane_log) {
+        // the pulling plane's masks, created after pulling (pulling_plane.cu:98-117)
+        for (Atom& a : atoms) a.beta = 0.0;
+        for (int32_t i : s.plane_pulled) atoms[i].beta = 2.0;
+        for (int32_t i : s.plane_fixed) atoms[i].beta = 1.0;
     }
     for (int r = 0; r < s.ntr; ++r) {
         const int run = r + s.firstrun;
@@ -184,6 +193,9 @@ OutputManagers::OutputManagers(Simulation& s)
             replace_run(g.str("restartname", "restart." + g.str("name", "unnamed") + "_<run>.pdb"), run));
         if (pull_log)
             pull_files.push_back(replace_run(g.str("pullOutput", "pull." + g.str("name", "unnamed") + "_<run>.dat"), run));
+        if (plane_log)
+            plane_files.push_back(
+                replace_run(g.str("pullingPlaneOutput", "pullplane." + g.str("name", "unnamed") + "_<run>.dat"), run));
     }
     if (indent_log) {
         indent_freq = g.integer("indentationOutputFreq", 1000);
@@ -277,11 +289,12 @@ OutputManagers::OutputManagers(Simulation& s)
         std::fclose(open_or_throw(dat_files[r], "w"));
         dcd_write_header(dcd_files[r], n + (int)extra.size(), (int)dcd_freq, 0.0f);
         if (pull_log) std::fclose(open_or_throw(pull_files[r], "w"));
+        if (plane_log) std::fclose(open_or_throw(plane_files[r], "w"));
     }
     if (indent_log) std::fclose(open_or_throw(indent_file, "w"));
     // one event-log row per updater pass at most: a run of this many steps
     // cannot wrap the ring
-    if (pull_log || indent_log) max_run_ = (int64_t)(p.log_rows - 2) * s.stride;
+    if (pull_log || indent_log || plane_log) max_run_ = (int64_t)(p.log_rows - 2) * s.stride;
 }
 
 int64_t OutputManagers::next_event(int64_t step) const {
@@ -432,7 +445,7 @@ void OutputManagers::tip_row(const sopb_log_row& row) {
 void OutputManagers::after_run(int64_t step) {
     // every row of the steps before `step` is on the device now
     std::vector<std::vector<sopb_log_row>> rows(sim.ntr);
-    if (pull_log || indent_log) {
+    if (pull_log || indent_log || plane_log) {
         for (int r = 0; r < sim.ntr; ++r) {
             std::vector<sopb_log_row> buf(4096);
             for (;;) {
@@ -450,6 +463,17 @@ void OutputManagers::after_run(int64_t step) {
                 if (q.kind == SOPB_LOG_PULL)
                     std::fprintf(f, "%12lld\t%5.3f\t%5.3f\t%5.3f\t%5.3f\t%5.3f\t%5.3f\n", (long long)q.step, q.v[0],
                                  q.v[1], q.v[2], q.v[3], q.v[4], q.v[5]);
+            std::fclose(f);
+        }
+    }
+    if (plane_log) {
+        // PullingPlaneUpdater::update's lines (pulling_plane.cu:234-246)
+        for (int r = 0; r < sim.ntr; ++r) {
+            FILE* f = open_or_throw(plane_files[r], "a");
+            for (const sopb_log_row& q : rows[r])
+                if (q.kind == SOPB_LOG_PLANE)
+                    std::fprintf(f, "%12lld\t%f\t%f\t%f\t%f\t%f\n", (long long)q.step, q.v[0], q.v[1], q.v[2], q.v[3],
+                                 q.v[4]);
             std::fclose(f);
         }
     }

@@ -22,7 +22,7 @@ HI_B_CHOLESKY, HI_B_REFCOMPAT = 0, 1
 COORDS, SEEDS, TEMP, FORCES, TIPFORCES, PULLSTATE, TIPSTATE, HISTATE, HIFACTOR, OBSERVABLES = range(10)
 OBSERVABLE_NAMES = ("T", "E_fene", "E_native", "E_pairs", "E_total", "native_contacts", "Rg", "tea_eps")
 # event-log rows (sopb_log_row): pulling lines every pullFreq, tip lines every nav
-LOG_PULL, LOG_TIP = 1, 2
+LOG_PULL, LOG_TIP, LOG_PLANE = 1, 2, 3
 LOG_ROW = np.dtype([("kind", "<i4"), ("pad", "<i4"), ("step", "<i8"), ("v", "<f4", (12,))])
 
 F3 = C.c_float * 3
@@ -56,7 +56,13 @@ class Params(C.Structure):
         ("hi_capricious", C.c_int32), ("hi_unlisted", C.c_int32), ("hi_epsmax", C.c_float),
         ("hi_b_mode", C.c_int32), ("hi_refresh", C.c_int32), ("lanes_per_bead", C.c_int32),
         ("cell_list", C.c_int32), ("grid_path", C.c_int32), ("R_limit_bond", C.c_float),
-        ("log_rows", C.c_int32), ("reserved", C.c_int32 * 3),
+        ("log_rows", C.c_int32),
+        ("indentationDiscreteSurf", C.c_int32), ("indentationSurfaceSize", C.c_int32),
+        ("indentationSurfaceStep", C.c_float), ("indentationPairsCutoff", C.c_float),
+        ("pullingPlane", C.c_int32), ("pullingPlaneDeltax", C.c_float), ("pullingPlaneKs", C.c_float),
+        ("pullingPlaneKsCant", C.c_float), ("pullingPlaneZeta", C.c_float), ("pullingPlaneDir", F3),
+        ("pullingPlanePos", F3), ("pullingPlaneUpdateFreq", C.c_int32), ("pullingPlaneOutputFreq", C.c_int32),
+        ("reserved2", C.c_int32 * 4),
     ]
 
 
@@ -68,6 +74,8 @@ class JobDesc(C.Structure):
         ("nfixed", C.c_int32), ("fixed", C.c_void_p), ("npulled", C.c_int32), ("pulled", C.c_void_p),
         ("seeds", C.c_void_p), ("seed", C.c_int32), ("reserved", C.c_int32),
         ("params", Params),
+        ("nplane_fixed", C.c_int32), ("plane_fixed", C.c_void_p),
+        ("nplane_pulled", C.c_int32), ("plane_pulled", C.c_void_p),
     ]
 
 
@@ -169,7 +177,8 @@ class JobSpec:
     """
 
     def __init__(self, xyz, bonds, bonds_r0, natives, natives_r0, natives_eh, params: Params,
-                 fixed: Sequence[int] = (), pulled: Sequence[int] = (), seeds: Optional[np.ndarray] = None, seed: int = 0):
+                 fixed: Sequence[int] = (), pulled: Sequence[int] = (), seeds: Optional[np.ndarray] = None, seed: int = 0,
+                 plane_fixed: Sequence[int] = (), plane_pulled: Sequence[int] = ()):
         self.xyz = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
         self.bonds = np.ascontiguousarray(bonds, np.int32).reshape(-1, 2)
         self.bonds_r0 = np.ascontiguousarray(bonds_r0, np.float32).reshape(-1)
@@ -181,6 +190,8 @@ class JobSpec:
         self.seeds = None if seeds is None else np.ascontiguousarray(seeds, np.uint32).reshape(-1, 4)
         self.seed = int(seed)
         self.params = params
+        self.plane_fixed = np.ascontiguousarray(plane_fixed, np.int32).reshape(-1)
+        self.plane_pulled = np.ascontiguousarray(plane_pulled, np.int32).reshape(-1)
 
     @classmethod
     def from_system(cls, sys_, params: Params, **kw) -> "JobSpec":
@@ -208,6 +219,10 @@ class JobSpec:
         d.seeds = self.seeds.ctypes.data if self.seeds is not None else None
         d.seed = self.seed
         d.params = self.params
+        d.nplane_fixed = self.plane_fixed.shape[0]
+        d.plane_fixed = self.plane_fixed.ctypes.data
+        d.nplane_pulled = self.plane_pulled.shape[0]
+        d.plane_pulled = self.plane_pulled.ctypes.data
         return d
 
     def footprint(self) -> int:

@@ -135,6 +135,8 @@ class JobConfig:
     numsteps: int
     topology: str
     coordinates: List[str]   # per run, <run> substituted
+    plane_fixed: List[int] = dataclasses.field(default_factory=list)
+    plane_pulled: List[int] = dataclasses.field(default_factory=list)
 
 
 def job_config(cfg: Config) -> JobConfig:
@@ -181,7 +183,11 @@ def job_config(cfg: Config) -> JobConfig:
         if ntr > 1:
             raise ConfigError("Many-runs-per-GPU mode is not supported by indentation potential.")
         if g.get_bool("indentationDiscreteSurf", False):
-            raise ConfigError("discrete-surface indentation is not supported by this library")
+            # the surface as a square of beads (indentation.cu:137-201)
+            p.indentationDiscreteSurf = 1
+            p.indentationSurfaceSize = g.get_int("indentationSurfaceSize", 51)
+            p.indentationSurfaceStep = g.get_float("indentationSurfaceStep", 1.4)
+            p.indentationPairsCutoff = g.get_float("indentationPairsCutoff", 40.0)
         chip = g.get_float3("indentationChip")
         sopb.set_param(p, "indentationChip", chip)
         sopb.set_param(p, "indentationTip", g.get_float3("indentationTip", chip))
@@ -200,6 +206,24 @@ def job_config(cfg: Config) -> JobConfig:
                      ("indentationTipZeta", 5000.0)):
             setattr(p, k, g.get_float(k, d))
         p.indentationRetractionStep = g.get_int("indentationRetractionStep", -1)
+    plane_fixed: List[int] = []
+    plane_pulled: List[int] = []
+    p.pullingPlane = int(g.get_bool("pullingPlane", False))
+    if p.pullingPlane:
+        # PullingPlanePotential ctor (src/Potentials/pulling_plane.cu:35-135)
+        p.pullingPlaneDeltax = g.get_float("pullingPlaneDeltax", 0.0)
+        if p.pullingPlaneDeltax == 0:
+            raise ConfigError("'pullingPlaneDeltax' parameter should be specified to initiate this->")
+        if g.has("plane_fixed_beads") or g.has("plane_pulled_beads"):
+            raise ConfigError("'plane_fixed_beads' and 'plane_pulled_beads' parameters are deprecated. "
+                              "Use 'plane_fixed' and 'plane_pulled' instead")
+        for k, d in (("pullingPlaneKs", 0.05), ("pullingPlaneKsCant", 0.05), ("pullingPlaneZeta", 200.0)):
+            setattr(p, k, g.get_float(k, d))
+        plane_fixed, plane_pulled = g.get_ints("plane_fixed"), g.get_ints("plane_pulled")
+        sopb.set_param(p, "pullingPlaneDir", g.get_float3("pullingPlaneDir"))
+        sopb.set_param(p, "pullingPlanePos", g.get_float3("pullingPlanePos"))
+        p.pullingPlaneUpdateFreq = g.get_int("pullingPlaneUpdateFreq", p.nav)
+        p.pullingPlaneOutputFreq = g.get_int("pullingPlaneOutputFreq", p.nav)
     p.hi_on = int(g.get_bool("hi_on", False))
     if p.hi_on:
         if p.minimization:
@@ -217,14 +241,19 @@ def job_config(cfg: Config) -> JobConfig:
         freqs.append(g.get_int("outputtiming", 10000))
     if p.pulling and p.deltax != 0:
         freqs.append(p.pullFreq)
+    if p.pullingPlane:
+        freqs.append(p.pullingPlaneUpdateFreq)
     if p.heating:
         freqs.append(p.tempFreq)
     if p.hi_on and not p.hi_exact:
         freqs.append(p.hi_epsilon_freq)
+    if p.hi_on and p.hi_exact and p.hi_refresh > 1:
+        freqs.append(p.hi_refresh)      # the factor refresh is an updater of this library
     p.stride = min(freqs)
     seed = g.get_int("seed") + firstrun
     coords = [g.get_str("coordinates").replace("<run>", str(r + firstrun)) for r in range(ntr)]
-    return JobConfig(p, fixed, pulled, seed, ntr, firstrun, g.get_int("numsteps"), g.get_str("topology"), coords)
+    return JobConfig(p, fixed, pulled, seed, ntr, firstrun, g.get_int("numsteps"), g.get_str("topology"), coords,
+                     plane_fixed, plane_pulled)
 
 
 def job_specs(jc: JobConfig, systems) -> List["sopb.JobSpec"]:
@@ -235,5 +264,6 @@ def job_specs(jc: JobConfig, systems) -> List["sopb.JobSpec"]:
     out = []
     for r, s in enumerate(systems):
         out.append(sopb.JobSpec.from_system(s, jc.params, fixed=jc.fixed, pulled=jc.pulled,
-                                            seeds=seeds[r * n:(r + 1) * n]))
+                                            seeds=seeds[r * n:(r + 1) * n], plane_fixed=jc.plane_fixed,
+                                            plane_pulled=jc.plane_pulled))
     return out

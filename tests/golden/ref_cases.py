@@ -70,6 +70,35 @@ CASES = {
         "run": "1", "seed": "777", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
         "hi_on": "yes", "hi_a": "1.9", "hi_unlisted": "yes", "hi_capricious": "no", "hi_epsilon_freq": "10",
         "outputtiming": "10", "dcdfreq": "10"}),
+    # pulling plane, two runs (one plane displacement each)
+    "plane": dict(n=150, sys_seed=17, runs=2, total=100, dumps=[1, 50, 100], files=True, cfg={
+        "runnum": "2", "firstrun": "1", "seed": "2468", "nav": "1000", "max_pairs": "200",
+        "max_possiblePairs": "200", "pullingPlane": "on", "pullingPlaneDeltax": "0.5", "pullingPlaneKs": "0.5",
+        "pullingPlaneKsCant": "0.2", "pullingPlaneZeta": "50", "pullingPlaneDir": "0.0 0.6 0.8",
+        "plane_fixed": "0 to 4", "plane_pulled": "145 to 149", "pullingPlaneUpdateFreq": "10",
+        "pullingPlaneOutputFreq": "20", "pullingPlaneOutput": "<name>_<run>_plane.dat", "outputtiming": "50",
+        "dcdfreq": "50"}),
+    # indentation on a discrete surface (surface-bead lists), chip moving
+    "mica": dict(n=200, sys_seed=13, runs=1, total=100, dumps=[1, 40, 100], files=True, cfg={
+        "run": "1", "seed": "4711", "nav": "20", "max_pairs": "256", "max_possiblePairs": "256",
+        "indentation": "on", "indentationTipR": "20.0", "indentationKs": "0.07", "indentationDeltaX": "0.05",
+        "indentationDirection": "0.0 1.0 0.0", "indentationSurfaceN": "0.0 -1.0 0.0", "indentationTipZeta": "500",
+        "indentationSurfA": "1.0", "indentationSurfB": "-2.0", "indentationSurfSigma": "3.0",
+        "indentationSurfEl": "0.2", "indentationFixTrans": "yes", "indentationOutput": "<name>_indent.dat",
+        "indentationOutputFreq": "20", "indentationDiscreteSurf": "yes", "indentationSurfaceSize": "15",
+        "indentationSurfaceStep": "3.0", "indentationPairsCutoff": "12.0", "indentationCantLength": "50.0",
+        "indentationSurfConnectFile": "<name>_mica.vmd", "outputtiming": "20", "dcdfreq": "40"}),
+    # the same with the surface moving towards the tip
+    "micamove": dict(n=200, sys_seed=13, runs=1, total=100, dumps=[1, 40, 100], files=True, cfg={
+        "run": "1", "seed": "4712", "nav": "20", "max_pairs": "256", "max_possiblePairs": "256",
+        "indentation": "on", "indentationTipR": "20.0", "indentationKs": "0.07", "indentationDeltaX": "-0.5",
+        "indentationDirection": "0.0 1.0 0.0", "indentationSurfaceN": "0.0 -1.0 0.0", "indentationTipZeta": "500",
+        "indentationSurfA": "1.0", "indentationSurfB": "-2.0", "indentationSurfSigma": "3.0",
+        "indentationSurfEl": "0.2", "indentationFixTrans": "yes", "indentationOutput": "<name>_indent.dat",
+        "indentationOutputFreq": "20", "indentationDiscreteSurf": "yes", "indentationSurfaceSize": "15",
+        "indentationSurfaceStep": "3.0", "indentationPairsCutoff": "12.0", "indentationMoveSurface": "yes",
+        "indentationCantLength": "50.0", "indentationSurfConnectFile": "<name>_mica.vmd", "outputtiming": "20",
+        "dcdfreq": "40"}),
     "heat": dict(n=100, sys_seed=6, runs=1, total=45, dumps=[45], cfg={
         "run": "1", "seed": "5", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
         "heating": "on", "initialT": "0.1", "deltaT": "0.2", "tempFreq": "10"}),
@@ -102,7 +131,13 @@ def config_text(name):
         tip = "%.4f %.4f %.4f" % (x[:, 0].mean(), top - 22.0, x[:, 2].mean())
         cfg["indentationChip"] = tip
         cfg["indentationTip"] = tip
-        cfg["indentationSurfaceR0"] = "0.0 %.4f 0.0" % (x[:, 1].max() + 6.0)
+        if c["cfg"].get("indentationDiscreteSurf") == "yes":    # the bead square under the chain
+            cfg["indentationSurfaceR0"] = "%.4f %.4f %.4f" % (x[:, 0].mean(), x[:, 1].max() + 6.0, x[:, 2].mean())
+        else:
+            cfg["indentationSurfaceR0"] = "0.0 %.4f 0.0" % (x[:, 1].max() + 6.0)
+    if c["cfg"].get("pullingPlane") == "on":
+        x = systems(name)[0].xyz.astype(np.float64)
+        cfg["pullingPlanePos"] = "%.4f %.4f %.4f" % tuple(x.mean(axis=0))
     return "".join("%s\t%s\n" % (k, v) for k, v in cfg.items())
 
 

@@ -189,6 +189,22 @@ def test_oracle_reproduces_pulling_lines(name):
         assert np.allclose(L["v"][:, :6], ref[:, 1:], atol=5.01e-4 + 1e-4)
 
 
+@pytest.mark.parametrize("name", [c for c in golden_cases() if ref_cases.CASES[c]["cfg"].get("pullingPlane")])
+def test_oracle_reproduces_plane_lines(name):
+    g, jc, specs = load(name)
+    c = ref_cases.CASES[name]
+    first = int(c["cfg"].get("firstrun", c["cfg"].get("run", "1")))
+    for r, sp in enumerate(specs):
+        ref = floats(dat_rows(gfile(g, "%s_%d_plane.dat" % (name, first + r))))
+        o = O.OracleJob(sp)
+        assert o.advance(c["total"]) == 0
+        L = o.log()
+        assert np.all(L["kind"] == 3)
+        assert np.array_equal(L["step"], ref[:, 0].astype(np.int64))
+        # printed with %f: 6 decimals
+        assert np.allclose(L["v"][:, :5], ref[:, 1:], rtol=1e-5, atol=1.5e-6)
+
+
 @pytest.mark.parametrize("name", [c for c in golden_cases() if ref_cases.CASES[c]["cfg"].get("indentation")])
 def test_oracle_reproduces_indentation_lines(name):
     g, jc, specs = load(name)

@@ -19,6 +19,14 @@ mkdir -p "$OUT"
     "$REF/src/Util/wrapper.cpp" "$REF/src/Util/mystl.cpp"
 echo "built $OUT/ref_host"
 
+# The reference's topology creator (src/sop-top.cpp, host code only), for
+# the golden files of the topology tool.
+/usr/bin/g++ -O2 -w -std=c++11 -I"$REF/src" -I/usr/local/cuda/include \
+    -o "$OUT/ref_sop_top" "$REF/src/sop-top.cpp" "$REF/src/IO/configreader.cpp" \
+    "$REF/src/IO/topio.cpp" "$REF/src/IO/pdbio.cpp" \
+    "$REF/src/Util/wrapper.cpp" "$REF/src/Util/mystl.cpp"
+echo "built $OUT/ref_sop_top"
+
 # The reference's CUDA path for sm_100a (golden harness ref_gpu).  As
 # shipped it targets sm_30 with texture references, both gone from CUDA 12:
 # -DNOTEXTURE selects its plain-load path and ref_texture_shim.h covers the

@@ -230,7 +230,7 @@ void save_pdb(const std::string& path, const std::vector<Atom>& atoms, const std
         for (const Atom& a : *set)
             std::fprintf(f, hex ? "ATOM  %5x %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n"
                                 : "ATOM  %5d %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n",
-                         ++id, a.name.c_str(), ' ', a.resName.c_str(), a.chain, a.resid, (double)a.x, (double)a.y,
+                         ++id, a.name.c_str(), a.altLoc, a.resName.c_str(), a.chain, a.resid, (double)a.x, (double)a.y,
                          (double)a.z, a.occupancy, a.beta);
     int last = -1;
     for (size_t b = 0; b + 1 < bonds.size(); b += 2) {

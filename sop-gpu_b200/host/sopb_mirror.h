@@ -53,10 +53,10 @@ private:
 // ---- topology and coordinates (src/IO/topio.cpp, src/IO/pdbio.cpp) --------
 struct Atom {                      // one PDB ATOM record (PDBAtom)
     std::string name = "CA", resName = "ALA";
-    char chain = 'A';
+    char altLoc = ' ', chain = 'A';
     int resid = 0;
     double occupancy = 0.0, beta = 0.0;
-    float x = 0.0f, y = 0.0f, z = 0.0f;
+    double x = 0.0, y = 0.0, z = 0.0;
 };
 struct Topology {
     int natoms = 0;

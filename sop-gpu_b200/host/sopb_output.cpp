@@ -263,7 +263,7 @@ OutputManagers::OutputManagers(Simulation& s)
                 m.x = m0[0] + i1 * step * r1[0] + i2 * step * r2[0];
                 m.y = m0[1] + i1 * step * r1[1] + i2 * step * r2[1];
                 m.z = m0[2] + i1 * step * r1[2] + i2 * step * r2[2];
-                surf0.insert(surf0.end(), {m.x, m.y, m.z});
+                surf0.insert(surf0.end(), {(float)m.x, (float)m.y, (float)m.z});
                 extra.push_back(m);
             }
         // VMD script joining the cantilever beads and the surface grid

@@ -1,0 +1,38 @@
+"""Runs the reference's own topology creator (oracle/_ref/ref_sop_top, built
+from src/sop-top.cpp by oracle/build_ref.sh) on every case of
+soptop_cases.py and packs its .top and coordinate files into soptop.npz
+(byte arrays "<case>.top", "<case>_ca.pdb").
+
+    python tests/golden/make_soptop_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, HERE)
+import soptop_cases  # noqa: E402
+
+REF = os.path.join(REPO, "oracle", "_ref", "ref_sop_top")
+
+
+def main():
+    arrays = {}
+    for name in soptop_cases.CASES:
+        with tempfile.TemporaryDirectory() as d:
+            cfg = soptop_cases.write_case(name, d)
+            subprocess.run([REF, os.path.basename(cfg)], cwd=d, check=True, stdout=subprocess.DEVNULL,
+                           stdin=subprocess.DEVNULL)
+            for f in (name + ".top", name + "_ca.pdb"):
+                with open(os.path.join(d, f), "rb") as fh:
+                    arrays[f] = np.frombuffer(fh.read(), np.uint8)
+    np.savez_compressed(os.path.join(HERE, "soptop.npz"), **arrays)
+    print("cases:", ", ".join(soptop_cases.CASES))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,90 @@
+"""Cases for the topology builder: a seeded synthetic all-atom structure
+(backbone N, CA, C, O and side-chain atoms, two chains, an SSBOND record)
+and configs in the reference topology creator's format.  Used by
+make_soptop_golden.py (golden files from the reference's own sop-top) and by
+tests/test_soptop.py."""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "sop-gpu_b200"))
+import sopb_synth as S  # noqa: E402
+
+RESNAMES = ["ALA", "GLY", "SER", "LEU", "VAL", "THR", "ASP", "ASN", "ILE", "PHE"]
+
+
+def structure(seed=5, chains=(("A", 45), ("B", 25))):
+    """PDB text of the structure, and the residues made CYS/LYS/GLU for the
+    SS bond and the covalent linker."""
+    rng = np.random.default_rng(seed)
+    n = sum(c for _, c in chains)
+    ca = S.random_walk(n, seed).astype(np.float64)
+    lines = []
+    atom = 0
+    res = []
+    k = 0
+    for ch, cnt in chains:
+        for r in range(1, cnt + 1):
+            res.append((ch, r, k))
+            k += 1
+    names = {i: RESNAMES[rng.integers(len(RESNAMES))] for i in range(n)}
+    # an SS bond between the closest pair of residues of different chains
+    ia = [i for c, r, i in res if c == chains[0][0]]
+    ib = [i for c, r, i in res if c != chains[0][0]]
+    d = np.linalg.norm(ca[ia][:, None, :] - ca[ib][None, :, :], axis=2)
+    p, q = np.unravel_index(np.argmin(d), d.shape)
+    ss = (ia[p], ib[q])
+    names[ss[0]] = names[ss[1]] = "CYS"
+    names[7] = "LYS"          # chain A resid 8
+    names[29] = "GLU"         # chain A resid 30
+    for c, r, i in res:
+        if c != chains[0][0] and names[i] in ("LYS", "GLU"):
+            names[i] = "ALA"
+    for c, r, i in res:
+        x = ca[i]
+        occ = 0.5 + rng.random() * 1.5
+        beta = 0.2 + rng.random() * 2.0
+        gly = names[i] == "GLY"
+        atoms = [("N", x + rng.normal(scale=0.9, size=3)), ("CA", x), ("C", x + rng.normal(scale=0.9, size=3)),
+                 ("O", x + rng.normal(scale=1.3, size=3))]
+        if not gly:
+            atoms.append(("CB", x + rng.normal(scale=1.2, size=3)))
+            if rng.random() < 0.6:
+                atoms.append(("CG", x + rng.normal(scale=2.2, size=3)))
+        for nm, pos in atoms:
+            atom += 1
+            lines.append("ATOM  %5d %-4s%c%3s %c%4d    %8.3f%8.3f%8.3f%6.2f%6.2f\n"
+                         % (atom, " " + nm if len(nm) < 4 else nm, " ", names[i], c, r, pos[0], pos[1], pos[2],
+                            occ, beta))
+    sa, sb = res[ss[0]], res[ss[1]]
+    head = "SSBOND %3d CYS %c %4d    CYS %c %4d\n" % (1, sa[0], sa[1], sb[0], sb[1])
+    return head + "".join(lines) + "END\n"
+
+
+BASE = {"structure": "aa.pdb"}
+
+CASES = {
+    "basic": {"eh": "1.5"},
+    "sidechain": {"eh": "O", "SC_limit_bond": "4.0", "covalentRepulsion": "yes", "pairs_threshold": "25.0"},
+    "linker": {"eh": "B", "covLinkersCount": "1", "covLinker1": "LYS8-GLU30", "covLinkersCutoff": "30.0",
+               "R_limit_bond": "7.0", "SS_cutoff": "40.0"},
+    "tandem": {"eh": "1.2", "createTandem": "yes", "linkerLength": "3", "monomerCount": "2", "fixedEnd": "0",
+               "pulledEnd": "44", "pairs_threshold": "30.0"},
+    "tandemvec": {"eh": "1.0", "createTandem": "yes", "linkerLength": "2", "monomerCount": "3", "fixedEnd": "0",
+                  "pulledEnd": "69", "tandemDirection": "vector", "tandemVectorX": "1.0", "tandemVectorY": "0.5",
+                  "tandemVectorZ": "0.0", "covalentRepulsion": "yes", "pairs_threshold": "20.0"},
+}
+
+
+def write_case(name, d):
+    """Writes aa.pdb and <name>.conf into d; returns the config path."""
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "aa.pdb"), "w") as f:
+        f.write(structure())
+    cfg = dict(BASE, topology=name + ".top", coordinates=name + "_ca.pdb", **CASES[name])
+    path = os.path.join(d, name + ".conf")
+    with open(path, "w") as f:
+        f.write("".join("%s %s\n" % kv for kv in cfg.items()))
+    return path

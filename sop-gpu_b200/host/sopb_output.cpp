@@ -521,7 +521,7 @@ void Simulation::runGPU() {
     for (;;) {
         if (step <= last) out.at_step(step);
         int64_t next = std::min(out.next_event(step), total);
-        next = std::min(next, step + out.max_run());
+        if (out.max_run() < next - step) next = step + out.max_run();   // (no overflow when unbounded)
         run(next - step);
         step = next;
         out.after_run(step);

@@ -134,7 +134,7 @@ def test_reference_files_decode(name):
     last = (c["total"] - 1) // jc.params.stride * jc.params.stride
     nframes = last // dcdfreq + 1
     extra = 0
-    if cfg.get("indentationShowTipSurf") == "yes":
+    if cfg.get("indentationShowTipSurf") == "yes" or cfg.get("indentationDiscreteSurf") == "yes":
         extra = 2 + int(cfg["indentationSurfaceSize"]) ** 2
     for r, sp in enumerate(specs):
         hdr, fr = read_dcd(gfile(g, "%s_%d.dcd" % (name, first + r)))

@@ -26,6 +26,11 @@ echo "built $OUT/ref_host"
     "$REF/src/IO/topio.cpp" "$REF/src/IO/pdbio.cpp" \
     "$REF/src/Util/wrapper.cpp" "$REF/src/Util/mystl.cpp"
 echo "built $OUT/ref_sop_top"
+/usr/bin/g++ -O2 -w -std=c++11 -I"$REF/src" -I/usr/local/cuda/include \
+    -o "$OUT/ref_sop_top2" "$REF/src/sop-top2.cpp" "$REF"/src/TopologyCreator/*.cpp \
+    "$REF/src/IO/configreader.cpp" "$REF/src/Util/wrapper.cpp" "$REF/src/Util/mystl.cpp" \
+    "$REF/src/Util/parameters.cpp"
+echo "built $OUT/ref_sop_top2"
 
 # The reference's CUDA path for sm_100a (golden harness ref_gpu).  As
 # shipped it targets sm_30 with texture references, both gone from CUDA 12:

@@ -1,7 +1,10 @@
-"""The topology builder `sopb-top` against the reference's own topology
-creator (src/sop-top.cpp, run by tests/golden/make_soptop_golden.py): the
-.top file and the Calpha coordinates PDB byte for byte, for plain,
-side-chain-contact, covalent-linker and tandem models.  The one tolerated
+"""The topology builders against the reference's own topology creators
+(run by tests/golden/make_soptop_golden.py).  `sopb-top` (src/sop-top.cpp):
+the .top file and the Calpha coordinates PDB byte for byte, for plain,
+side-chain-contact, covalent-linker and tandem models.  `sopb-top2`
+(src/sop-top2.cpp): the coarse-grained PDB, .top and the two PSF files byte
+for byte, for one- and two-bead-per-residue descriptions, segments or
+chains, and an extra-bond file.  The one tolerated
 difference: the reference leaves the alternate-location column of its linker
 beads uninitialised (a NUL byte in the golden files); sopb-top writes a
 space there."""
@@ -16,15 +19,28 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 GOLD = os.path.join(HERE, "golden")
 TOOL = os.path.join(REPO, "sop-gpu_b200", "sopb-top")
+TOOL2 = os.path.join(REPO, "sop-gpu_b200", "sopb-top2")
 sys.path.insert(0, GOLD)
 import soptop_cases  # noqa: E402
 
 
 @pytest.fixture(scope="module")
 def tool():
-    if not os.path.exists(TOOL):
+    if not (os.path.exists(TOOL) and os.path.exists(TOOL2)):
         subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "sop-gpu_b200")])
     return TOOL
+
+
+@pytest.mark.parametrize("name", list(soptop_cases.CG_CASES))
+def test_coarse_grained_model_matches_reference_tool(tmp_path, tool, name):
+    g = np.load(os.path.join(GOLD, "soptop.npz"))
+    cfg = soptop_cases.write_cg_case(name, str(tmp_path))
+    r = subprocess.run([TOOL2, os.path.basename(cfg)], cwd=str(tmp_path), capture_output=True, text=True,
+                       stdin=subprocess.DEVNULL)
+    assert r.returncode == 0, r.stderr
+    for f in (name + "_cg.pdb", name + ".top", name + ".psf", name + "_nat.psf"):
+        with open(tmp_path / f, "rb") as fh:
+            assert fh.read() == bytes(g[f]), f
 
 
 @pytest.mark.parametrize("name", list(soptop_cases.CASES))

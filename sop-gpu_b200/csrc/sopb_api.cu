@@ -151,6 +151,7 @@ struct sopb_job {
     cudaEvent_t la_fork = nullptr, la_join = nullptr;
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
     uint32_t log_tail = 0;             // event-log rows drained so far
+    bool ev_lazy = false;              // ev not yet recorded after the work on st (see job_ev)
 };
 
 #define CUDA_TRY(call)                                                                         \
@@ -317,7 +318,21 @@ void reclaim(sopb_context* c, bool wait) {
 
 // The io stream after the job's last work (its work on other streams after
 // that is unrelated); `modify`: the job's next work comes after this io.
+// A job's event, recorded now on the job's stream if its last work left it
+// unrecorded.  Batch operations on one stream (a run, a bulk copy) mark their
+// jobs instead of recording an event per job: the event is recorded when
+// something first has to wait for it, and then covers everything ordered on
+// that stream so far (the job's work included).
+int job_ev(sopb_job* j) {
+    if (j->ev_lazy) {
+        CUDA_TRY(cudaEventRecord(j->ev, j->st));
+        j->ev_lazy = false;
+    }
+    return SOPB_OK;
+}
+
 int io_begin(sopb_job* j) {
+    SOPB_TRY(job_ev(j));
     CUDA_TRY(cudaStreamWaitEvent(j->ctx->io, j->ev, 0));
     return SOPB_OK;
 }
@@ -326,12 +341,14 @@ int io_end(sopb_job* j, bool modify) {
     if (modify) {
         CUDA_TRY(cudaEventRecord(j->ev, c->io));
         j->st = c->io;
+        j->ev_lazy = false;
     }
     CUDA_TRY(cudaStreamSynchronize(c->io));
     return SOPB_OK;
 }
 
 int read_slot(sopb_job* j) {
+    SOPB_TRY(job_ev(j));
     CUDA_TRY(cudaEventSynchronize(j->ev));
     CUDA_TRY(cudaMemcpy(&j->h, &j->ctx->d_jobs[j->slot], sizeof(JobDev), cudaMemcpyDeviceToHost));
     return SOPB_OK;
@@ -476,7 +493,10 @@ extern "C" int sopb_context_sync(sopb_context* c) {
     CUDA_TRY(cudaSetDevice(c->device));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     for (sopb_job* j : c->slots)
-        if (j) CUDA_TRY(cudaEventSynchronize(j->ev));
+        if (j) {
+            SOPB_TRY(job_ev(j));
+            CUDA_TRY(cudaEventSynchronize(j->ev));
+        }
     return SOPB_OK;
 }
 
@@ -1229,6 +1249,7 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
         cudaEventDestroy(j->la_fork);
         cudaEventDestroy(j->la_join);
     }
+    SOPB_TRY(job_ev(j));
     CUDA_TRY(cudaStreamWaitEvent(c->io, j->ev, 0));
     if (j->amem) CUDA_TRY(cudaFreeAsync(j->amem, c->io));
     CUDA_TRY(cudaFreeAsync(j->dmem, c->io));
@@ -1292,6 +1313,7 @@ extern "C" int sopb_run_ragged(sopb_context* c, sopb_job* const* jobs, int32_t n
     for (int32_t k = 0; k < njobs; ++k) {
         sopb_job* j = jobs[k];
         if (j->st != st) {
+            SOPB_TRY(job_ev(j));
             CUDA_TRY(cudaStreamWaitEvent(st, j->ev, 0));
             j->st = st;
         }
@@ -1305,8 +1327,8 @@ extern "C" int sopb_run_ragged(sopb_context* c, sopb_job* const* jobs, int32_t n
             n.push_back(nsteps[k]);
         }
     int rc = act.empty() ? SOPB_OK : run_ordered(c, act.data(), (int32_t)act.size(), n.data(), st);
-    // the jobs' last work is this run
-    for (int32_t k = 0; k < njobs; ++k) CUDA_TRY(cudaEventRecord(jobs[k]->ev, st));
+    // the jobs' last work is this run (their events are recorded on demand)
+    for (int32_t k = 0; k < njobs; ++k) jobs[k]->ev_lazy = true;
     return rc;
 }
 
@@ -1627,6 +1649,7 @@ int bulk_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, void* hos
     for (int32_t k = 0; k < njobs; ++k) {
         sopb_job* j = jobs[k];
         if (j->st != c->stream) {
+            SOPB_TRY(job_ev(j));
             CUDA_TRY(cudaStreamWaitEvent(c->stream, j->ev, 0));
             j->st = c->stream;
         }
@@ -1648,8 +1671,8 @@ int bulk_coords(sopb_context* c, sopb_job* const* jobs, int32_t njobs, void* hos
             h += b;
         }
     }
-    if (up)   // the jobs' next work comes after the upload
-        for (int32_t k = 0; k < njobs; ++k) CUDA_TRY(cudaEventRecord(jobs[k]->ev, c->stream));
+    if (up)   // the jobs' next work comes after the upload (events on demand)
+        for (int32_t k = 0; k < njobs; ++k) jobs[k]->ev_lazy = true;
     return SOPB_OK;
 }
 }  // namespace

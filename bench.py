@@ -267,11 +267,11 @@ def run_gpu(args):
     specs = batch_specs(rank=rank)
     log("rank %d: generated %d systems in %.1fs" % (rank, len(specs), time.perf_counter() - t0))
     tuned = None
-    if args.policy:
+    if args.policy and not args.autotune:
         lpb, bpg, maxb = args.policy.split(",")
         ctx.set_shape_policy(int(lpb), float(bpg), int(maxb))
         tuned = {"policy": (int(lpb), float(bpg), int(maxb))}
-    elif not args.no_autotune:
+    elif args.autotune:
         import sopb_autotune
         t0 = time.perf_counter()
         tuned = sopb_autotune.autotune(ctx, specs, steps=100, log=log if rank == 0 else None)
@@ -665,14 +665,18 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the shape policy by short timed runs instead of --policy")
     ap.add_argument("--workload", default="batch512", choices=["batch512", "serve", "capsid", "hi"])
     ap.add_argument("--hi-beads", type=int, default=4000)
     ap.add_argument("--serve-jobs", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-quantum", type=int, default=1000)
     ap.add_argument("--serve-step-scale", type=float, default=0.1)
-    ap.add_argument("--policy", default="", help="lanes_per_bead,beads_per_group,max_block (skips the autotuner)")
+    # 4 lanes per bead, one bead per lane group, CTAs of up to 1024 threads:
+    # the fastest policy on this workload in full-length runs (the autotuner's
+    # 100-step trials cannot separate it from its neighbours reliably)
+    ap.add_argument("--policy", default="4,1,1024", help="lanes_per_bead,beads_per_group,max_block")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -234,9 +234,10 @@ int sopb_context_create(int32_t device, void* stream, sopb_context** out);
 int sopb_context_destroy(sopb_context* ctx);
 /* Shape policy of the resident kernel for jobs created from now on: lanes
  * cooperating on one bead's force sum (a power of two up to 32, default
- * 32), and beads per lane group (default 8; the CTA holds about
- * n / beads_per_group groups, between 64 threads and max_block; <= 0 means
- * one bead per group).  The autotuner's knob; a job keeps the shape it was
+ * 4), and beads per lane group (default 1; the CTA holds about
+ * n / beads_per_group groups, between 64 threads and max_block (default
+ * 1024); <= 0 means one bead per group).  The defaults are the fastest
+ * shape measured on a batch of 60-600-bead systems.  The autotuner's knob; a job keeps the shape it was
  * created with, so its result is the same alone and in any mix.  No
  * reference counterpart (the reference runs one thread per bead,
  * src/gsop.cuh:13). */

@@ -69,8 +69,8 @@ constexpr float kNearSkin = 4.0f;
 
 // Shape policy of the resident kernel (see launch_shape).
 struct ShapePolicy {
-    int32_t lpb = 32;
-    float beads_per_group = 8.0f;
+    int32_t lpb = 4;
+    float beads_per_group = 1.0f;
     int32_t max_block = 1024;
 };
 

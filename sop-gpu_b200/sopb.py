@@ -335,7 +335,7 @@ class Context:
     def sync(self) -> None:
         check(lib().sopb_context_sync(self.handle), "sync")
 
-    def set_shape_policy(self, lanes_per_bead: int = 32, beads_per_group: float = 8.0, max_block: int = 1024) -> None:
+    def set_shape_policy(self, lanes_per_bead: int = 4, beads_per_group: float = 1.0, max_block: int = 1024) -> None:
         """Resident-kernel shape for jobs created from now on (autotuner knob)."""
         check(lib().sopb_context_set_shape_policy(self.handle, int(lanes_per_bead), float(beads_per_group),
                                                   int(max_block)), "set_shape_policy")

@@ -74,6 +74,27 @@ struct ShapePolicy {
     int32_t max_block = 1024;
 };
 
+struct LaunchClass {
+    int block = 0;
+    int32_t max_n = 0;
+    size_t smem = 0;
+    std::vector<int32_t> ids;
+};
+
+// The last resident launch plan ordered on each stream of a context: its
+// jobs and step counts, classes and the id/step table it uploaded.  A run
+// of the same jobs with the same counts on the same stream, with no job
+// created or destroyed since, reuses the plan and the device table (no
+// other run writes that stream's table in between) instead of grouping and
+// uploading again.
+struct RunPlan {
+    uint64_t generation = 0;
+    std::vector<sopb_job*> jobs;
+    std::vector<int64_t> steps;
+    std::vector<LaunchClass> cls;
+    std::vector<size_t> off;
+};
+
 }  // namespace
 
 struct sopb_context {
@@ -81,6 +102,8 @@ struct sopb_context {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 0;
+    uint64_t generation = 0;      // bumped by every job creation and destruction
+    std::map<cudaStream_t, RunPlan> plans;   // the last resident launch plan per stream
     int64_t bead_cap = 0;
     float4* x = nullptr;
     float4* xalt = nullptr;
@@ -1218,6 +1241,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
             return rc2;
         }
     }
+    c->generation++;
     const int slot = c->free_slots.back();
     c->free_slots.pop_back();
     CUDA_TRY(cudaMemcpyAsync(&c->d_jobs[slot], &h, sizeof(JobDev), cudaMemcpyHostToDevice, st));
@@ -1255,6 +1279,7 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     CUDA_TRY(cudaFreeAsync(j->dmem, c->io));
     CUDA_TRY(cudaEventRecord(j->ev, c->io));
     c->slots[j->slot] = nullptr;
+    c->generation++;
     c->deferred.push_back({j->ev, j->b0, j->n, j->slot});
     delete j;
     return SOPB_OK;
@@ -1263,12 +1288,7 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
 namespace {
 // Groups jobs by CTA size class; returns (block, ids) per class, largest
 // jobs' class first so the longest CTAs start first.
-struct LaunchClass {
-    int block = 0;
-    int32_t max_n = 0;
-    size_t smem = 0;
-    std::vector<int32_t> ids;
-};
+
 // CTAs of a job's resident launch that fit one SM: 1024 threads' worth of
 // registers (the kernel's launch bound) and the SM's shared memory.
 int ctas_per_sm(const sopb_context* c, int block, size_t smem) {
@@ -1341,38 +1361,55 @@ extern "C" int sopb_run_on(sopb_context* c, sopb_job* const* jobs, int32_t njobs
 namespace {
 int run_ordered(sopb_context* c, sopb_job* const* jobs, int32_t njobs, const int64_t* nsteps, cudaStream_t st) {
     std::vector<sopb_job*> resident, grid;
-    std::vector<int64_t> gsteps;
-    std::map<const sopb_job*, int64_t> steps_of;
+    std::vector<int64_t> rsteps, gsteps;
     for (int32_t k = 0; k < njobs; ++k) {
         if (jobs[k]->h.grid) {
             grid.push_back(jobs[k]);
             gsteps.push_back(nsteps[k]);
         } else {
             resident.push_back(jobs[k]);
-            steps_of[jobs[k]] = nsteps[k];
+            rsteps.push_back(nsteps[k]);
         }
     }
     // resident jobs: one launch per class; the class table goes up first
-    std::vector<LaunchClass> cls;
-    std::vector<size_t> off;
     int32_t* d_ids = nullptr;
     int64_t* d_steps = nullptr;
     int rc;
+    RunPlan& plan = c->plans[st];
+    const std::vector<LaunchClass>& cls = plan.cls;
+    const std::vector<size_t>& off = plan.off;
     if (!resident.empty()) {
-        group_jobs(c, resident.data(), (int32_t)resident.size(), cls);
-        std::vector<int32_t> ids;
-        std::vector<int64_t> steps;
-        for (auto& L : cls) {
-            off.push_back(ids.size());
-            ids.insert(ids.end(), L.ids.begin(), L.ids.end());
-            for (int32_t slot : L.ids) steps.push_back(steps_of[c->slots[slot]]);
+        const bool same = plan.generation == c->generation && plan.jobs == resident && plan.steps == rsteps;
+        if (!same) {
+            plan.generation = c->generation;
+            plan.jobs = resident;
+            plan.steps = rsteps;
+            plan.cls.clear();
+            plan.off.clear();
+            group_jobs(c, resident.data(), (int32_t)resident.size(), plan.cls);
         }
-        if ((rc = ensure_ids(c, st, (int64_t)ids.size(), &d_ids, &d_steps))) return rc;
-        // (a copy from pageable memory is staged before the call returns)
-        CUDA_TRY(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
-        CUDA_TRY(cudaMemcpyAsync(d_steps, steps.data(), steps.size() * 8, cudaMemcpyHostToDevice, st));
+        std::vector<int64_t> slot_steps(c->slots.size(), 0);
+        for (size_t k = 0; k < resident.size(); ++k) slot_steps[resident[k]->slot] = rsteps[k];
+        int64_t total = 0;
+        for (auto& L : cls) total += (int64_t)L.ids.size();
+        if ((rc = ensure_ids(c, st, total, &d_ids, &d_steps))) return rc;
+        if (!same) {
+            std::vector<int32_t> ids;
+            std::vector<int64_t> steps;
+            for (auto& L : cls) {
+                plan.off.push_back(ids.size());
+                ids.insert(ids.end(), L.ids.begin(), L.ids.end());
+                for (int32_t slot : L.ids) steps.push_back(slot_steps[slot]);
+            }
+            // (a copy from pageable memory is staged before the call returns)
+            CUDA_TRY(cudaMemcpyAsync(d_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(d_steps, steps.data(), steps.size() * 8, cudaMemcpyHostToDevice, st));
+        }
         if (grid.empty() && cls.size() == 1)
             return launch_resident(cls[0].block, (int)cls[0].ids.size(), cls[0].smem, st, c->d_jobs, d_ids, d_steps);
+    } else {
+        plan.jobs.clear();          // the table on this stream is no longer the plan's
+        plan.generation = ~uint64_t(0);
     }
     // one grid job alone: straight on the stream
     if (resident.empty() && grid.size() == 1) return grid_run(grid[0], st, gsteps[0]);
@@ -1464,6 +1501,7 @@ extern "C" int sopb_job_read(sopb_job* j, int32_t what, void* out) {
         }
         int32_t* d_ids = nullptr;
         int rc = ensure_ids(c, c->io, 1, &d_ids);
+        c->plans.erase(c->io);   // the io stream's table no longer holds a run plan
         if (rc) return rc;
         const int32_t id = j->slot;
         CUDA_TRY(cudaMemcpyAsync(d_ids, &id, 4, cudaMemcpyHostToDevice, c->io));
@@ -1630,6 +1668,7 @@ extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t ver
     }
     int32_t* d_ids = nullptr;
     int rc = ensure_ids(c, c->io, 1, &d_ids);
+    c->plans.erase(c->io);   // the io stream's table no longer holds a run plan
     if (rc) return rc;
     const int32_t id = j->slot;
     CUDA_TRY(cudaMemcpyAsync(d_ids, &id, 4, cudaMemcpyHostToDevice, c->io));

@@ -777,7 +777,8 @@ int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, bool ref
     }
     const int fb = (int)std::min<int64_t>((j->n + (kGridBlock / kGridLpb) - 1) / (kGridBlock / kGridLpb), (int64_t)c->sm_count * 8);
     for (int s = 0; s < steps; ++s) {
-        k_g_forces<<<fb, kGridBlock, 0, st>>>(Jp, a);
+        if (j->h.discrete || j->h.plane) k_g_forces<true><<<fb, kGridBlock, 0, st>>>(Jp, a);
+        else k_g_forces<false><<<fb, kGridBlock, 0, st>>>(Jp, a);
         if (!j->h.hi) {
             k_g_langevin<<<nb, kGridBlock, 0, st>>>(Jp, a);
         } else if (!j->h.hi_exact) {

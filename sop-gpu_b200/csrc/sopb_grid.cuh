@@ -54,6 +54,9 @@ __device__ __forceinline__ int64_t job_step(const JobDev* Jp) { return *(volatil
 // ---- potentials ------------------------------------------------------------
 // All potentials of every bead at the current coordinates into aux.F; the
 // tip's share accumulates per bead (indentation_kernel.cu:71-128).
+// EXT: the job has a discrete surface or a pulling plane (a separate
+// instantiation, so the common one keeps its register budget).
+template <bool EXT>
 __global__ void __launch_bounds__(kGridBlock)
 k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
     __shared__ JobDev Js;
@@ -77,19 +80,19 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
         if (act) {
             bonded_partial(J, global_bonded(J), J.x, i, xi, l, lpb, f);
             pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
-            if (J.discrete) mica_partial(J, i, xi, l, lpb, f);
+            if (EXT && J.discrete) mica_partial(J, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);
         if (act && l == 0) {
             if (J.indent) {
                 float3 tf;
-                if (J.discrete) tip_term(xi, ig, f, tf);
+                if (EXT && J.discrete) tip_term(xi, ig, f, tf);
                 else indentation_term(xi, ig, f, tf);
                 float4 t = J.tipF[i];
                 t.x += tf.x; t.y += tf.y; t.z += tf.z;
                 J.tipF[i] = t;
             }
-            if (J.plane) {
+            if (EXT && J.plane) {
                 const int mask = J.plane_mask[i];
                 if (mask) J.plane_f[i] = plane_term(J, J.plane_displ, mask, xi, J.plane_r0[i], f);
             }

@@ -5,10 +5,16 @@
 //
 //   ref_gpu <config.sop> <outdir> <total_steps> <dump steps...>
 //
+// With no dump steps it only times the loop: the wall time from the first
+// updater pass to the device's completion of the last step (set-up, input
+// reading and the step-0 possible-pairs scan excluded), printed as
+// "ref_gpu_time <seconds> <bead-steps/s>".
+//
 // The loop is runGPU's (src/gsop.cu:111-148): updaters every `stride` steps,
 // then every potential's compute() and the integrator.  At a dump step s the
 // files <outdir>/<what>_<s>.bin hold the state after s steps; forces_0.bin
 // holds the potential forces of step 0 (after the step-0 updaters).
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -71,11 +77,14 @@ int main(int argc, char** argv) {
     FILE* meta = std::fopen((dir + "/meta.txt").c_str(), "w");
     std::fprintf(meta, "aminoCount %zu\nNtr %d\nstride %d\nmax_pairs %d\n", N, gsop.Ntr, stride, hc_pairs.max_pairs);
     std::fclose(meta);
+    const bool timing = dumps.empty();
+    cudaDeviceSynchronize();
+    const auto t0 = std::chrono::steady_clock::now();
     for (long done = 0; done < total;) {
         for (int u = 0; u < updatersCount; u++) updaters[u]->update();
         for (int j = 0; j < stride && done < total; j++) {
             for (int p = 0; p < potentialsCount; p++) potentials[p]->compute();
-            if (done == 0) dump(dir, "forces", 0, gsop.d_forces, N * sizeof(float4));
+            if (done == 0 && !timing) dump(dir, "forces", 0, gsop.d_forces, N * sizeof(float4));
             integrator->integrate();
             checkCUDAError();
             done++;
@@ -93,6 +102,8 @@ int main(int argc, char** argv) {
     }
     cudaDeviceSynchronize();
     checkCUDAError();
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::printf("ref_gpu: %ld steps, %zu beads, stride %d\n", total, N, stride);
+    if (timing) std::printf("ref_gpu_time %.6f %.6e\n", secs, (double)N * total / secs);
     return 0;
 }

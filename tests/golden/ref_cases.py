@@ -99,6 +99,20 @@ CASES = {
         "indentationSurfaceStep": "3.0", "indentationPairsCutoff": "12.0", "indentationMoveSurface": "yes",
         "indentationCantLength": "50.0", "indentationSurfConnectFile": "<name>_mica.vmd", "outputtiming": "20",
         "dcdfreq": "40"}),
+    # speed comparisons with the reference's CUDA path (timed, no dumps):
+    # the plain 200-bead ramp pull, 512 force-clamp replicas of one 200-bead
+    # system, TEA at 4000 beads
+    "speed_plain": dict(n=200, sys_seed=2024, runs=1, total=20000, dumps=[], speed=True, cfg={
+        "run": "1", "seed": "1119726", "nav": "1000", "max_pairs": "256", "max_possiblePairs": "256",
+        "pulling": "on", "deltax": "0.5", "k_trans": "0.05", "pullFreq": "1000", "fixed": "0", "pulled": "199",
+        "fixedEnd": "0", "pulledEnd": "199", "pullDirection": "endToEnd"}),
+    "speed_batch": dict(n=200, sys_seed=2024, runs=512, total=2000, dumps=[], speed=True, cfg={
+        "runnum": "512", "firstrun": "1", "seed": "1119726", "nav": "1000", "max_pairs": "256",
+        "max_possiblePairs": "256", "pulling": "on", "fconst": "2.0", "fixed": "0", "pulled": "199",
+        "fixedEnd": "0", "pulledEnd": "199", "pullDirection": "endToEnd"}),
+    "speed_tea": dict(n=4000, sys_seed=4000, runs=1, total=20, dumps=[], speed=True, cfg={
+        "run": "1", "seed": "777", "nav": "1000", "max_pairs": "1024", "max_possiblePairs": "4096",
+        "hi_on": "yes", "hi_a": "3.8", "hi_unlisted": "yes", "hi_capricious": "no", "hi_epsilon_freq": "10"}),
     "heat": dict(n=100, sys_seed=6, runs=1, total=45, dumps=[45], cfg={
         "run": "1", "seed": "5", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
         "heating": "on", "initialT": "0.1", "deltaT": "0.2", "tempFreq": "10"}),

@@ -2,6 +2,7 @@
 (tests/golden/make_ref_gpu_golden.py) and checked by
 tests/test_ref_gpu_golden.py.  Each case is a config file in the reference's
 format plus seeded synthetic inputs; both sides read the same files."""
+import functools
 import os
 import sys
 
@@ -113,6 +114,14 @@ CASES = {
     "speed_tea": dict(n=4000, sys_seed=4000, runs=1, total=20, dumps=[], speed=True, cfg={
         "run": "1", "seed": "777", "nav": "1000", "max_pairs": "1024", "max_possiblePairs": "4096",
         "hi_on": "yes", "hi_a": "3.8", "hi_unlisted": "yes", "hi_capricious": "no", "hi_epsilon_freq": "10"}),
+    # the 198 000-bead shell indented by a 10 nm tip, 200 steps
+    "speed_capsid": dict(n=198000, sys_seed=7, runs=1, total=200, dumps=[], speed=True, system="capsid", cfg={
+        "run": "1", "seed": "5032015", "nav": "100", "pairs_threshold": "40.0", "max_possiblePairs": "2048",
+        "max_pairs": "512", "possiblepairs_freq": "100000", "indentation": "on", "indentationTipR": "100.0",
+        "indentationKs": "0.07", "indentationDeltaX": "0.012", "indentationDirection": "0.0 -1.0 0.0",
+        "indentationSurfaceN": "0.0 1.0 0.0", "indentationTipZeta": "5000", "indentationSurfA": "1.0",
+        "indentationSurfB": "-2.0", "indentationSurfSigma": "10.0", "indentationSurfEl": "0.2",
+        "indentationFixTrans": "yes"}),
     "heat": dict(n=100, sys_seed=6, runs=1, total=45, dumps=[45], cfg={
         "run": "1", "seed": "5", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
         "heating": "on", "initialT": "0.1", "deltaT": "0.2", "tempFreq": "10"}),
@@ -122,9 +131,16 @@ CASES = {
 }
 
 
+@functools.lru_cache(maxsize=4)
+def _capsid():
+    return S.make_capsid()[0]
+
+
 def systems(name):
     """The case's systems, one per run (run k > 0 is a perturbed copy)."""
     c = CASES[name]
+    if c.get("system") == "capsid":
+        return [_capsid()]
     base = S.make_system(c["n"], c["sys_seed"])
     out = [base]
     rng = np.random.default_rng(c["sys_seed"])
@@ -139,7 +155,16 @@ def config_text(name):
     cfg = dict(COMMON)
     cfg.update(c["cfg"])
     cfg["name"] = name
-    if c["cfg"].get("indentation") == "on":
+    if c.get("system") == "capsid":
+        # a 10 nm tip over the shell, the substrate under it (the capsid
+        # workload's geometry)
+        x = systems(name)[0].xyz.astype(np.float64)
+        m = x.mean(axis=0)
+        tip = "%.4f %.4f %.4f" % (m[0], x[:, 1].max() + 104.0, m[2])
+        cfg["indentationChip"] = tip
+        cfg["indentationTip"] = tip
+        cfg["indentationSurfaceR0"] = "0.0 %.4f 0.0" % (x[:, 1].min() - 10.0)
+    elif c["cfg"].get("indentation") == "on":
         x = systems(name)[0].xyz.astype(np.float64)
         top = x[:, 1].min()
         tip = "%.4f %.4f %.4f" % (x[:, 0].mean(), top - 22.0, x[:, 2].mean())

@@ -148,7 +148,14 @@ typedef struct sopb_params {
     float pullingPlanePos[3];        /* a point of both planes at step 0       */
     int32_t pullingPlaneUpdateFreq;  /* defaults to nav                        */
     int32_t pullingPlaneOutputFreq;  /* defaults to nav                        */
-    int32_t reserved2[4];
+    /* key added by this library */
+    float verlet_skin;               /* near list kept between Verlet         */
+                                     /* rebuilds: the possible pairs within   */
+                                     /* pairlist_cutoff + skin, re-filtered   */
+                                     /* until a bead moved skin/2; the Verlet */
+                                     /* rows are those of a full filter.      */
+                                     /* A; 0 = 4, < 0 = no near list          */
+    int32_t reserved2[3];
 } sopb_params;
 
 /*

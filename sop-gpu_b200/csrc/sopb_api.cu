@@ -63,9 +63,17 @@ struct RangeAlloc {
 
 inline size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
-// Skin of the resident jobs' near list (A): the Verlet rebuild filters the
-// possible pairs within pairlist_cutoff + skin instead of scanning them all.
+// Default skin of the near list (A): a Verlet rebuild filters the possible
+// pairs within pairlist_cutoff + skin instead of all of them.
 constexpr float kNearSkin = 4.0f;
+
+inline float near_skin(const sopb_params& p) { return p.verlet_skin == 0.0f ? kNearSkin : p.verlet_skin; }
+
+// Near-row capacity of a grid job (int32 rows): twice the Verlet rows, at
+// most the possible rows.  0: no near list.
+inline int64_t grid_cap_nr(const sopb_params& p, int64_t cap_pp, int64_t cap_pl) {
+    return near_skin(p) > 0.02f ? std::max<int64_t>(1, std::min<int64_t>(cap_pp, 2 * cap_pl)) : 0;
+}
 
 // Shape policy of the resident kernel (see launch_shape).
 struct ShapePolicy {
@@ -167,8 +175,9 @@ struct sopb_job {
     GridAux aux{};
     void* amem = nullptr;
     int64_t host_step = 0;             // the device step counter, tracked on the host
-    cudaGraphExec_t chunk = nullptr;   // one stride chunk: updaters + stride steps
-    cudaGraphExec_t chunk_r = nullptr; // the same with the Cholesky refresh at its first step
+    // one stride chunk (updaters + stride steps) per set of updaters due at
+    // its first step (kDue* bits)
+    std::map<int, cudaGraphExec_t> chunks;
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
     cudaStream_t la = nullptr;         // exact HI: the factorisation's second stream
     cudaEvent_t la_fork = nullptr, la_join = nullptr;
@@ -460,8 +469,7 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     reclaim(c, true);
     for (sopb_job* j : c->slots)
         if (j) {
-            if (j->chunk) cudaGraphExecDestroy(j->chunk);
-            if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
+            for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
             if (j->la) {
                 cudaStreamDestroy(j->la);
                 cudaEventDestroy(j->la_fork);
@@ -539,6 +547,7 @@ int validate_desc(const sopb_job_desc* d) {
     if (p.nav <= 0 || p.pairs_freq <= 0 || p.possiblepairs_freq <= 0) return SOPB_ERR_INVALID;
     if (p.heating && p.tempFreq <= 0) return SOPB_ERR_INVALID;
     if (p.log_rows < 0 || p.log_rows > (1 << 24) || (p.log_rows & (p.log_rows - 1))) return SOPB_ERR_INVALID;
+    if (!std::isfinite(p.verlet_skin) || p.verlet_skin > 1000.0f) return SOPB_ERR_INVALID;
     if (d->nbonds < 0 || d->nnatives < 0 || d->nfixed < 0 || d->npulled < 0) return SOPB_ERR_INVALID;
     if ((d->nbonds && (!d->bonds || !d->bonds_r0)) || (d->nnatives && (!d->natives || !d->natives_r0 || !d->natives_eh)))
         return SOPB_ERR_INVALID;
@@ -624,7 +633,7 @@ namespace {
 
 // Buffers of the grid path: force buffer (the context's second coordinate
 // pool), reduction partials and, for large jobs, the cell list.
-int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
+int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, int32_t cap_pp, int32_t cap_pl) {
     GridAux& a = j->aux;
     j->bead_blocks = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)c->sm_count * 8);
     a.npart = j->bead_blocks;
@@ -658,6 +667,15 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
         o_cb = off; off += align256((size_t)n * 4);
         o_bc = off; off += align256((size_t)n * 4);
     }
+    // near list of the Verlet rebuilds
+    a.cap_nr = (int32_t)grid_cap_nr(p, cap_pp, cap_pl);
+    size_t o_nrj = 0, o_nrc = 0, o_xref = 0;
+    const size_t o_near = off; off += align256(4 * sizeof(int32_t));
+    if (a.cap_nr) {
+        o_nrj = off; off += align256((size_t)n * a.cap_nr * 4);
+        o_nrc = off; off += align256((size_t)n * 4);
+        o_xref = off; off += align256((size_t)n * 16);
+    }
     if (cudaMallocAsync(&j->amem, off, c->upload) != cudaSuccess) {
         cudaGetLastError();
         return SOPB_ERR_NOMEM;
@@ -679,6 +697,12 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n) {
         }
     }
     a.cell_geo = (float*)(b + o_geo);
+    a.near = (int32_t*)(b + o_near);
+    if (a.cap_nr) {
+        a.nr_j = (int32_t*)(b + o_nrj);
+        a.nr_cnt = (int32_t*)(b + o_nrc);
+        a.x_ref = (float4*)(b + o_xref);
+    }
     if (a.use_cells) {
         a.cell_count = (int32_t*)(b + o_cc);
         a.cell_start = (int32_t*)(b + o_cs);
@@ -748,11 +772,29 @@ int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     return SOPB_OK;
 }
 
-int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, bool refresh_first = false) {
+// Updaters due at a stride boundary, from the host's copy of the step.  The
+// kernels of an updater that is not due return at once (each gates on the
+// device step itself); a launch sequence leaves them out.
+enum : int { kDuePossible = 1, kDueVerlet = 2, kDueTReset = 4, kDueTeaEps = 8, kDueRefresh = 16 };
+
+int due_at(const sopb_job* j, int64_t step) {
+    const JobDev& h = j->h;
+    int d = 0;
+    if (step % h.pp_freq == 0) d |= kDuePossible;
+    if (step % h.pairs_freq == 0) d |= kDueVerlet;
+    if (step % h.nav == 0) d |= kDueTReset;
+    if (step % h.eps_freq == 0) d |= kDueTeaEps;
+    if (h.hi && h.hi_exact && h.hi_refresh > 1 && step % h.hi_refresh == 0) d |= kDueRefresh;
+    return d;
+}
+
+// Updaters (at a stride boundary, those of `due`) and `steps` Langevin steps.
+int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, int due = 0) {
     sopb_context* c = j->ctx;
     JobDev* Jp = &c->d_jobs[j->slot];
     GridAux& a = j->aux;
     const int nb = j->bead_blocks;
+    const bool refresh_first = (due & kDueRefresh) != 0;
     if (updaters) {
         k_g_tip_partial<<<nb, kGridBlock, 0, st>>>(Jp, a);
         k_g_scalar_updaters<<<1, 32, 0, st>>>(Jp, a);
@@ -762,12 +804,18 @@ int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, bool ref
             const int mb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
             k_g_mica<<<mb, kGridBlock, 0, st>>>(Jp);
         }
-        k_g_treset<<<nb, kGridBlock, 0, st>>>(Jp);
-        int rc = grid_possible(j, Jp, st, 0);
-        if (rc) return rc;
-        const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
-        k_g_verlet<<<wb, kGridBlock, 0, st>>>(Jp, 0);
-        if (j->h.hi && !j->h.hi_exact) {
+        if (due & kDueTReset) k_g_treset<<<nb, kGridBlock, 0, st>>>(Jp);
+        if (due & kDuePossible) {
+            int rc = grid_possible(j, Jp, st, 0);
+            if (rc) return rc;
+        }
+        if (due & kDueVerlet) {
+            const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
+            if (a.cap_nr) k_g_drift<<<nb, kGridBlock, 0, st>>>(Jp, a);
+            k_g_verlet<<<wb, kGridBlock, 0, st>>>(Jp, a, 0);
+        }
+        if (a.cap_nr && (due & (kDuePossible | kDueVerlet))) k_g_near_commit<<<1, 32, 0, st>>>(Jp, a, -1, -1);
+        if (j->h.hi && !j->h.hi_exact && (due & kDueTeaEps)) {
             // TeaUpdater (src/Integrators/bdhitea.cu:133-176), last updater
             const dim3 tg((j->n + kHiTile - 1) / kHiTile, j->jsplit);
             k_tea_eps_partial<<<tg, kHiTile, 0, st>>>(Jp, a, j->jsplit, 0);
@@ -823,18 +871,15 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
         j->host_step++;
         left--;
     }
-    // Cholesky refresh at an updater boundary (hi_refresh > 1)
-    const int32_t refresh = j->h.hi && j->h.hi_exact ? j->h.hi_refresh : 0;
-    auto refresh_due = [&](int64_t step) { return refresh > 1 && step % refresh == 0; };
     const int64_t chunks = left / stride;
     for (int64_t k = 0; k < chunks; ++k) {
-        const bool r = refresh_due(j->host_step);
-        cudaGraphExec_t& ge = r ? j->chunk_r : j->chunk;
+        const int due = due_at(j, j->host_step);
+        cudaGraphExec_t& ge = j->chunks[due];
         if (!ge) {
             cudaGraph_t g;
             cudaStream_t cap = j->ctx->capture;
             CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-            rc = grid_launch(j, cap, true, stride, r);
+            rc = grid_launch(j, cap, true, stride, due);
             cudaError_t e = cudaStreamEndCapture(cap, &g);
             if (rc) return rc;
             CUDA_TRY(e);
@@ -847,7 +892,7 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
     }
     while (left > 0) {
         const bool boundary = j->host_step % stride == 0;
-        if ((rc = grid_launch(j, st, boundary, 1, boundary && refresh_due(j->host_step)))) return rc;
+        if ((rc = grid_launch(j, st, boundary, 1, boundary ? due_at(j, j->host_step) : 0))) return rc;
         j->host_step++;
         left--;
     }
@@ -870,7 +915,9 @@ extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
     b += align256(n * 4) * 2;                       // counts
     b += align256(n * cap_pp * 4) + align256(n * cap_pl * 4);
     b += n * (16 + 16 + 16 + 4 + 16 + 1);           // bead pools
-    b += align256(n * std::min<int64_t>(n - 1, 2 * cap_pl) * 2) + align256(n * 4) + align256(n * 16);   // near list
+    // near list: u16 rows of a resident job, int32 rows of a grid job
+    b += std::max(align256(n * std::min<int64_t>(n - 1, 2 * cap_pl) * 2),
+                  align256(n * grid_cap_nr(d->params, cap_pp, cap_pl) * 4)) + align256(n * 4) + align256(n * 16);
     const sopb_params& p = d->params;
     if ((p.pulling && p.deltax != 0.0f) || p.indentation || p.pullingPlane)
         b += align256((size_t)(p.log_rows > 0 ? p.log_rows : 1024) * 64);                        // event log
@@ -926,10 +973,11 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     h.pl_t = sqrt_threshold(p.pairlist_cutoff);
     h.pp_t = sqrt_threshold(p.pairs_threshold);
     // near list skin: valid while no bead moved more than half of it (less
-    // a margin far above the rounding of the distances)
-    h.nr_t = sqrt_threshold(p.pairlist_cutoff + kNearSkin);
+    // a margin far above the rounding of the distances); drift2 0 = no near list
+    const float skin = near_skin(p);
+    h.nr_t = sqrt_threshold(p.pairlist_cutoff + std::max(skin, 0.0f));
     h.rlb = p.R_limit_bond > 0.0f ? p.R_limit_bond : 8.0f;
-    h.drift2 = (0.5f * kNearSkin - 0.01f) * (0.5f * kNearSkin - 0.01f);
+    h.drift2 = skin > 0.02f ? (0.5f * skin - 0.01f) * (0.5f * skin - 0.01f) : 0.0f;
     h.h = p.timestep;
     h.zeta = p.zeta;
     h.hOverZeta = p.timestep / p.zeta;
@@ -1234,7 +1282,7 @@ extern "C" int sopb_job_create(sopb_context* c, const sopb_job_desc* d, sopb_job
     j->b0 = b0;   // the grid buffers are views of the job's bead range
     j->n = n;
     if (h.grid) {
-        int rc2 = grid_alloc(c, j, p, n);
+        int rc2 = grid_alloc(c, j, p, n, h.cap_pp, h.cap_pl);
         if (rc2) {
             cudaFreeAsync(j->dmem, c->upload);
             c->beads.release(b0, n);
@@ -1267,8 +1315,7 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     CUDA_TRY(cudaSetDevice(c->device));
     // nothing waits here: graphs and memory are released after the job's
     // last work on its stream, the bead range and slot once it has finished
-    if (j->chunk) cudaGraphExecDestroy(j->chunk);
-    if (j->chunk_r) cudaGraphExecDestroy(j->chunk_r);
+    for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
     if (j->la) {   // released by the runtime once its work is done
         cudaStreamDestroy(j->la);
         cudaEventDestroy(j->la_fork);
@@ -1661,9 +1708,11 @@ extern "C" int sopb_job_rebuild_lists(sopb_job* j, int32_t possible, int32_t ver
         if (rc) return rc;
         if (verlet) {
             const int wb = (int)std::min<int64_t>((j->n + 7) / 8, (int64_t)c->sm_count * 16);
-            k_g_verlet<<<wb, kGridBlock, 0, c->io>>>(Jp, 1);
-            CUDA_TRY(cudaGetLastError());
+            k_g_verlet<<<wb, kGridBlock, 0, c->io>>>(Jp, j->aux, 1);
         }
+        if (j->aux.cap_nr && (possible || verlet))
+            k_g_near_commit<<<1, 32, 0, c->io>>>(Jp, j->aux, possible ? 1 : 0, verlet ? 1 : 0);
+        CUDA_TRY(cudaGetLastError());
         SOPB_TRY(io_end(j, true));
         return SOPB_OK;
     }

@@ -47,6 +47,13 @@ struct GridAux {
     int32_t* bead_cell;  // [n]
     float* cell_geo;     // origin[3], size, dims[3] (as float), ncell
     int32_t use_cells;
+    // near list of the Verlet rebuilds (null: none, every rebuild filters
+    // the possible rows)
+    int32_t* nr_j;       // [n * cap_nr] possible pairs within pairlist_cutoff + skin
+    int32_t* nr_cnt;     // [n]
+    float4* x_ref;       // coordinates it was built at
+    int32_t* near;       // [3] drift bits, overflow, usable
+    int32_t cap_nr;
 };
 
 __device__ __forceinline__ int64_t job_step(const JobDev* Jp) { return *(volatile const int64_t*)&Jp->step; }
@@ -517,42 +524,116 @@ k_cl_sort_rows(JobDev* __restrict__ Jp, int force) {
     }
 }
 
-// Verlet rows from the possible rows (pairlist_kernel.cu:33-76), order kept.
+// Near list of the Verlet rebuilds (a grid job with a skin): the possible
+// pairs within pairlist_cutoff + skin, in the order of the possible rows,
+// with the coordinates it was built at.  While no bead has moved more than
+// half the skin since, every possible pair now closer than pairlist_cutoff
+// was closer than pairlist_cutoff + skin then, so filtering the near rows with
+// the same exact test gives the rows a filter of the possible rows gives.
+// aux.near: [0] largest squared drift (float bits), [1] a near row overflowed
+// its capacity, [2] the near list is usable.  [0] and [1] are cleared by
+// k_g_near_commit, the last kernel of every rebuild.
+__device__ __forceinline__ bool verlet_from_near(const JobDev& J, const GridAux& a, int64_t step, int force) {
+    return !force && a.nr_j && a.near[2] && step % J.pp_freq != 0 && __int_as_float(a.near[0]) < J.drift2;
+}
+
+// Largest squared displacement since the near list was built, at a Verlet
+// step that may reuse it.
 __global__ void __launch_bounds__(kGridBlock)
-k_g_verlet(JobDev* __restrict__ Jp, int force) {
+k_g_drift(JobDev* __restrict__ Jp, GridAux a) {
+    const JobDev& J = *Jp;
+    const int64_t step = job_step(Jp);
+    if (J.status || step % J.stride != 0 || step % J.pairs_freq != 0 || step % J.pp_freq == 0 || !a.near[2]) return;
+    float d2 = 0.f;
+    for (int i = blockIdx.x * kGridBlock + threadIdx.x; i < J.n; i += gridDim.x * kGridBlock)
+        d2 = fmaxf(d2, dist2_rn(a.x_ref[i], J.x[i]));
+    for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+    if ((threadIdx.x & 31) == 0 && d2 > 0.f) atomicMax(&a.near[0], __float_as_int(d2));   // non-negative floats order as ints
+}
+
+// Verlet rows (pairlist_kernel.cu:33-76), order kept: a warp per bead, lanes
+// over 32 candidates at a time, a ballot places the hits.  From the near rows
+// when they are usable and no bead drifted too far; else from the possible
+// rows, renewing the near rows at the current coordinates.
+__global__ void __launch_bounds__(kGridBlock)
+k_g_verlet(JobDev* __restrict__ Jp, GridAux a, int force) {
     __shared__ JobDev Js;
     load_job<kGridBlock>(Js, Jp);
     __syncthreads();
     const JobDev& J = Js;
     const int64_t step = J.step;
     if (J.status || (!force && (step % J.stride != 0 || step % J.pairs_freq != 0))) return;
+    const bool near = verlet_from_near(J, a, step, force);
+    const bool renew = !near && a.nr_j;
     const int l = threadIdx.x & 31;
-    int err = 0;
+    const unsigned below = (1u << l) - 1u;
+    int err = 0, over = 0;
     for (int i = blockIdx.x * (kGridBlock / 32) + threadIdx.x / 32; i < J.n; i += gridDim.x * (kGridBlock / 32)) {
         const float4 xi = J.x[i];
-        const int npp = J.pp_cnt[i];
-        const int32_t* prow = J.pp_j + (size_t)i * J.cap_pp;
+        const int src = near ? a.nr_cnt[i] : J.pp_cnt[i];
+        const int32_t* srow = near ? a.nr_j + (size_t)i * a.cap_nr : J.pp_j + (size_t)i * J.cap_pp;
         int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
-        int cnt = 0;
-        for (int kb = 0; kb < npp; kb += 32) {
+        int32_t* nrow = renew ? a.nr_j + (size_t)i * a.cap_nr : nullptr;
+        int cnt = 0, ncnt = 0;
+        for (int kb = 0; kb < src; kb += 32) {
             const int k = kb + l;
             int q = 0;
-            bool ok = k < npp;
-            if (ok) {
-                q = prow[k];
-                ok = within_cutoff(xi, J.x[q], J.pl_t);
+            float r2 = 0.f;
+            const bool cand = k < src;
+            if (cand) {
+                q = srow[k];
+                r2 = dist2_rn(xi, J.x[q]);
             }
+            const bool ok = cand && r2 < J.pl_t;
             const unsigned m = __ballot_sync(0xffffffffu, ok);
             if (ok) {
-                const int pos = cnt + __popc(m & ((1u << l) - 1u));
+                const int pos = cnt + __popc(m & below);
                 if (pos < J.cap_pl) row[pos] = q;
                 else err = SOPB_STATUS_CAPACITY;
             }
             cnt += __popc(m);
+            if (renew) {
+                const bool nok = cand && r2 < J.nr_t;
+                const unsigned nm = __ballot_sync(0xffffffffu, nok);
+                if (nok) {
+                    const int pos = ncnt + __popc(nm & below);
+                    if (pos < a.cap_nr) nrow[pos] = q;
+                    else over = 1;
+                }
+                ncnt += __popc(nm);
+            }
         }
-        if (l == 0) J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
+        if (l == 0) {
+            J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
+            if (renew) {
+                a.nr_cnt[i] = ncnt < a.cap_nr ? ncnt : a.cap_nr;
+                a.x_ref[i] = xi;
+            }
+        }
     }
     if (err) atomicMax(&Jp->status, err);
+    if (over) atomicOr(&a.near[1], 1);
+}
+
+// Closes a rebuild: the near list is usable after a rebuild that renewed it
+// without overflow, unusable after new possible pairs without a Verlet
+// rebuild, unchanged otherwise.  possible/verlet: an explicit rebuild (-1 in
+// a run, where the step decides).
+__global__ void k_g_near_commit(JobDev* __restrict__ Jp, GridAux a, int possible, int verlet) {
+    if (threadIdx.x != 0 || blockIdx.x != 0 || !a.nr_j) return;
+    const JobDev& J = *Jp;
+    const int64_t step = job_step(Jp);
+    const bool force = verlet >= 0;
+    if (!force) {
+        const bool at = step % J.stride == 0;
+        possible = at && step % J.pp_freq == 0;
+        verlet = at && step % J.pairs_freq == 0;
+    }
+    if (J.status) a.near[2] = 0;
+    else if (verlet && !verlet_from_near(J, a, step, force ? 1 : 0)) a.near[2] = a.near[1] ? 0 : 1;
+    else if (possible && !verlet) a.near[2] = 0;
+    a.near[0] = 0;
+    a.near[1] = 0;
 }
 
 // Advances the job's step counter by `by` (last launch of a chunk) and flags

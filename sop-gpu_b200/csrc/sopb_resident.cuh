@@ -297,7 +297,7 @@ __device__ void rebuild_verlet(const JobDev& J, const float4* __restrict__ xs, i
     build_verlet<BLOCK>(J, xs, err, &near_over);
     for (int i = tid; i < n; i += BLOCK) J.x_ref[i] = xs[i];
     __syncthreads();
-    valid = near_over ? 0 : 1;
+    valid = near_over || !(J.drift2 > 0.f) ? 0 : 1;   // drift2 0: the job keeps no near list
 }
 
 // Deterministic CTA sum of a float3 (fixed tree for a given BLOCK).
@@ -532,6 +532,7 @@ __device__ __noinline__ int run_updaters(const JobDev& J, StepScalars& sc, const
     if (step % J.nav == 0)
         for (int i = tid; i < n; i += BLOCK) Ts[i] = 0.0f;   // output_manager.cu:125-127
     const bool verlet = step % J.pairs_freq == 0;
+    if (pp && !verlet && tid == 0) sc.nr_valid = 0;   // the near list no longer matches the possible pairs
     if (verlet) {
         if (pp) __syncthreads();
         int valid = sc.nr_valid;

@@ -477,6 +477,7 @@ void Simulation::initFF() {
         integrator.reset(new NamedIntegrator("Langevin", p.timestep));
     }
     p.log_rows = 4096;   // event-log ring of the pulling, indentation and plane lines
+    p.verlet_skin = g.real("verlet_skin", 0.0f);   // near list of the Verlet rebuilds (this library)
     // runGPU's stride (src/gsop.cu:117-122)
     stride = p.nav;
     for (auto& u : updaters) stride = std::min(stride, u->frequency);

@@ -62,7 +62,7 @@ class Params(C.Structure):
         ("pullingPlane", C.c_int32), ("pullingPlaneDeltax", C.c_float), ("pullingPlaneKs", C.c_float),
         ("pullingPlaneKsCant", C.c_float), ("pullingPlaneZeta", C.c_float), ("pullingPlaneDir", F3),
         ("pullingPlanePos", F3), ("pullingPlaneUpdateFreq", C.c_int32), ("pullingPlaneOutputFreq", C.c_int32),
-        ("reserved2", C.c_int32 * 4),
+        ("verlet_skin", C.c_float), ("reserved2", C.c_int32 * 3),
     ]
 
 

@@ -235,6 +235,7 @@ def job_config(cfg: Config) -> JobConfig:
             p.hi_unlisted = int(g.get_bool("hi_unlisted", True))
         p.hi_b_mode = {"cholesky": sopb.HI_B_CHOLESKY, "reference": sopb.HI_B_REFCOMPAT}[g.get_str("hi_b_mode", "cholesky")]
         p.hi_refresh = g.get_int("hi_refresh", 1)
+    p.verlet_skin = g.get_float("verlet_skin", 0.0)   # near list of the Verlet rebuilds (this library)
     # runGPU's stride: nav and every updater's frequency (src/gsop.cu:117-122)
     freqs = [p.nav, p.possiblepairs_freq, g.get_int("outputtiming", 10000), p.pairs_freq, g.get_int("dcdfreq", 10000)]
     if p.indentation and g.get_bool("indentationShowTipSurf", False):

@@ -31,17 +31,19 @@ def test_library_exports(name):
 
 
 def test_struct_layout_matches_c(tmp_path):
+    # every field of the ctypes mirrors at the C compiler's offset
+    fields = [("sopb_params", sopb.Params, f[0]) for f in sopb.Params._fields_]
+    fields += [("sopb_job_desc", sopb.JobDesc, f[0]) for f in sopb.JobDesc._fields_]
+    body = "".join('printf("%%zu\\n", offsetof(%s, %s));' % (c, f) for c, _, f in fields)
     prog = tmp_path / "layout.c"
     prog.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "sopb.h"\n'
-        'int main(void){printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(sopb_params), sizeof(sopb_job_desc),'
-        ' offsetof(sopb_params, indentationRetractionStep), offsetof(sopb_params, hi_on),'
-        ' offsetof(sopb_job_desc, params), offsetof(sopb_params, lanes_per_bead)); return 0;}\n')
+        'int main(void){printf("%zu\\n%zu\\n", sizeof(sopb_params), sizeof(sopb_job_desc));' + body +
+        ' return 0;}\n')
     exe = tmp_path / "layout"
     subprocess.check_call(["gcc", "-I", os.path.join(REPO, "include"), str(prog), "-o", str(exe)])
     vals = [int(v) for v in subprocess.check_output([str(exe)]).split()]
-    want = [ctypes.sizeof(sopb.Params), ctypes.sizeof(sopb.JobDesc), sopb.Params.indentationRetractionStep.offset,
-            sopb.Params.hi_on.offset, sopb.JobDesc.params.offset, sopb.Params.lanes_per_bead.offset]
+    want = [ctypes.sizeof(sopb.Params), ctypes.sizeof(sopb.JobDesc)] + [getattr(t, f).offset for _, t, f in fields]
     assert vals == want
 
 

@@ -59,6 +59,35 @@ struct GridAux {
 __device__ __forceinline__ int64_t job_step(const JobDev* Jp) { return *(volatile const int64_t*)&Jp->step; }
 
 // ---- potentials ------------------------------------------------------------
+// Verlet-pair terms of bead i from its row (16-byte aligned), a 4-lane group:
+// lane l takes entries 4l..4l+3 of every 16 with one 16-byte load, and the
+// next block's indices are fetched before this block's four gathers, so the
+// row load overlaps the coordinate gathers.
+static_assert(kGridLpb == 4, "one int4 of row entries per lane");
+__device__ __forceinline__ void pair_row_v4(const JobDev& J, const float4* __restrict__ xs,
+                                            const int32_t* __restrict__ row, int cnt, float4 xi, int l, float3& f) {
+    const float c8 = J.c8, cut2 = J.cut2;
+    const int4* __restrict__ r4 = reinterpret_cast<const int4*>(row);
+    int k = 4 * l;
+    int4 nx = make_int4(0, 0, 0, 0);
+    if (k < cnt) nx = __ldg(r4 + l);
+    for (; k < cnt; k += 16) {
+        const int4 cur = nx;
+        if (k + 16 < cnt) nx = __ldg(r4 + (k >> 2) + 4);
+        if (k + 3 < cnt) {
+            const float4 x0 = xs[cur.x], x1 = xs[cur.y], x2 = xs[cur.z], x3 = xs[cur.w];
+            pair_term(xi, x0, c8, cut2, f);
+            pair_term(xi, x1, c8, cut2, f);
+            pair_term(xi, x2, c8, cut2, f);
+            pair_term(xi, x3, c8, cut2, f);
+        } else {
+            pair_term(xi, xs[cur.x], c8, cut2, f);
+            if (k + 1 < cnt) pair_term(xi, xs[cur.y], c8, cut2, f);
+            if (k + 2 < cnt) pair_term(xi, xs[cur.z], c8, cut2, f);
+        }
+    }
+}
+
 // All potentials of every bead at the current coordinates into aux.F; the
 // tip's share accumulates per bead (indentation_kernel.cu:71-128).
 // EXT: the job has a discrete surface or a pulling plane (a separate
@@ -86,7 +115,8 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
         float3 f = make_float3(0.f, 0.f, 0.f);
         if (act) {
             bonded_partial(J, global_bonded(J), J.x, i, xi, l, lpb, f);
-            pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
+            if ((J.cap_pl & 3) == 0) pair_row_v4(J, J.x, J.pl_j + (size_t)i * J.cap_pl, J.pl_cnt[i], xi, l, f);
+            else pairs_partial(J, J.x, nullptr, nullptr, 0, i, xi, l, lpb, f);
             if (EXT && J.discrete) mica_partial(J, i, xi, l, lpb, f);
         }
         f = group_reduce(f, lpb);

@@ -102,11 +102,6 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
     if (J.status) return;
     const int lpb = kGridLpb, l = threadIdx.x % lpb;
     const int groups = gridDim.x * (kGridBlock / lpb);
-    IndentGeom ig;
-    if (J.indent) {
-        for (int c = 0; c < 3; ++c) { ig.tip[c] = J.tip[c]; ig.micaR[c] = J.micaR[c]; ig.micaN[c] = J.micaN[c]; }
-        ig.tipR = J.tipR; ig.tipAp = J.tipAp; ig.tipBp = J.tipBp; ig.surfAp = J.surfAp; ig.surfBp = J.surfBp;
-    }
     const int g0 = blockIdx.x * (kGridBlock / lpb) + threadIdx.x / lpb;
     for (int base = 0; base < J.n; base += groups) {
         const int i = base + g0;
@@ -122,6 +117,10 @@ k_g_forces(JobDev* __restrict__ Jp, GridAux aux) {
         f = group_reduce(f, lpb);
         if (act && l == 0) {
             if (J.indent) {
+                // read from the shared copy here, not held in registers over the pair loop
+                IndentGeom ig;
+                for (int c = 0; c < 3; ++c) { ig.tip[c] = J.tip[c]; ig.micaR[c] = J.micaR[c]; ig.micaN[c] = J.micaN[c]; }
+                ig.tipR = J.tipR; ig.tipAp = J.tipAp; ig.tipBp = J.tipBp; ig.surfAp = J.surfAp; ig.surfBp = J.surfBp;
                 float3 tf;
                 if (EXT && J.discrete) tip_term(xi, ig, f, tf);
                 else indentation_term(xi, ig, f, tf);
@@ -581,10 +580,40 @@ k_g_drift(JobDev* __restrict__ Jp, GridAux a) {
     if ((threadIdx.x & 31) == 0 && d2 > 0.f) atomicMax(&a.near[0], __float_as_int(d2));   // non-negative floats order as ints
 }
 
-// Verlet rows (pairlist_kernel.cu:33-76), order kept: a warp per bead, lanes
-// over 32 candidates at a time, a ballot places the hits.  From the near rows
-// when they are usable and no bead drifted too far; else from the possible
-// rows, renewing the near rows at the current coordinates.
+// Exclusive prefix sum over the warp's lanes, and the warp total.
+__device__ __forceinline__ int warp_excl_scan(int v, int l, int& total) {
+    int s = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, s, o);
+        if (l >= o) s += t;
+    }
+    total = __shfl_sync(0xffffffffu, s, 31);
+    return s - v;
+}
+
+// Appends the candidates of `hits` (bit u: q[u]) to a row in entry order:
+// lane l holds entries 4l..4l+3 of the warp's 128, so its first hit goes
+// after the hits of the lanes below.  Returns 1 when the row overflowed.
+__device__ __forceinline__ int append_hits(int32_t* row, int cap, int& cnt, unsigned hits, const int (&q)[4], int l) {
+    int total;
+    int pos = cnt + warp_excl_scan(__popc(hits), l, total);
+    int over = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if ((hits >> u) & 1u) {
+            if (pos < cap) row[pos] = q[u];
+            else over = 1;
+            ++pos;
+        }
+    cnt += total;
+    return over;
+}
+
+// Verlet rows (pairlist_kernel.cu:33-76), order kept: a warp per bead, each
+// lane testing four consecutive candidates of the warp's 128 (four gathers in
+// flight), an order-preserving warp scan placing the hits.  From the near
+// rows when they are usable and no bead drifted too far; else from the
+// possible rows, renewing the near rows at the current coordinates.
 __global__ void __launch_bounds__(kGridBlock)
 k_g_verlet(JobDev* __restrict__ Jp, GridAux a, int force) {
     __shared__ JobDev Js;
@@ -595,8 +624,9 @@ k_g_verlet(JobDev* __restrict__ Jp, GridAux a, int force) {
     if (J.status || (!force && (step % J.stride != 0 || step % J.pairs_freq != 0))) return;
     const bool near = verlet_from_near(J, a, step, force);
     const bool renew = !near && a.nr_j;
+    const int srcw = near ? a.cap_nr : J.cap_pp;
+    const bool vec = (srcw & 3) == 0;      // 16-byte aligned source rows
     const int l = threadIdx.x & 31;
-    const unsigned below = (1u << l) - 1u;
     int err = 0, over = 0;
     for (int i = blockIdx.x * (kGridBlock / 32) + threadIdx.x / 32; i < J.n; i += gridDim.x * (kGridBlock / 32)) {
         const float4 xi = J.x[i];
@@ -605,33 +635,29 @@ k_g_verlet(JobDev* __restrict__ Jp, GridAux a, int force) {
         int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
         int32_t* nrow = renew ? a.nr_j + (size_t)i * a.cap_nr : nullptr;
         int cnt = 0, ncnt = 0;
-        for (int kb = 0; kb < src; kb += 32) {
-            const int k = kb + l;
-            int q = 0;
-            float r2 = 0.f;
-            const bool cand = k < src;
-            if (cand) {
-                q = srow[k];
-                r2 = dist2_rn(xi, J.x[q]);
+        for (int kb = 0; kb < src; kb += 128) {
+            const int k = kb + 4 * l;
+            int q[4] = {0, 0, 0, 0};
+            if (vec && k + 3 < src) {
+                const int4 v = __ldg(reinterpret_cast<const int4*>(srow + k));
+                q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (k + u < src) q[u] = __ldg(srow + k + u);
             }
-            const bool ok = cand && r2 < J.pl_t;
-            const unsigned m = __ballot_sync(0xffffffffu, ok);
-            if (ok) {
-                const int pos = cnt + __popc(m & below);
-                if (pos < J.cap_pl) row[pos] = q;
-                else err = SOPB_STATUS_CAPACITY;
+            float r2[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) r2[u] = k + u < src ? dist2_rn(xi, J.x[q[u]]) : 0.f;
+            unsigned hits = 0u, nhits = 0u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool cand = k + u < src;
+                if (cand && r2[u] < J.pl_t) hits |= 1u << u;
+                if (cand && r2[u] < J.nr_t) nhits |= 1u << u;
             }
-            cnt += __popc(m);
-            if (renew) {
-                const bool nok = cand && r2 < J.nr_t;
-                const unsigned nm = __ballot_sync(0xffffffffu, nok);
-                if (nok) {
-                    const int pos = ncnt + __popc(nm & below);
-                    if (pos < a.cap_nr) nrow[pos] = q;
-                    else over = 1;
-                }
-                ncnt += __popc(nm);
-            }
+            if (append_hits(row, J.cap_pl, cnt, hits, q, l)) err = SOPB_STATUS_CAPACITY;
+            if (renew) over |= append_hits(nrow, a.cap_nr, ncnt, nhits, q, l);
         }
         if (l == 0) {
             J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;

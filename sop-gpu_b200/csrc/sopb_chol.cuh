@@ -8,7 +8,7 @@
 // row-major matrix with a 32-float aligned leading dimension and factorised
 // in place, lower triangle, by a right-looking blocked algorithm with 64-wide
 // panels:
-//   k_chol_potrf   the 64 x 64 diagonal block, one CTA, entries in registers;
+//   k_chol_potrf   the 64 x 64 diagonal block, one CTA, in shared memory;
 //   k_chol_trsm    the panel below it, L_ik = A_ik L_kk^-T, a warp per row;
 //   k_chol_syrk_tc the trailing lower triangle, A_ij -= L_ik L_jk^T, in
 //                  128 x 128 output tiles on the tensor cores (tcgen05,
@@ -64,57 +64,89 @@ k_hi_assemble(const JobDev* __restrict__ Jp, GridAux aux) {
     }
 }
 
-// Cholesky of the diagonal block at (k, k), nb <= 64 rows: 1024 threads,
-// each holding up to 3 entries of the block's packed lower triangle in
-// registers for the whole factorisation.  Column c: the owners of column c
-// publish its entries (double-buffered), one barrier, then every thread
-// finishes its column-c entries (L_cc = sqrt(a_cc), L_rc = a_rc / L_cc) and
-// updates its entries right of c, a_rs -= a_rc a_sc / a_cc.  One barrier per
-// column.  A pivot that is not positive sets the job's status.
-constexpr int kPotrfThreads = 1024;
-constexpr int kPotrfPer = (kCholNB * (kCholNB + 1) / 2 + kPotrfThreads - 1) / kPotrfThreads;
+// Cholesky of the diagonal block at (k, k), nb <= 64 rows, in shared memory,
+// by 8-wide sub-panels: warp 0 factors the sub-panel (its diagonal 8 x 8 and
+// the rows below; lane l holds rows l, l+32 of it, the pivots and the L
+// entries of the sub-panel's columns travel by shuffles), then the 256
+// threads subtract its product from the trailing lower triangle, eight terms
+// per entry in column order.  Two barriers per sub-panel, 16 in all (the
+// unblocked form it replaced took one barrier of 1024 threads per column).
+// A pivot that is not positive sets the job's status.
+constexpr int kPotrfThreads = 256;
+constexpr int kPotrfW = 8;                    // sub-panel width
+constexpr int kPotrfRows = kCholNB / 32;      // sub-panel rows per lane
 
 __global__ void __launch_bounds__(kPotrfThreads)
 k_chol_potrf(JobDev* __restrict__ Jp, GridAux aux, int k) {
-    __shared__ float col[2][kCholNB];
+    __shared__ float A[kCholNB][kCholLdp];
     if (Jp->status) return;
     const int m = 3 * Jp->n, ld = aux.ld, nb = min(kCholNB, m - k);
-    const int tid = threadIdx.x, total = nb * (nb + 1) / 2;
+    const int tid = threadIdx.x, lane = tid & 31;
     float* M = aux.tensor + (size_t)k * ld + k;
-    float a[kPotrfPer];
-    int rs[kPotrfPer];   // row << 8 | column
-#pragma unroll
-    for (int u = 0; u < kPotrfPer; ++u) {
-        const int e = tid + u * kPotrfThreads;
-        int r = (int)((sqrtf(8.f * (float)e + 1.f) - 1.f) * 0.5f);
-        while ((r + 1) * (r + 2) / 2 <= e) ++r;
-        while (r * (r + 1) / 2 > e) --r;
-        const int c = e - r * (r + 1) / 2;
-        rs[u] = e < total ? (r << 8 | c) : -1;
-        a[u] = e < total ? M[(size_t)r * ld + c] : 0.f;
+    for (int e = tid; e < nb * nb; e += kPotrfThreads) {
+        const int r = e / nb, c = e - r * nb;
+        if (c <= r) A[r][c] = M[(size_t)r * ld + c];
     }
+    __syncthreads();
     int bad = 0;
-    for (int c = 0; c < nb; ++c) {
-        float* cb = col[c & 1];
+    for (int c0 = 0; c0 < nb; c0 += kPotrfW) {
+        const int w = min(kPotrfW, nb - c0);
+        if (tid < 32) {
+            // rows c0 + lane + 32 h of the sub-panel
+            float v[kPotrfRows][kPotrfW];
 #pragma unroll
-        for (int u = 0; u < kPotrfPer; ++u)
-            if (rs[u] >= 0 && (rs[u] & 255) == c) cb[rs[u] >> 8] = a[u];
-        __syncthreads();
-        const float d = cb[c];
-        if (!(d > 0.f)) bad = 1;
-        const float inv = 1.0f / d, rsd = rsqrtf(d);
+            for (int h = 0; h < kPotrfRows; ++h) {
+                const int r = c0 + lane + 32 * h;
 #pragma unroll
-        for (int u = 0; u < kPotrfPer; ++u) {
-            if (rs[u] < 0) continue;
-            const int r = rs[u] >> 8, s = rs[u] & 255;
-            if (s == c) a[u] = r == c ? sqrtf(d) : a[u] * rsd;
-            else if (s > c) a[u] -= cb[r] * cb[s] * inv;
+                for (int c = 0; c < kPotrfW; ++c) v[h][c] = (r < nb && c < w) ? A[r][c0 + c] : 0.f;
+            }
+#pragma unroll
+            for (int c = 0; c < kPotrfW; ++c) {
+                if (c >= w) break;
+                const float d = __shfl_sync(0xffffffffu, v[0][c], c);
+                if (!(d > 0.f)) bad = 1;
+                const float rsd = rsqrtf(d), sd = sqrtf(d);
+#pragma unroll
+                for (int h = 0; h < kPotrfRows; ++h) {
+                    const int r = lane + 32 * h;   // row within the sub-panel
+                    if (r == c) v[h][c] = sd;
+                    else if (r > c) v[h][c] *= rsd;
+                }
+#pragma unroll
+                for (int t = c + 1; t < kPotrfW; ++t) {
+                    const float lt = __shfl_sync(0xffffffffu, v[0][c], t);   // L of row c0+t, column c
+#pragma unroll
+                    for (int h = 0; h < kPotrfRows; ++h)
+                        if (lane + 32 * h >= t) v[h][t] -= v[h][c] * lt;
+                }
+            }
+#pragma unroll
+            for (int h = 0; h < kPotrfRows; ++h) {
+                const int r = c0 + lane + 32 * h;
+#pragma unroll
+                for (int c = 0; c < kPotrfW; ++c)
+                    if (r < nb && c < w && c0 + c <= r) A[r][c0 + c] = v[h][c];
+            }
         }
-    }
+        __syncthreads();
+        // trailing lower triangle: rows and columns c0 + w .. nb - 1
+        const int t0 = c0 + w, R = nb - t0;
+        for (int e = tid; e < R * R; e += kPotrfThreads) {
+            const int r = t0 + e / R, q = t0 + e % R;
+            if (q > r) continue;
+            float acc = A[r][q];
 #pragma unroll
-    for (int u = 0; u < kPotrfPer; ++u)
-        if (rs[u] >= 0) M[(size_t)(rs[u] >> 8) * ld + (rs[u] & 255)] = a[u];
-    if (bad && tid == 0) Jp->status = SOPB_ERR_HI;
+            for (int c = 0; c < kPotrfW; ++c)
+                if (c < w) acc -= A[r][c0 + c] * A[q][c0 + c];
+            A[r][q] = acc;
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < nb * nb; e += kPotrfThreads) {
+        const int r = e / nb, c = e - r * nb;
+        if (c <= r) M[(size_t)r * ld + c] = A[r][c];
+    }
+    if (bad) atomicMax(&Jp->status, SOPB_ERR_HI);
 }
 
 // Panel solve below the diagonal block: row r of A[k+nb.., k..k+nb) becomes
@@ -423,6 +455,9 @@ k_chol_syrk_tc(JobDev* __restrict__ Jp, GridAux aux, int k, int part) {
             : "r"(s_mbar), "r"(0u)
             : "memory");
     }
+    // one verdict for the whole CTA, so the warp-wide TMEM reads below run
+    // in every lane or in none
+    done = __syncthreads_and((int)done) ? 1u : 0u;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     // accumulator -> shared memory (the A operands are no longer read)
     float* acc_s = reinterpret_cast<float*>(buf);

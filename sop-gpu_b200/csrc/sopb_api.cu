@@ -1456,7 +1456,12 @@ int run_ordered(sopb_context* c, sopb_job* const* jobs, int32_t njobs, const int
         if (grid.empty() && cls.size() == 1)
             return launch_resident(cls[0].block, (int)cls[0].ids.size(), cls[0].smem, st, c->d_jobs, d_ids, d_steps);
     } else {
-        plan.jobs.clear();          // the table on this stream is no longer the plan's
+        // no resident jobs in this run: no classes to launch, and the table
+        // on this stream is no longer the plan's
+        plan.jobs.clear();
+        plan.steps.clear();
+        plan.cls.clear();
+        plan.off.clear();
         plan.generation = ~uint64_t(0);
     }
     // one grid job alone: straight on the stream

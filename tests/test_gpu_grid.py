@@ -77,3 +77,27 @@ def test_concurrent_grid_jobs_equal_alone(gpu_ctx):
         assert j.status() == 0
         assert np.array_equal(j.read(sopb.COORDS), ref)
         j.destroy()
+
+
+def test_grid_only_run_after_resident_run_on_the_same_stream(gpu_ctx):
+    # a run of several grid jobs and no resident job, after a run of resident
+    # jobs on the same stream, launches nothing of that earlier run: each
+    # grid job equals itself run alone
+    specs = [spec(200, 81, "clamp", grid_path=1), spec(260, 82, "ramp", grid_path=1)]
+    alone = []
+    for sp in specs:
+        j = gpu_ctx.job(sp)
+        gpu_ctx.run([j], 40)
+        alone.append(j.read(sopb.COORDS))
+        j.destroy()
+    res = [gpu_ctx.job(spec(120 + 30 * k, 90 + k, "clamp")) for k in range(3)]
+    gpu_ctx.run(res, [30, 20, 10])
+    for j in res:
+        assert j.status() == 0
+        j.destroy()
+    jobs = [gpu_ctx.job(sp) for sp in specs]
+    gpu_ctx.run(jobs, 40)
+    for j, ref in zip(jobs, alone):
+        assert j.status() == 0
+        assert np.array_equal(j.read(sopb.COORDS), ref)
+        j.destroy()

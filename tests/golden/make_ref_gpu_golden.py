@@ -31,7 +31,7 @@ def main():
     pack_only = bool(args) and args[0] == "--pack"
     if pack_only:
         args = args[1:]
-    out = os.path.abspath(args[0] if args else "gpurun_out/refgold")
+    out = os.path.abspath(args[0] if args else "refgold")
     names = args[1:] or [c for c in ref_cases.CASES if not ref_cases.CASES[c].get("speed")]
     for name in names:
         c = ref_cases.CASES[name]

@@ -367,8 +367,10 @@ def run_gpu(args):
         if world == 1 and not args.no_cpu:
             sample = specs[:: max(1, len(specs) // 64)]
             v, cores, desc = cpu_rate(sample, target_s=args.ref_seconds)
+            v1, _, desc1 = cpu_rate(sample[:8], target_s=args.ref_seconds / 2, nthreads=1)
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                   "sample": "CPU restatement, OpenMP over jobs: " + desc}
+                   "sample": "CPU restatement, OpenMP over jobs: " + desc,
+                   "single_thread": {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}}
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

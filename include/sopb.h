@@ -254,7 +254,12 @@ int sopb_context_set_shape_policy(sopb_context* ctx, int32_t lanes_per_bead, flo
  * drain. */
 int sopb_context_sync(sopb_context* ctx);
 
-/* Device bytes a job needs (admission by HBM footprint). */
+/* Device bytes a job needs (admission by HBM footprint): its maps and
+ * lists, its share of the context's bead pools and, for a job on the grid
+ * path (HI, above 2048 beads, or grid_path 1), its own buffers -- the HI
+ * buffers and the exact-HI tensor included -- sized for the current
+ * device.  Host arithmetic only; the reference has no counterpart (each of
+ * its plugins allocates in its constructor). */
 int sopb_job_footprint(const sopb_job_desc* desc, size_t* bytes);
 
 /* Builds a job's device state: coordinates, covalent and native maps,

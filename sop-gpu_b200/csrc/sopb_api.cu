@@ -903,22 +903,59 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
 
 }  // namespace
 
+namespace {
+// Device bytes of a grid job's own buffers beyond the job block: the same
+// sizes grid_alloc allocates (force partials, the HI buffers and the exact-HI
+// tensor, the cell list, the near list), for `sms` SMs.
+size_t grid_aux_bytes(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl) {
+    const int64_t npart = std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)sms * 8);
+    const bool cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
+    const bool hi = p.hi_on != 0;
+    const int64_t itiles = (n + kHiTile - 1) / kHiTile;
+    const bool blocked = hi && p.hi_exact && n > 128;
+    int64_t jsplit = 1;
+    if ((hi && !p.hi_exact && p.hi_unlisted) || blocked)
+        jsplit = std::max<int64_t>(1, std::min<int64_t>((4 * (int64_t)sms + itiles - 1) / itiles, itiles));
+    size_t b = align256((size_t)std::max<int64_t>(2 * npart, hi ? jsplit * n : 0) * 16);
+    if (hi) {
+        b += 4 * align256((size_t)n * 16) + align256((size_t)n * 4);
+        if (p.hi_exact) {
+            const int64_t ld = blocked ? chol_ld((int)n) : 3 * n;
+            b += align256((size_t)(3 * n) * ld * 4);
+        }
+    }
+    b += align256(8 * sizeof(float));
+    if (cells) b += 2 * align256(((size_t)kCellMax + 1) * 4) + 2 * align256((size_t)n * 4);
+    const int64_t cap_nr = grid_cap_nr(p, cap_pp, cap_pl);
+    b += align256(4 * sizeof(int32_t));
+    if (cap_nr) b += align256((size_t)n * cap_nr * 4) + align256((size_t)n * 4) + align256((size_t)n * 16);
+    return b;
+}
+}  // namespace
+
 extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
     if (!d || !bytes || d->n <= 0) return SOPB_ERR_INVALID;
     const int64_t n = d->n;
     const int64_t cap_pp = std::max<int64_t>(1, std::min<int64_t>(d->params.max_possiblePairs > 0 ? d->params.max_possiblePairs : 4096, n - 1));
     const int64_t cap_pl = std::max<int64_t>(1, std::min<int64_t>(d->params.max_pairs > 0 ? d->params.max_pairs : 512, n - 1));
+    const sopb_params& p = d->params;
+    const bool grid = p.grid_path == 1 || p.hi_on || n > kMaxResidentBeads;
     size_t b = 0;
     b += align256((n + 1) * 4) * 2;                 // offsets
     b += align256(2 * (size_t)d->nbonds * 8);       // cov_j + r0
     b += align256(2 * (size_t)d->nnatives * 12);    // nat_j + par
     b += align256(n * 4) * 2;                       // counts
-    b += align256(n * cap_pp * 4) + align256(n * cap_pl * 4);
+    if (grid) {
+        b += align256(n * cap_pp * 4);              // possible-pair rows
+    } else {
+        const int64_t W = (n + 31) / 32;
+        b += 2 * align256(n * W * 4);               // exclusion and possible-pair masks
+        // near list (u16 rows) and the coordinates it was built at
+        b += align256(n * std::max<int64_t>(1, std::min<int64_t>(n - 1, 2 * cap_pl)) * 2) + align256(n * 4) +
+             align256(n * 16);
+    }
+    b += align256(n * cap_pl * 4);                  // Verlet rows
     b += n * (16 + 16 + 16 + 4 + 16 + 1);           // bead pools
-    // near list: u16 rows of a resident job, int32 rows of a grid job
-    b += std::max(align256(n * std::min<int64_t>(n - 1, 2 * cap_pl) * 2),
-                  align256(n * grid_cap_nr(d->params, cap_pp, cap_pl) * 4)) + align256(n * 4) + align256(n * 16);
-    const sopb_params& p = d->params;
     if ((p.pulling && p.deltax != 0.0f) || p.indentation || p.pullingPlane)
         b += align256((size_t)(p.log_rows > 0 ? p.log_rows : 1024) * 64);                        // event log
     if (p.indentation && p.indentationDiscreteSurf) {
@@ -926,6 +963,16 @@ extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
         b += 2 * align256(ns * 16) + align256(n * ((ns + 31) / 32) * 4);                          // surface, lists
     }
     if (p.pullingPlane) b += align256(n) + 2 * align256(n * 4) + align256(n * 4 + 4);            // plane
+    // a job on the grid path (HI, above the resident size, or asked for):
+    // its own buffers, sized for the current device's SMs (148 without one)
+    if (grid) {
+        int sms = 148, dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        b += grid_aux_bytes(p, n, sms, cap_pp, cap_pl);
+    }
     *bytes = b;
     return SOPB_OK;
 }

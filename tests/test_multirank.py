@@ -47,3 +47,22 @@ def test_one_process_needs_no_collective():
     sys.path.insert(0, REPO)
     import bench
     assert bench.reduce_over_ranks(None, 123, 4.5, "cpu") == (123.0, 4.5)
+
+
+def test_reference_arm_under_two_ranks_prints_one_line():
+    # the driver launches the reference arm like its own (torchrun, one
+    # process per GPU): rank 0 times the CPU restatement and prints the one
+    # JSON line, the other rank exits 0 without work
+    import json
+    import subprocess
+    port = 30500 + os.getpid() % 1000
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.join(REPO, "bench.py"),
+           "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0", "--ref-seconds", "0.3"]
+    r = subprocess.run(cmd, cwd=REPO, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0

@@ -376,15 +376,20 @@ int sopb_jobs_download_coords(sopb_context* ctx, sopb_job* const* jobs, int32_t 
  *   d_ci4      out: float[4n] per bead, the squared row sums of the normalised
  *                   RPY blocks (x y z) and the sum of their entries (w), the
  *                   reference's d_ci / d_epsilon (bdhitea_kernel.cu:234-249);
- *   d_beta_eps out: float[2] beta' and epsilon (bdhitea.cu:143-169, without
- *                   the capricious abort).
+ *   d_beta_eps out: float[2] beta' and epsilon (bdhitea.cu:143-169, as with
+ *                   hi_capricious off: an epsilon above 1 is set to 1 without
+ *                   an error, and hi_epsmax is not checked -- a caller that
+ *                   needs either test compares epsilon with 1 or its limit).
+ * d_xyzw and d_ci4 must be 16-byte aligned and d_beta_eps 4-byte aligned
+ * (SOPB_ERR_INVALID otherwise).
  * Scratch is a 4 MiB array in the library image (held by every GPU that
  * loads the library until exit), shared by all calls: calls that overlap on
  * the GPU race and must be ordered by the caller.  n up to 262144 beads
- * (SOPB_ERR_CAPACITY above).  The first call on a device does a one-time
- * set-up and should come before any stream capture.  Work is queued on
- * `stream` (a cudaStream_t, NULL = the default stream); the call does not
- * wait for it. */
+ * (SOPB_ERR_CAPACITY above).  The first call in each CUDA context (the
+ * device's primary context, one made with cuCtxCreate, or the new primary
+ * context after a cudaDeviceReset) does a one-time set-up and should come
+ * before any stream capture.  Work is queued on `stream` (a cudaStream_t,
+ * NULL = the default stream); the call does not wait for it. */
 int sopb_tea_coefficients_noalloc(const float* d_xyzw, int32_t n, float hi_a, float* d_ci4, float* d_beta_eps,
                                   void* stream);
 

@@ -2,9 +2,10 @@
 # Compiles the reference's own host code for the golden-vector harness from
 # the SOP-GPU source tree where it lies (read only), into oracle/_ref/.
 # Nothing from the reference tree is copied into this repository.
-# Usage: oracle/build_ref.sh [path-to-SOP-GPU]   (default /root/reference)
+# Usage: oracle/build_ref.sh [path-to-SOP-GPU]
+# (default: $SOPB_REFERENCE_DIR, else the build container's /root/reference)
 set -e
-REF=${1:-/root/reference}
+REF=${1:-${SOPB_REFERENCE_DIR:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then

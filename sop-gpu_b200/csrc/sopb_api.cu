@@ -631,85 +631,105 @@ void build_maps(const sopb_job_desc* d, HostMaps& m) {
 
 namespace {
 
+// Byte layout of a grid job's own buffer block: force partials, the HI
+// buffers and the exact-HI tensor, the cell-list arrays and the near list.
+// grid_alloc carves the block by these offsets and sopb_job_footprint adds
+// its total, so admission and allocation cannot disagree.
+struct GridLayout {
+    int npart = 0, jsplit = 1, cap_nr = 0, ld = 0;
+    bool cells = false, hi = false, exact = false, blocked = false;
+    size_t part = 0, rf = 0, mf = 0, xc = 0, ci = 0, eps = 0, ten = 0, geo = 0;
+    size_t cc = 0, cs = 0, cb = 0, bc = 0, near = 0, nrj = 0, nrc = 0, xref = 0;
+    size_t total = 0;
+};
+
+GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl) {
+    GridLayout L;
+    L.npart = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)sms * 8);
+    L.cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
+    L.hi = p.hi_on != 0;
+    L.exact = L.hi && p.hi_exact;
+    L.blocked = L.exact && n > 128;
+    const int64_t itiles = (n + kHiTile - 1) / kHiTile;
+    if ((L.hi && !p.hi_exact && p.hi_unlisted) || L.blocked)
+        L.jsplit = (int)std::max<int64_t>(1, std::min<int64_t>((4 * (int64_t)sms + itiles - 1) / itiles, itiles));
+    size_t off = 0;
+    auto take = [&](size_t bytes) { const size_t o = off; off += align256(bytes); return o; };
+    L.part = take(std::max<size_t>(2 * (size_t)L.npart, L.hi ? (size_t)L.jsplit * n : 0) * sizeof(float4));
+    if (L.hi) {
+        L.rf = take((size_t)n * 16);
+        L.mf = take((size_t)n * 16);
+        L.xc = take((size_t)n * 16);
+        L.ci = take((size_t)n * 16);
+        L.eps = take((size_t)n * 4);
+        if (L.exact) {
+            L.ld = L.blocked ? chol_ld((int)n) : (int)(3 * n);
+            L.ten = take((size_t)3 * n * L.ld * 4);
+        }
+    }
+    L.geo = take(8 * sizeof(float));
+    if (L.cells) {
+        L.cc = take(((size_t)kCellMax + 1) * 4);
+        L.cs = take(((size_t)kCellMax + 1) * 4);
+        L.cb = take((size_t)n * 4);
+        L.bc = take((size_t)n * 4);
+    }
+    L.cap_nr = (int)grid_cap_nr(p, cap_pp, cap_pl);
+    L.near = take(4 * sizeof(int32_t));
+    if (L.cap_nr) {
+        L.nrj = take((size_t)n * L.cap_nr * 4);
+        L.nrc = take((size_t)n * 4);
+        L.xref = take((size_t)n * 16);
+    }
+    L.total = off;
+    return L;
+}
+
 // Buffers of the grid path: force buffer (the context's second coordinate
 // pool), reduction partials and, for large jobs, the cell list.
 int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, int32_t cap_pp, int32_t cap_pl) {
     GridAux& a = j->aux;
-    j->bead_blocks = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)c->sm_count * 8);
-    a.npart = j->bead_blocks;
-    a.use_cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
-    const bool hi = p.hi_on != 0;
-    const int itiles = (n + kHiTile - 1) / kHiTile;
-    j->jsplit = 1;
-    const bool blocked = hi && p.hi_exact && n > 128;
-    if ((hi && !p.hi_exact && p.hi_unlisted) || blocked)
-        j->jsplit = std::max(1, std::min((4 * c->sm_count + itiles - 1) / itiles, itiles));
-    const size_t part_elems = std::max<size_t>(2 * (size_t)a.npart, hi ? (size_t)j->jsplit * n : 0);
-    size_t off = 0;
-    const size_t o_part = off; off += align256(part_elems * sizeof(float4));
-    size_t o_rf = 0, o_mf = 0, o_xc = 0, o_ci = 0, o_eps = 0, o_ten = 0;
-    if (hi) {
-        o_rf = off; off += align256((size_t)n * 16);
-        o_mf = off; off += align256((size_t)n * 16);
-        o_xc = off; off += align256((size_t)n * 16);
-        o_ci = off; off += align256((size_t)n * 16);
-        o_eps = off; off += align256((size_t)n * 4);
-        if (p.hi_exact) {
-            a.ld = blocked ? chol_ld(n) : 3 * n;
-            o_ten = off; off += align256((size_t)3 * n * a.ld * 4);
-        }
-    }
-    const size_t o_geo = off; off += align256(8 * sizeof(float));
-    size_t o_cc = 0, o_cs = 0, o_cb = 0, o_bc = 0;
-    if (a.use_cells) {
-        o_cc = off; off += align256(((size_t)kCellMax + 1) * 4);
-        o_cs = off; off += align256(((size_t)kCellMax + 1) * 4);
-        o_cb = off; off += align256((size_t)n * 4);
-        o_bc = off; off += align256((size_t)n * 4);
-    }
-    // near list of the Verlet rebuilds
-    a.cap_nr = (int32_t)grid_cap_nr(p, cap_pp, cap_pl);
-    size_t o_nrj = 0, o_nrc = 0, o_xref = 0;
-    const size_t o_near = off; off += align256(4 * sizeof(int32_t));
-    if (a.cap_nr) {
-        o_nrj = off; off += align256((size_t)n * a.cap_nr * 4);
-        o_nrc = off; off += align256((size_t)n * 4);
-        o_xref = off; off += align256((size_t)n * 16);
-    }
-    if (cudaMallocAsync(&j->amem, off, c->upload) != cudaSuccess) {
+    const GridLayout L = grid_layout(p, n, c->sm_count, cap_pp, cap_pl);
+    j->bead_blocks = L.npart;
+    j->jsplit = L.jsplit;
+    a.npart = L.npart;
+    a.use_cells = L.cells;
+    a.cap_nr = L.cap_nr;
+    if (L.exact) a.ld = L.ld;
+    if (cudaMallocAsync(&j->amem, L.total, c->upload) != cudaSuccess) {
         cudaGetLastError();
         return SOPB_ERR_NOMEM;
     }
     char* b = (char*)j->amem;
     a.F = c->xalt + j->b0;
-    a.part = (float4*)(b + o_part);
-    if (hi) {
-        a.rf = (float4*)(b + o_rf);
-        a.mf = (float4*)(b + o_mf);
-        a.xc = (float4*)(b + o_xc);
-        a.ci4 = (float4*)(b + o_ci);
-        a.eps = (float*)(b + o_eps);
-        if (p.hi_exact) a.tensor = (float*)(b + o_ten);
-        if (blocked) {
+    a.part = (float4*)(b + L.part);
+    if (L.hi) {
+        a.rf = (float4*)(b + L.rf);
+        a.mf = (float4*)(b + L.mf);
+        a.xc = (float4*)(b + L.xc);
+        a.ci4 = (float4*)(b + L.ci);
+        a.eps = (float*)(b + L.eps);
+        if (L.exact) a.tensor = (float*)(b + L.ten);
+        if (L.blocked) {
             CUDA_TRY(cudaStreamCreateWithFlags(&j->la, cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&j->la_fork, cudaEventDisableTiming));
             CUDA_TRY(cudaEventCreateWithFlags(&j->la_join, cudaEventDisableTiming));
         }
     }
-    a.cell_geo = (float*)(b + o_geo);
-    a.near = (int32_t*)(b + o_near);
+    a.cell_geo = (float*)(b + L.geo);
+    a.near = (int32_t*)(b + L.near);
     if (a.cap_nr) {
-        a.nr_j = (int32_t*)(b + o_nrj);
-        a.nr_cnt = (int32_t*)(b + o_nrc);
-        a.x_ref = (float4*)(b + o_xref);
+        a.nr_j = (int32_t*)(b + L.nrj);
+        a.nr_cnt = (int32_t*)(b + L.nrc);
+        a.x_ref = (float4*)(b + L.xref);
     }
     if (a.use_cells) {
-        a.cell_count = (int32_t*)(b + o_cc);
-        a.cell_start = (int32_t*)(b + o_cs);
-        a.cell_beads = (int32_t*)(b + o_cb);
-        a.bead_cell = (int32_t*)(b + o_bc);
+        a.cell_count = (int32_t*)(b + L.cc);
+        a.cell_start = (int32_t*)(b + L.cs);
+        a.cell_beads = (int32_t*)(b + L.cb);
+        a.bead_cell = (int32_t*)(b + L.bc);
     }
-    CUDA_TRY(cudaMemsetAsync(j->amem, 0, off, c->upload));
+    CUDA_TRY(cudaMemsetAsync(j->amem, 0, L.total, c->upload));
     return SOPB_OK;
 }
 
@@ -903,36 +923,6 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
 
 }  // namespace
 
-namespace {
-// Device bytes of a grid job's own buffers beyond the job block: the same
-// sizes grid_alloc allocates (force partials, the HI buffers and the exact-HI
-// tensor, the cell list, the near list), for `sms` SMs.
-size_t grid_aux_bytes(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl) {
-    const int64_t npart = std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)sms * 8);
-    const bool cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
-    const bool hi = p.hi_on != 0;
-    const int64_t itiles = (n + kHiTile - 1) / kHiTile;
-    const bool blocked = hi && p.hi_exact && n > 128;
-    int64_t jsplit = 1;
-    if ((hi && !p.hi_exact && p.hi_unlisted) || blocked)
-        jsplit = std::max<int64_t>(1, std::min<int64_t>((4 * (int64_t)sms + itiles - 1) / itiles, itiles));
-    size_t b = align256((size_t)std::max<int64_t>(2 * npart, hi ? jsplit * n : 0) * 16);
-    if (hi) {
-        b += 4 * align256((size_t)n * 16) + align256((size_t)n * 4);
-        if (p.hi_exact) {
-            const int64_t ld = blocked ? chol_ld((int)n) : 3 * n;
-            b += align256((size_t)(3 * n) * ld * 4);
-        }
-    }
-    b += align256(8 * sizeof(float));
-    if (cells) b += 2 * align256(((size_t)kCellMax + 1) * 4) + 2 * align256((size_t)n * 4);
-    const int64_t cap_nr = grid_cap_nr(p, cap_pp, cap_pl);
-    b += align256(4 * sizeof(int32_t));
-    if (cap_nr) b += align256((size_t)n * cap_nr * 4) + align256((size_t)n * 4) + align256((size_t)n * 16);
-    return b;
-}
-}  // namespace
-
 extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
     if (!d || !bytes || d->n <= 0) return SOPB_ERR_INVALID;
     const int64_t n = d->n;
@@ -971,7 +961,7 @@ extern "C" int sopb_job_footprint(const sopb_job_desc* d, size_t* bytes) {
             cudaGetLastError();
             sms = 148;
         }
-        b += grid_aux_bytes(p, n, sms, cap_pp, cap_pl);
+        b += grid_layout(p, n, sms, cap_pp, cap_pl).total;
     }
     *bytes = b;
     return SOPB_OK;
@@ -1846,11 +1836,17 @@ extern "C" int sopb_jobs_download_coords(sopb_context* c, sopb_job* const* jobs,
 // it keeps the last call's contents; each call overwrites every slot it reads
 // before reading it, so nothing has to start at zero.  Calls that overlap on
 // the GPU (two streams, or two host threads) race on the array and must be
-// ordered by the caller.  The first call on a device does the set-up (it
-// looks up the array's device address with cudaGetSymbolAddress, with that
-// device current); make that first call before any stream capture.
+// ordered by the caller.  The first call in each CUDA context does the set-up
+// (it looks up the array's device address in that context with
+// cudaGetSymbolAddress); make that first call before any stream capture.  A
+// context is told apart by its driver-assigned id, unique for the life of the
+// process, so a context made with cuCtxCreate, or the new primary context
+// after a cudaDeviceReset, gets its own look-up instead of a stale address.
 // ===========================================================================
 #include <mutex>
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 namespace {
 
@@ -1858,10 +1854,43 @@ namespace {
 constexpr int kNoAllocSlots = 1 << 18;   // 4 MiB
 static __device__ __align__(256) float4 s_tea_partials[kNoAllocSlots];
 
-constexpr int kMaxDevices = 64;
+// Set-up cache: the device address of s_tea_partials and the SM count, per
+// CUDA context.  Host code cannot use the symbol itself as a device address.
+struct NoAllocSetup {
+    unsigned long long ctx_id;   // 0 = empty slot (driver ids start at 1)
+    float4* part;
+    int sms;
+};
+constexpr int kNoAllocContexts = 64;
 std::mutex g_mutex;
-float4* g_partials[kMaxDevices] = {};     // device address of s_tea_partials, per device
-int g_sms[kMaxDevices] = {};
+NoAllocSetup g_setup[kNoAllocContexts] = {};
+int g_setup_next = 0;             // slot to reuse once all are taken
+PFN_cuCtxGetId_v12000 g_ctx_get_id = nullptr;
+
+// Id of the current CUDA context (cuCtxGetId through the runtime's driver
+// entry-point table, so the library needs no link against libcuda).  With
+// no context current yet, the current device's primary context is made
+// current first.  Called with g_mutex held.
+int current_context_id(unsigned long long* id) {
+    if (!g_ctx_get_id) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return SOPB_ERR_CUDA;
+        }
+        g_ctx_get_id = reinterpret_cast<PFN_cuCtxGetId_v12000>(fn);
+    }
+    if (g_ctx_get_id(nullptr, id) == CUDA_SUCCESS && *id != 0) return SOPB_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return SOPB_ERR_NODEVICE;
+    }
+    if (g_ctx_get_id(nullptr, id) == CUDA_SUCCESS && *id != 0) return SOPB_OK;
+    return SOPB_ERR_CUDA;
+}
 
 // Unlisted branch of k_tea_eps_partial on plain pointers.
 __global__ void __launch_bounds__(kHiTile)
@@ -1927,33 +1956,37 @@ k_tea_beta_raw(const float4* __restrict__ ci4, int n, float* __restrict__ out) {
 extern "C" int sopb_tea_coefficients_noalloc(const float* d_xyzw, int32_t n, float hi_a, float* d_ci4,
                                              float* d_beta_eps, void* stream) {
     if (!d_xyzw || !d_ci4 || !d_beta_eps || n < 1 || !(hi_a > 0.0f)) return SOPB_ERR_INVALID;
+    // float4 loads and stores need 16-byte alignment, the two floats 4 bytes
+    if ((((uintptr_t)d_xyzw | (uintptr_t)d_ci4) & 15) || ((uintptr_t)d_beta_eps & 3)) return SOPB_ERR_INVALID;
     if (n > kNoAllocSlots) return SOPB_ERR_CAPACITY;   // one slice of n partials must fit the array
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        cudaGetLastError();
-        return SOPB_ERR_NODEVICE;
-    }
     float4* part = nullptr;
     int sms = 0;
     {
-        // set-up, once per device, with that device current: the device
-        // address of the array (host code cannot use the symbol itself)
+        // set-up, once per CUDA context, with that context current
         std::lock_guard<std::mutex> lock(g_mutex);
-        if (!g_partials[dev]) {
+        unsigned long long id = 0;
+        const int rc = current_context_id(&id);
+        if (rc != SOPB_OK) return rc;
+        const NoAllocSetup* hit = nullptr;
+        for (const NoAllocSetup& e : g_setup)
+            if (e.ctx_id == id) { hit = &e; break; }
+        if (!hit) {
             void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, s_tea_partials);
-            if (e != cudaSuccess || !p) {
+            int dev = 0, nsm = 0;
+            if (cudaGetSymbolAddress(&p, s_tea_partials) != cudaSuccess || !p || cudaGetDevice(&dev) != cudaSuccess ||
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || nsm < 1) {
                 cudaGetLastError();
                 return SOPB_ERR_CUDA;
             }
-            if (cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
-                cudaGetLastError();
-                return SOPB_ERR_CUDA;
-            }
-            g_partials[dev] = static_cast<float4*>(p);
+            int slot = -1;
+            for (int k = 0; k < kNoAllocContexts && slot < 0; ++k)
+                if (g_setup[k].ctx_id == 0) slot = k;
+            if (slot < 0) slot = g_setup_next++ % kNoAllocContexts;
+            g_setup[slot] = NoAllocSetup{id, static_cast<float4*>(p), nsm};
+            hit = &g_setup[slot];
         }
-        part = g_partials[dev];
-        sms = g_sms[dev];
+        part = hit->part;
+        sms = hit->sms;
     }
     // the TEA updater's slicing (4 CTAs per SM), capped by the array
     const int itiles = (n + kHiTile - 1) / kHiTile;

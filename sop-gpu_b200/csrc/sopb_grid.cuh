@@ -574,8 +574,10 @@ k_g_drift(JobDev* __restrict__ Jp, GridAux a) {
     const int64_t step = job_step(Jp);
     if (J.status || step % J.stride != 0 || step % J.pairs_freq != 0 || step % J.pp_freq == 0 || !a.near[2]) return;
     float d2 = 0.f;
-    for (int i = blockIdx.x * kGridBlock + threadIdx.x; i < J.n; i += gridDim.x * kGridBlock)
-        d2 = fmaxf(d2, dist2_rn(a.x_ref[i], J.x[i]));
+    for (int i = blockIdx.x * kGridBlock + threadIdx.x; i < J.n; i += gridDim.x * kGridBlock) {
+        const float e = dist2_rn(a.x_ref[i], J.x[i]);
+        d2 = fmaxf(d2, isfinite(e) ? e : INFINITY);   // fmaxf drops a NaN: count it as an infinite drift
+    }
     for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
     if ((threadIdx.x & 31) == 0 && d2 > 0.f) atomicMax(&a.near[0], __float_as_int(d2));   // non-negative floats order as ints
 }

@@ -286,7 +286,10 @@ __device__ void rebuild_verlet(const JobDev& J, const float4* __restrict__ xs, i
     __syncthreads();
     if (valid && !possible_changed) {
         float d2 = 0.f;
-        for (int i = tid; i < n; i += BLOCK) d2 = fmaxf(d2, dist2_rn(J.x_ref[i], xs[i]));
+        for (int i = tid; i < n; i += BLOCK) {
+            const float e = dist2_rn(J.x_ref[i], xs[i]);
+            d2 = fmaxf(d2, isfinite(e) ? e : INFINITY);   // fmaxf drops a NaN: count it as an infinite drift
+        }
         if (d2 > 0.f) atomicMax(&drift_bits, __float_as_int(d2));   // non-negative floats order as ints
     }
     __syncthreads();

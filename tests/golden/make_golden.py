@@ -37,7 +37,7 @@ def run(*args):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SOPB_REFERENCE_DIR", "/root/reference")
     subprocess.check_call([os.path.join(REPO, "oracle", "build_ref.sh"), ref])
     if not os.path.exists(REF_HOST):
         sys.exit("reference harness not built")

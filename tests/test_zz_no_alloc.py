@@ -64,3 +64,67 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
                                                   d.data_ptr(), None)
     assert rc == sopb.ERR_CAPACITY
     assert sopb.lib().sopb_tea_coefficients_noalloc(None, 10, ctypes.c_float(1.9), None, None, None) == sopb.ERR_INVALID
+    # a caller's pool may hand out buffers at any offset: float4 buffers off
+    # a 16-byte boundary are refused instead of faulting
+    buf = torch.zeros(64, dtype=torch.float32, device="cuda")
+    base = buf.data_ptr()
+    assert base % 256 == 0
+    for xo, co, bo in ((4, 0, 0), (8, 0, 0), (0, 4, 0), (0, 0, 2)):
+        rc = sopb.lib().sopb_tea_coefficients_noalloc(base + xo, 2, ctypes.c_float(1.9), base + 64 + co,
+                                                      base + 128 + bo, None)
+        assert rc == sopb.ERR_INVALID, (xo, co, bo)
+    torch.cuda.synchronize()
+
+
+def _noalloc_on_primary_context(x, n, a):
+    import torch
+    d_x = torch.from_numpy(x).cuda()
+    d_ci = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    d_be = torch.empty(2, dtype=torch.float32, device="cuda")
+    rc = sopb.lib().sopb_tea_coefficients_noalloc(d_x.data_ptr(), n, ctypes.c_float(a), d_ci.data_ptr(),
+                                                  d_be.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert rc == sopb.OK
+    torch.cuda.synchronize()
+    return d_ci.cpu().numpy(), d_be.cpu().numpy()
+
+
+def test_noalloc_in_a_context_of_its_own():
+    """A host that creates its own CUDA context (cuCtxCreate) gets the
+    scratch address of that context, not the one cached for the primary
+    context: the results are bit-identical to the primary context's, and the
+    primary context still works after the other one is destroyed."""
+    from cuda.bindings import driver as cu
+    n, a = 500, 1.9
+    sp = spec(n, 5, "free")
+    x = np.zeros((n, 4), np.float32)
+    x[:, :3] = sp.xyz
+    ci0, be0 = _noalloc_on_primary_context(x, n, a)
+
+    def ok(res):
+        err = res[0] if isinstance(res, tuple) else res
+        assert err == cu.CUresult.CUDA_SUCCESS, err
+        return res[1] if isinstance(res, tuple) and len(res) > 1 else None
+
+    ok(cu.cuInit(0))
+    dev = ok(cu.cuDeviceGet(0))
+    ctx = ok(cu.cuCtxCreate(0, dev))
+    try:
+        d_x = ok(cu.cuMemAlloc(x.nbytes))
+        d_ci = ok(cu.cuMemAlloc(x.nbytes))
+        d_be = ok(cu.cuMemAlloc(8))
+        ok(cu.cuMemcpyHtoD(d_x, x.ctypes.data, x.nbytes))
+        for _ in range(2):
+            rc = sopb.lib().sopb_tea_coefficients_noalloc(int(d_x), n, ctypes.c_float(a), int(d_ci), int(d_be), None)
+            assert rc == sopb.OK
+            ok(cu.cuCtxSynchronize())
+            ci = np.empty_like(x)
+            be = np.empty(2, np.float32)
+            ok(cu.cuMemcpyDtoH(ci.ctypes.data, d_ci, ci.nbytes))
+            ok(cu.cuMemcpyDtoH(be.ctypes.data, d_be, be.nbytes))
+            assert np.array_equal(be, be0) and np.array_equal(ci, ci0)
+        for d in (d_x, d_ci, d_be):
+            ok(cu.cuMemFree(d))
+    finally:
+        ok(cu.cuCtxDestroy(ctx))
+    ci1, be1 = _noalloc_on_primary_context(x, n, a)
+    assert np.array_equal(be1, be0) and np.array_equal(ci1, ci0)

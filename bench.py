@@ -46,15 +46,18 @@ def log(*a):
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def plain_params(**kw):
+def plain_params(defaults=None, **kw):
+    """Parameters of the bench workloads over the reference defaults, from
+    `defaults` (the library's sopb.default_params unless given: the CPU arm
+    passes the oracle's own table so that it loads no product library)."""
     import sopb
     base = dict(timestep=0.08, zeta=50.0, temperature=0.6, pairs_freq=10, pairlist_cutoff=20.0, pairs_cutoff=20.0,
                 pairs_threshold=200.0, nav=1000)
     base.update(kw)
-    return sopb.default_params(**base)
+    return (defaults or sopb.default_params)(**base)
 
 
-def batch_specs(count=512, lo=60, hi=600, seed=2024, rank=0):
+def batch_specs(count=512, lo=60, hi=600, seed=2024, rank=0, defaults=None):
     """The ragged force-clamp batch (one independent copy per rank)."""
     import sopb
     import sopb_synth as S
@@ -66,7 +69,7 @@ def batch_specs(count=512, lo=60, hi=600, seed=2024, rank=0):
     for k, n in enumerate(sizes):
         n = int(n)
         s = S.make_system(n, base * 1000 + k)
-        p = plain_params(pulling=1, fconst=float(f_pn[k] / 70.0), fixedEnd=0, pulledEnd=n - 1)
+        p = plain_params(defaults, pulling=1, fconst=float(f_pn[k] / 70.0), fixedEnd=0, pulledEnd=n - 1)
         specs.append(sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[n - 1], seed=1119727 + k))
     return specs
 
@@ -78,6 +81,14 @@ def plain_spec(seed=2024):
     s = S.make_system(200, seed)
     p = plain_params(pulling=1, deltax=0.5, k_trans=0.05, pullFreq=1000, fixedEnd=0, pulledEnd=199)
     return sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[199], seed=1119727)
+
+
+def batch_config(specs, chunk, world):
+    """The `config` object of the batch512 line, shared by both arms."""
+    return {"workload": "batch512_lognormal_60-600_clamp", "replicas": len(specs),
+            "beads": int(sum(sp.n for sp in specs)), "langevin_steps_per_step": chunk, "pairs_freq": 10,
+            "pairlist_cutoff_A": 20.0, "dt_tauH": 0.08, "parallelism": "replicas-dp%d" % world,
+            "l2": "flushed between timed steps"}
 
 
 def list_stats(jobs, specs):
@@ -207,7 +218,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    specs = batch_specs(rank=0)
+    import oracle_py
+    import sopb
+    specs = batch_specs(rank=0, defaults=oracle_py.default_params)
     threads = os.cpu_count()
     vals = []
     sample = ""
@@ -219,11 +232,13 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded globular chains)",
-        "config": {"workload": "batch512_lognormal_60-600_clamp", "replicas": len(specs), "pairs_freq": 10},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded globular chains; no public dataset)",
+        "config": batch_config(specs, args.chunk, args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if sopb._lib is not None:
+        raise RuntimeError("the CPU reference arm loaded the product library")
     print(json.dumps(line), flush=True)
     return 0
 
@@ -376,9 +391,7 @@ def run_gpu(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded globular chains; no public dataset)",
-            "config": {"workload": "batch512_lognormal_60-600_clamp", "replicas": len(specs), "beads": beads,
-                       "langevin_steps_per_step": chunk, "pairs_freq": 10, "pairlist_cutoff_A": 20.0,
-                       "dt_tauH": 0.08, "parallelism": "replicas-dp%d" % world, "l2": "flushed between timed steps"},
+            "config": batch_config(specs, chunk, world),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": beads * 16, "d2h_bytes_per_step": beads * 16},
             "gpu_launches": launches,
             "shape_policy": None if tuned is None else {"lanes_per_bead": tuned["policy"][0],

@@ -17,7 +17,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "sop-gpu_b200"))
-import sopb  # noqa: E402  (structure layouts only)
+import sopb  # noqa: E402  (structure layouts only: sopb.py loads libsopb.so only when lib() is called)
 
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 _lib = None
@@ -35,6 +35,7 @@ def lib() -> C.CDLL:
         L = C.CDLL(LIB_PATH)
         vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
         sig = {
+            "orc_default_params": ([vp], None),
             "orc_generate_seeds": ([i32, i64, vp], None),
             "orc_rforce_n": ([i32, vp, vp], None),
             "orc_hybrid_taus": ([vp, i32, vp], None),
@@ -61,6 +62,16 @@ def lib() -> C.CDLL:
             fn.restype = res
         _lib = L
     return _lib
+
+
+def default_params(**kw) -> "sopb.Params":
+    """The reference defaults from the oracle's own table, with keyword
+    overrides (config-key names); loads no product library."""
+    p = sopb.Params()
+    lib().orc_default_params(C.byref(p))
+    for k, v in kw.items():
+        sopb.set_param(p, k, v)
+    return p
 
 
 def generate_seeds(seed: int, count: int) -> np.ndarray:

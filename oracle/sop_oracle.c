@@ -24,6 +24,53 @@
 #define F4(a, i) (&(a)[4 * (size_t)(i)])
 
 /* ------------------------------------------------------------------------ */
+/* PARAMETER() defaults of the reference headers; keys this library adds    */
+/* take the values that keep the reference's behaviour.                     */
+/* ------------------------------------------------------------------------ */
+void orc_default_params(sopb_params* p) {
+    memset(p, 0, sizeof(*p));
+    p->zeta = 50.0f;                    /* Integrators/langevin.h:13 */
+    p->temperature = 0.6f;              /* Integrators/langevin.h:14 */
+    p->kspring_cov = 20.0f;             /* Potentials/covalent.h:12 */
+    p->R_limit = 2.0f;                  /* Potentials/covalent.h:13 */
+    p->R_limit_bond = 8.0f;             /* the output manager's intact-contact cutoff */
+    p->pairs_cutoff = 20.0f;            /* Potentials/pairs.h:12 */
+    p->el = 1.0f;                       /* Potentials/pairs.h:13 */
+    p->a = 3.8f;                        /* Potentials/pairs.h:14 */
+    p->max_pairs = 512;                 /* Potentials/pairs.h:15 */
+    p->pairlist_cutoff = 20.0f;         /* Updaters/pairlist.h:12 */
+    p->pairs_freq = 1000;               /* Updaters/pairlist.h:13 */
+    p->max_possiblePairs = 4096;        /* Updaters/pairlist.h:14 */
+    p->pairs_threshold = 200.0f;        /* Updaters/possiblepairlist.h:14 */
+    p->possiblepairs_freq = 100000;     /* Updaters/possiblepairlist.h:15 */
+    p->nav = 1000;                      /* gsop.h, nav */
+    p->k_trans = 0.05f;                 /* Potentials/pulling.h:17 */
+    p->pull_direction = SOPB_PULL_END_TO_END;   /* Potentials/pulling.h:21 */
+    p->indentationTipSigma = 1.0f;      /* Potentials/indentation.h:24-25 */
+    p->indentationSurfSigma = 1.0f;     /* Potentials/indentation.h:24,26 */
+    p->indentationTipEl = 1.0f;         /* Potentials/indentation.h:27-28 */
+    p->indentationSurfEl = 1.0f;        /* Potentials/indentation.h:27,29 */
+    p->indentationTipA = 0.0f;          /* Potentials/indentation.h:30 */
+    p->indentationTipB = 1.0f;          /* Potentials/indentation.h:31 */
+    p->indentationSurfA = 0.0f;         /* Potentials/indentation.h:32 */
+    p->indentationSurfB = 1.0f;         /* Potentials/indentation.h:33 */
+    p->indentationTipZeta = 5000.0f;    /* Potentials/indentation.h:35 */
+    p->indentationRetractionStep = -1;  /* Potentials/indentation.h:37 */
+    p->indentationPairsCutoff = 40.0f;  /* Potentials/indentation.h:41 */
+    p->indentationSurfaceSize = 51;     /* Potentials/indentation.h:45 */
+    p->indentationSurfaceStep = 1.4f;   /* Potentials/indentation.h:46 */
+    p->pullingPlaneKs = 0.05f;          /* Potentials/pulling_plane.h:15 */
+    p->pullingPlaneKsCant = 0.05f;      /* Potentials/pulling_plane.h:16 */
+    p->pullingPlaneZeta = 200.0f;       /* Potentials/pulling_plane.h:17 */
+    p->hi_a = 1.8f;                     /* Integrators/bdhitea.h:17 */
+    p->hi_capricious = 1;               /* Integrators/bdhitea.h:19 */
+    p->hi_unlisted = 1;                 /* Integrators/bdhitea.h:20 */
+    p->hi_epsmax = 999.0f;              /* Integrators/bdhitea.h:21 */
+    p->hi_b_mode = SOPB_HI_B_CHOLESKY;
+    p->hi_refresh = 1;                  /* the reference refactors D every step */
+}
+
+/* ------------------------------------------------------------------------ */
 /* ran2: L'Ecuyer's combined LCG with a Bays-Durham shuffle, in the form of */
 /* Numerical Recipes (src/Integrators/ran2.cpp:51-89).  The reference keeps */
 /* idum2/iy/iv in static storage; a fresh process starts from idum2 =       */

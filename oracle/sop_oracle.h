@@ -22,6 +22,11 @@ extern "C" {
 
 typedef struct orc_job orc_job;
 
+/* The reference's PARAMETER() defaults (mandatory keys zero), written from
+ * the headers under src/ for the oracle's own use, so that the CPU baseline
+ * fills a job description without the product library. */
+void orc_default_params(sopb_params* p);
+
 /* ran2 as seen by a fresh process (src/Integrators/ran2.cpp:51-89). */
 double orc_ran2(int32_t* idum, int32_t* state /* [34]: idum2, iy, iv[32] */);
 void orc_ran2_state_init(int32_t* state);

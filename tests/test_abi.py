@@ -80,3 +80,13 @@ def test_context_without_device_reports_nodevice():
         pytest.skip("a GPU is present")
     h = ctypes.c_void_p()
     assert sopb.lib().sopb_context_create(0, None, ctypes.byref(h)) == sopb.ERR_NODEVICE
+
+
+def test_oracle_defaults_equal_library_defaults():
+    """The CPU baseline fills its job descriptions from the oracle's own
+    table of the reference's PARAMETER() defaults; it must equal the
+    library's sopb_default_params field for field."""
+    import oracle_py
+    a = sopb.params_dict(oracle_py.default_params())
+    b = sopb.params_dict(sopb.default_params())
+    assert a == b

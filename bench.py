@@ -35,6 +35,8 @@ for sub in ("sop-gpu_b200", "oracle"):
 
 import numpy as np  # noqa: E402
 
+from sopb_workloads import batch_config, batch_specs, capsid_spec, hi_spec, plain_params, plain_spec  # noqa: E402,F401
+
 METRIC = "bead-steps/s (batched ragged 512-replica stream)"
 UNIT = "bead-steps/s"
 
@@ -46,51 +48,6 @@ def log(*a):
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
-def plain_params(defaults=None, **kw):
-    """Parameters of the bench workloads over the reference defaults, from
-    `defaults` (the library's sopb.default_params unless given: the CPU arm
-    passes the oracle's own table so that it loads no product library)."""
-    import sopb
-    base = dict(timestep=0.08, zeta=50.0, temperature=0.6, pairs_freq=10, pairlist_cutoff=20.0, pairs_cutoff=20.0,
-                pairs_threshold=200.0, nav=1000)
-    base.update(kw)
-    return (defaults or sopb.default_params)(**base)
-
-
-def batch_specs(count=512, lo=60, hi=600, seed=2024, rank=0, defaults=None):
-    """The ragged force-clamp batch (one independent copy per rank)."""
-    import sopb
-    import sopb_synth as S
-    base = seed + 7919 * rank
-    sizes = S.lognormal_sizes(count, lo, hi, base)
-    rng = np.random.default_rng(base + 1)
-    f_pn = rng.uniform(100.0, 300.0, count)
-    specs = []
-    for k, n in enumerate(sizes):
-        n = int(n)
-        s = S.make_system(n, base * 1000 + k)
-        p = plain_params(defaults, pulling=1, fconst=float(f_pn[k] / 70.0), fixedEnd=0, pulledEnd=n - 1)
-        specs.append(sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[n - 1], seed=1119727 + k))
-    return specs
-
-
-def plain_spec(seed=2024):
-    """One 200-bead force-ramp pull: first bead fixed, last pulled."""
-    import sopb
-    import sopb_synth as S
-    s = S.make_system(200, seed)
-    p = plain_params(pulling=1, deltax=0.5, k_trans=0.05, pullFreq=1000, fixedEnd=0, pulledEnd=199)
-    return sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[199], seed=1119727)
-
-
-def batch_config(specs, chunk, world):
-    """The `config` object of the batch512 line, shared by both arms."""
-    return {"workload": "batch512_lognormal_60-600_clamp", "replicas": len(specs),
-            "beads": int(sum(sp.n for sp in specs)), "langevin_steps_per_step": chunk, "pairs_freq": 10,
-            "pairlist_cutoff_A": 20.0, "dt_tauH": 0.08, "parallelism": "replicas-dp%d" % world,
-            "l2": "flushed between timed steps"}
-
-
 def list_stats(jobs, specs):
     """Mean per-bead list lengths (for the algorithmic-bytes model)."""
     tot = nb = nn = npl = npp = 0
@@ -414,27 +371,6 @@ def run_gpu(args):
     return 0
 
 
-def capsid_spec():
-    """The 198k-bead shell (180 copies of an 1100-bead chain, icosahedral
-    60 x 3 placement), nanoindented by a 10 nm tip on a ramped cantilever
-    against an attractive substrate; cell-list pairlist."""
-    import sopb
-    import sopb_synth as S
-    s, info = S.make_capsid()
-    x = s.xyz.astype(np.float64)
-    c = x.mean(axis=0)
-    tipR = 100.0
-    tip = [float(c[0]), float(x[:, 1].max() + tipR + 4.0), float(c[2])]
-    p = plain_params(pairs_threshold=40.0, max_possiblePairs=2048, max_pairs=512, possiblepairs_freq=100000,
-                     indentation=1, indentationTipR=tipR, indentationKs=0.07, indentationDeltaX=0.012,
-                     indentationTip=tip, indentationChip=tip, indentationDirection=[0.0, -1.0, 0.0],
-                     indentationSurfaceR0=[0.0, float(x[:, 1].min() - 10.0), 0.0],
-                     indentationSurfaceN=[0.0, 1.0, 0.0], indentationTipZeta=5000.0,
-                     indentationSurfA=1.0, indentationSurfB=-2.0, indentationSurfSigma=10.0, indentationSurfEl=0.2,
-                     indentationFixTrans=1, nav=100)
-    return sopb.JobSpec.from_system(s, p, seed=5032015), info
-
-
 def run_capsid(args):
     """Large-assembly workload: one 198k-bead job on the grid path."""
     import torch
@@ -498,19 +434,6 @@ def run_capsid(args):
     print(json.dumps(out), flush=True)
     ctx.close()
     return 0
-
-
-def hi_spec(n, exact, refresh=10, seed=4000):
-    """The HI configuration: one n-bead globule (the plain configuration's
-    generator and force-ramp pull), RPY radius 3.8 A; exact (Cholesky factor
-    refreshed every `refresh` steps) or TEA (epsilon every 10 steps)."""
-    import sopb
-    import sopb_synth as S
-    s = S.make_system(n, seed)
-    p = plain_params(pulling=1, deltax=0.5, k_trans=0.05, pullFreq=1000, fixedEnd=0, pulledEnd=n - 1,
-                     hi_on=1, hi_a=3.8, hi_exact=1 if exact else 0, hi_refresh=refresh, hi_epsilon_freq=10,
-                     hi_capricious=0, max_possiblePairs=4096)
-    return sopb.JobSpec.from_system(s, p, fixed=[0], pulled=[n - 1], seed=1119727)
 
 
 def factor_error(job, ctx, spec):

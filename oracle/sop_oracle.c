@@ -1134,6 +1134,8 @@ static void chol_D(orc_job* j, int assemble) {
     const int32_t n = j->n, m = 3 * n;
     float* M = j->tensor;
     float* nm = (float*)malloc(16 * (size_t)n);
+    /* bead i writes block column i of M and its own sum: no sharing */
+#pragma omp parallel for schedule(static) if (n > 512)
     for (int32_t i = 0; i < n; i++) {
         const float* xi = F4(j->x, i);
         float f[4];
@@ -1175,26 +1177,63 @@ static void chol_D(orc_job* j, int assemble) {
 }
 
 /* integrateCholesky_decompose (src/Integrators/bdhitea_kernel.cu:154-190):
- * column by column; afterwards M holds L below and L^T above the diagonal. */
+ * column by column; afterwards M holds L below and L^T above the diagonal.
+ * Column c starts from row c of M (D[c][t] for t >= c, and L[c][k] for
+ * k < c written by the earlier columns), subtracts L[t][k] * L[c][k] for
+ * k = 0, 1, ..., c-1 in that order, and divides by sqrtf of the diagonal.
+ *
+ * The columns are taken in panels of ORC_CHOL_PANEL: the subtractions of
+ * the columns finished before a panel are applied to all of its columns
+ * while each row k of M is in cache (OpenMP over t), then the panel's own
+ * columns are finished one after the other.  Every entry still sees its
+ * subtractions in increasing k, one rounding each (no contraction), so the
+ * result is bit-identical to the column-at-a-time loop. */
+#define ORC_CHOL_PANEL 64
 void orc_cholesky_ref(int32_t m, float* M) {
-    float* row = (float*)malloc(sizeof(float) * m);
-    float* val = (float*)malloc(sizeof(float) * m);
-    for (int32_t c = 0; c < m; c++) {
-        for (int32_t t = 0; t < m; t++) row[t] = M[(size_t)c * m + t];
-        for (int32_t t = 0; t < m; t++) {
-            float v = row[t];
-            if (t >= c) for (int32_t k = 0; k < c; k++) v -= M[(size_t)k * m + t] * row[k];
-            val[t] = v;
+    const int32_t P = ORC_CHOL_PANEL;
+    float* V = (float*)malloc(sizeof(float) * (size_t)P * m);   /* V[(c - c0) * m + t] */
+    for (int32_t c0 = 0; c0 < m; c0 += P) {
+        const int32_t c1 = c0 + P < m ? c0 + P : m, w = c1 - c0;
+        /* the panel's rows of D and the columns finished before it */
+#pragma omp parallel for schedule(static)
+        for (int32_t tb = c0; tb < m; tb += 256) {
+            const int32_t te = tb + 256 < m ? tb + 256 : m;
+            for (int32_t c = c0; c < c1; c++)
+                for (int32_t t = tb; t < te; t++) V[(size_t)(c - c0) * m + t] = M[(size_t)c * m + t];
+            for (int32_t k = 0; k < c0; k++) {
+                const float* Mk = &M[(size_t)k * m];
+                for (int32_t c = c0; c < c1; c++) {
+                    const float lck = M[(size_t)c * m + k];
+                    float* v = &V[(size_t)(c - c0) * m];
+                    const int32_t t0 = tb > c ? tb : c;
+#pragma omp simd
+                    for (int32_t t = t0; t < te; t++) v[t] -= Mk[t] * lck;
+                }
+            }
         }
-        float diag = sqrtf(val[c]);
-        for (int32_t t = c; t < m; t++) {
-            float v = val[t] / diag;
-            M[(size_t)t * m + c] = v;
-            M[(size_t)c * m + t] = v;
+        /* the panel's own columns, in order */
+        for (int32_t c = c0; c < c1; c++) {
+            float* v = &V[(size_t)(c - c0) * m];
+#pragma omp parallel for schedule(static) if (m - c > 2048)
+            for (int32_t tb = c; tb < m; tb += 512) {
+                const int32_t te = tb + 512 < m ? tb + 512 : m;
+                for (int32_t k = c0; k < c; k++) {
+                    const float* Mk = &M[(size_t)k * m];
+                    const float lck = M[(size_t)c * m + k];
+#pragma omp simd
+                    for (int32_t t = tb; t < te; t++) v[t] -= Mk[t] * lck;
+                }
+            }
+            const float diag = sqrtf(v[c]);
+            for (int32_t t = c; t < m; t++) {
+                const float q = v[t] / diag;
+                M[(size_t)t * m + c] = q;
+                M[(size_t)c * m + t] = q;
+            }
         }
+        (void)w;
     }
-    free(row);
-    free(val);
+    free(V);
 }
 
 /* integrateCholesky_L (src/Integrators/bdhitea_kernel.cu:303-361): block

@@ -250,6 +250,16 @@ int sopb_context_destroy(sopb_context* ctx);
  * src/gsop.cuh:13). */
 int sopb_context_set_shape_policy(sopb_context* ctx, int32_t lanes_per_bead, float beads_per_group, int32_t max_block);
 
+/* Launch policy of grid-path HI jobs created from now on: the width of the
+ * exact-HI factorisation's outer panels, in 128-column tiles (default 4:
+ * each trailing tile is updated once per 512 columns), and the CTAs per SM
+ * that the O(N^2) TEA and D F sums are sliced for (default 4).  Both change
+ * only the order of floating-point sums; a job keeps the policy it was
+ * created with.  The autotuner's knob for HI jobs; no reference counterpart
+ * (the reference factorises unblocked, one CTA per trajectory,
+ * src/Integrators/bdhitea_kernel.cu:154-190). */
+int sopb_context_set_hi_policy(sopb_context* ctx, int32_t chol_panel_tiles, int32_t hi_ctas_per_sm);
+
 /* Blocks until the context's stream and the streams its jobs last ran on
  * drain. */
 int sopb_context_sync(sopb_context* ctx);

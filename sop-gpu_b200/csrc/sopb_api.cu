@@ -1,5 +1,7 @@
 // sopb_api.cu — the C ABI: device context, job construction and the batched
 // launch of the resident Langevin step kernel.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -8,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -80,6 +83,10 @@ struct ShapePolicy {
     int32_t lpb = 4;
     float beads_per_group = 1.0f;
     int32_t max_block = 1024;
+    // grid-path HI jobs: outer-panel width of the exact-HI factorisation (tile
+    // columns) and the CTAs per SM the O(N^2) sums are sliced for
+    int32_t chol_panel_tiles = kCholPanelTiles;
+    int32_t hi_ctas_per_sm = 4;
 };
 
 struct LaunchClass {
@@ -179,9 +186,13 @@ struct sopb_job {
     // its first step (kDue* bits)
     std::map<int, cudaGraphExec_t> chunks;
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
-    cudaStream_t la = nullptr;         // exact HI: the factorisation's second stream
-    cudaEvent_t la_fork = nullptr, la_join = nullptr;
+    cudaStream_t la = nullptr;         // exact HI: the trailing updates (lowest priority)
+    cudaStream_t hp = nullptr;         // exact HI: the panel chain (highest priority)
+    cudaEvent_t la_fork = nullptr, la_join = nullptr, hp_fork = nullptr, hp_join = nullptr;
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
+    int chol_w = kCholPanelTiles;      // exact HI: outer-panel width of the factorisation, tile columns
+    CUtensorMap tmap_ten{};            // exact HI: TMA maps of the tensor and of the diagonal tile's
+    CUtensorMap tmap_linv{};           //   inverse (128 x 32 FP32 boxes, 128-byte swizzle)
     uint32_t log_tail = 0;             // event-log rows drained so far
     bool ev_lazy = false;              // ev not yet recorded after the work on st (see job_ev)
 };
@@ -454,8 +465,8 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
         (rc = set_smem_attr<1024>(device, dm, &ss[4])))
         return rc;
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
-    CUDA_TRY(cudaFuncSetAttribute(k_chol_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholTrsmSmem));
-    CUDA_TRY(cudaFuncSetAttribute(k_chol_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_potrf64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrfSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_apply_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kCholMaxBeads * 12));
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
     *out = c;
@@ -472,8 +483,8 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
             for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
             if (j->la) {
                 cudaStreamDestroy(j->la);
-                cudaEventDestroy(j->la_fork);
-                cudaEventDestroy(j->la_join);
+                cudaStreamDestroy(j->hp);
+                for (cudaEvent_t e : {j->la_fork, j->la_join, j->hp_fork, j->hp_join}) cudaEventDestroy(e);
             }
             if (j->amem) cudaFree(j->amem);
             cudaFree(j->dmem);
@@ -516,6 +527,14 @@ extern "C" int sopb_context_set_shape_policy(sopb_context* c, int32_t lanes_per_
     c->policy.lpb = lanes_per_bead;
     c->policy.beads_per_group = beads_per_group;
     c->policy.max_block = max_block;
+    return SOPB_OK;
+}
+
+extern "C" int sopb_context_set_hi_policy(sopb_context* c, int32_t chol_panel_tiles, int32_t hi_ctas_per_sm) {
+    if (!c || chol_panel_tiles < 1 || chol_panel_tiles > 64 || hi_ctas_per_sm < 1 || hi_ctas_per_sm > 64)
+        return SOPB_ERR_INVALID;
+    c->policy.chol_panel_tiles = chol_panel_tiles;
+    c->policy.hi_ctas_per_sm = hi_ctas_per_sm;
     return SOPB_OK;
 }
 
@@ -631,6 +650,41 @@ void build_maps(const sopb_job_desc* d, HostMaps& m) {
 
 namespace {
 
+// Driver entry points the library calls through the runtime's table, so it
+// needs no link against libcuda (it loads on machines without a driver).
+template <typename Fn>
+Fn driver_fn(const char* name, Fn* cache) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!*cache) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion(name, &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            *cache = reinterpret_cast<Fn>(f);
+        else
+            cudaGetLastError();
+    }
+    return *cache;
+}
+
+// TMA map of a row-major FP32 matrix (rows x cols, leading dimension ld,
+// 16-byte aligned base): 128-row x 32-column boxes, 128-byte swizzle, zero
+// fill outside the matrix.  No multicast anywhere.
+int encode_tmap_f32(CUtensorMap* map, float* base, int rows, int cols, int ld) {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!driver_fn("cuTensorMapEncodeTiled", &fn)) return SOPB_ERR_CUDA;
+    if (((uintptr_t)base & 15) || (ld * sizeof(float)) % 16) return SOPB_ERR_INVALID;
+    const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)kTcKC, (cuuint32_t)kCT};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? SOPB_OK : SOPB_ERR_CUDA;
+}
+
 // Byte layout of a grid job's own buffer block: force partials, the HI
 // buffers and the exact-HI tensor, the cell-list arrays and the near list.
 // grid_alloc carves the block by these offsets and sopb_job_footprint adds
@@ -638,12 +692,12 @@ namespace {
 struct GridLayout {
     int npart = 0, jsplit = 1, cap_nr = 0, ld = 0;
     bool cells = false, hi = false, exact = false, blocked = false;
-    size_t part = 0, rf = 0, mf = 0, xc = 0, ci = 0, eps = 0, ten = 0, geo = 0;
+    size_t part = 0, rf = 0, mf = 0, xc = 0, ci = 0, eps = 0, ten = 0, linv = 0, geo = 0;
     size_t cc = 0, cs = 0, cb = 0, bc = 0, near = 0, nrj = 0, nrc = 0, xref = 0;
     size_t total = 0;
 };
 
-GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl) {
+GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl, int hi_cps = 4) {
     GridLayout L;
     L.npart = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)sms * 8);
     L.cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
@@ -652,7 +706,7 @@ GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp,
     L.blocked = L.exact && n > 128;
     const int64_t itiles = (n + kHiTile - 1) / kHiTile;
     if ((L.hi && !p.hi_exact && p.hi_unlisted) || L.blocked)
-        L.jsplit = (int)std::max<int64_t>(1, std::min<int64_t>((4 * (int64_t)sms + itiles - 1) / itiles, itiles));
+        L.jsplit = (int)std::max<int64_t>(1, std::min<int64_t>((hi_cps * (int64_t)sms + itiles - 1) / itiles, itiles));
     size_t off = 0;
     auto take = [&](size_t bytes) { const size_t o = off; off += align256(bytes); return o; };
     L.part = take(std::max<size_t>(2 * (size_t)L.npart, L.hi ? (size_t)L.jsplit * n : 0) * sizeof(float4));
@@ -665,6 +719,7 @@ GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp,
         if (L.exact) {
             L.ld = L.blocked ? chol_ld((int)n) : (int)(3 * n);
             L.ten = take((size_t)3 * n * L.ld * 4);
+            if (L.blocked) L.linv = take((size_t)kCT * kCT * 4);
         }
     }
     L.geo = take(8 * sizeof(float));
@@ -689,9 +744,10 @@ GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp,
 // pool), reduction partials and, for large jobs, the cell list.
 int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, int32_t cap_pp, int32_t cap_pl) {
     GridAux& a = j->aux;
-    const GridLayout L = grid_layout(p, n, c->sm_count, cap_pp, cap_pl);
+    const GridLayout L = grid_layout(p, n, c->sm_count, cap_pp, cap_pl, c->policy.hi_ctas_per_sm);
     j->bead_blocks = L.npart;
     j->jsplit = L.jsplit;
+    j->chol_w = c->policy.chol_panel_tiles;
     a.npart = L.npart;
     a.use_cells = L.cells;
     a.cap_nr = L.cap_nr;
@@ -711,9 +767,16 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, in
         a.eps = (float*)(b + L.eps);
         if (L.exact) a.tensor = (float*)(b + L.ten);
         if (L.blocked) {
-            CUDA_TRY(cudaStreamCreateWithFlags(&j->la, cudaStreamNonBlocking));
-            CUDA_TRY(cudaEventCreateWithFlags(&j->la_fork, cudaEventDisableTiming));
-            CUDA_TRY(cudaEventCreateWithFlags(&j->la_join, cudaEventDisableTiming));
+            const int m = 3 * n;
+            a.linv = (float*)(b + L.linv);
+            SOPB_TRY(encode_tmap_f32(&j->tmap_ten, a.tensor, m, m, a.ld));
+            SOPB_TRY(encode_tmap_f32(&j->tmap_linv, a.linv, kCT, kCT, kCT));
+            int lo = 0, hi = 0;
+            CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            CUDA_TRY(cudaStreamCreateWithPriority(&j->la, cudaStreamNonBlocking, lo));
+            CUDA_TRY(cudaStreamCreateWithPriority(&j->hp, cudaStreamNonBlocking, hi));
+            for (cudaEvent_t* e : {&j->la_fork, &j->la_join, &j->hp_fork, &j->hp_join})
+                CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
         }
     }
     a.cell_geo = (float*)(b + L.geo);
@@ -760,34 +823,56 @@ int grid_possible(sopb_job* j, JobDev* Jp, cudaStream_t st, int force) {
 
 // Updaters of a stride boundary (each gated on the device step), then
 // `steps` Langevin steps, then the step counter moves by `steps`.
-// Exact HI of a job above 128 beads: assemble D and factorise it in place,
-// the panel kernels one panel ahead on the job's look-ahead stream pair.
+// Exact HI of a job above 128 beads: assemble D and factorise it in place in
+// 128 x 128 tiles, outer panel by outer panel (chol_w tile columns each).
+// The panel chain runs on the job's highest-priority stream: inside an outer
+// panel, each tile column is brought up to date from the panel's earlier
+// columns (one long-K tensor-core pass per tile), its diagonal tile is
+// factorised in FP64 with the inverse of its factor, and the tiles below are
+// solved as a tensor-core product; then the trailing update of the next outer
+// panel's tile columns (K = this panel's columns).  The rest of the trailing
+// update runs on the lowest-priority stream beside the next outer panel's
+// chain, and the chain waits for it before it touches columns that rest
+// updated.  The caller's stream waits for both at the end.
 int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     GridAux& a = j->aux;
-    const int n = j->n, m = 3 * n, sms = j->ctx->sm_count;
-    auto panel = [&](int k) {
-        k_chol_potrf<<<1, kPotrfThreads, 0, st>>>(Jp, a, k);
-        const int rows = m - (k + kCholNB);
-        if (rows > 0)
-            k_chol_trsm<<<std::min((rows + 8 * kTrsmRows - 1) / (8 * kTrsmRows), 2 * sms), 256, kCholTrsmSmem, st>>>(
-                Jp, a, k);
+    const int n = j->n, m = 3 * n, T = chol_tiles(m), W = std::max(1, j->chol_w);
+    auto update = [&](cudaStream_t s, int jc0, int jc1, int k0, int k1) {
+        int tiles = 0;
+        for (int J = jc0; J < jc1; ++J) tiles += T - J;
+        if (tiles > 0 && k1 > k0)
+            k_chol_tc<<<tiles, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_ten, Jp, a, jc0, k0, k1, kTcUpdate);
     };
-    k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, st>>>(Jp, a);
-    panel(0);
-    for (int k = 0; k + kCholNB < m; k += kCholNB) {
-        const int t0 = k + kCholNB, rows = m - t0;
-        const int t = (rows + kTcTile - 1) / kTcTile;
-        // the first tile column (the next panels) on the critical path
-        k_chol_syrk_tc<<<t, kTcThreads, kTcSmem, st>>>(Jp, a, k, 1);
-        if (t > 1) {
-            CUDA_TRY(cudaEventRecord(j->la_fork, st));
-            CUDA_TRY(cudaStreamWaitEvent(j->la, j->la_fork, 0));
-            k_chol_syrk_tc<<<t * (t - 1) / 2, kTcThreads, kTcSmem, j->la>>>(Jp, a, k, 2);
-            CUDA_TRY(cudaEventRecord(j->la_join, j->la));
+    cudaStream_t hp = j->hp, la = j->la;
+    CUDA_TRY(cudaEventRecord(j->hp_fork, st));
+    CUDA_TRY(cudaStreamWaitEvent(hp, j->hp_fork, 0));
+    k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, hp>>>(Jp, a);
+    bool rest_pending = false;   // a rest update on `la` that the next part must follow
+    for (int P0 = 0; P0 < T; P0 += W) {
+        const int P1 = std::min(T, P0 + W);
+        for (int J = P0; J < P1; ++J) {
+            update(hp, J, J + 1, P0 * kCT, J * kCT);
+            k_chol_potrf64<<<1, kPotrfThreads, kPotrfSmem, hp>>>(Jp, a, J);
+            if (J + 1 < T)   // the tiles below: L_IJ = A_IJ X^T on the tensor cores
+                k_chol_tc<<<T - J - 1, kTcThreads, kTcSmem, hp>>>(j->tmap_ten, j->tmap_linv, Jp, a, J, J * kCT,
+                                                                    (J + 1) * kCT, kTcSolve);
         }
-        panel(t0);
-        if (t > 1) CUDA_TRY(cudaStreamWaitEvent(st, j->la_join, 0));
+        if (P1 < T) {
+            const int Q1 = std::min(T, P1 + W);
+            CUDA_TRY(cudaEventRecord(j->la_fork, hp));                       // this outer panel is final
+            if (rest_pending) CUDA_TRY(cudaStreamWaitEvent(hp, j->la_join, 0));
+            update(hp, P1, Q1, P0 * kCT, P1 * kCT);                         // the next outer panel's columns
+            if (Q1 < T) {
+                CUDA_TRY(cudaStreamWaitEvent(la, j->la_fork, 0));
+                update(la, Q1, T, P0 * kCT, P1 * kCT);                      // the rest, beside the chain
+                CUDA_TRY(cudaEventRecord(j->la_join, la));
+                rest_pending = true;
+            }
+        }
     }
+    CUDA_TRY(cudaEventRecord(j->hp_join, hp));
+    CUDA_TRY(cudaStreamWaitEvent(st, j->hp_join, 0));
+    if (rest_pending) CUDA_TRY(cudaStreamWaitEvent(st, j->la_join, 0));
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
@@ -903,7 +988,7 @@ int grid_run(sopb_job* j, cudaStream_t st, int64_t nsteps) {
             cudaError_t e = cudaStreamEndCapture(cap, &g);
             if (rc) return rc;
             CUDA_TRY(e);
-            CUDA_TRY(cudaGraphInstantiate(&ge, g, 0));
+            CUDA_TRY(cudaGraphInstantiate(&ge, g, cudaGraphInstantiateFlagUseNodePriority));
             cudaGraphDestroy(g);
         }
         CUDA_TRY(cudaGraphLaunch(ge, st));
@@ -1355,8 +1440,8 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
     if (j->la) {   // released by the runtime once its work is done
         cudaStreamDestroy(j->la);
-        cudaEventDestroy(j->la_fork);
-        cudaEventDestroy(j->la_join);
+        cudaStreamDestroy(j->hp);
+        for (cudaEvent_t e : {j->la_fork, j->la_join, j->hp_fork, j->hp_join}) cudaEventDestroy(e);
     }
     SOPB_TRY(job_ev(j));
     CUDA_TRY(cudaStreamWaitEvent(c->io, j->ev, 0));
@@ -1843,10 +1928,6 @@ extern "C" int sopb_jobs_download_coords(sopb_context* c, sopb_job* const* jobs,
 // process, so a context made with cuCtxCreate, or the new primary context
 // after a cudaDeviceReset, gets its own look-up instead of a stale address.
 // ===========================================================================
-#include <mutex>
-
-#include <cuda.h>
-#include <cudaTypedefs.h>
 
 namespace {
 

@@ -6,18 +6,25 @@
 // limits it to n <= 128 (integrateCholesky_decompose,
 // src/Integrators/bdhitea_kernel.cu:154-190).  Here D is assembled into a
 // row-major matrix with a 32-float aligned leading dimension and factorised
-// in place, lower triangle, by a right-looking blocked algorithm with 64-wide
-// panels:
-//   k_chol_potrf   the 64 x 64 diagonal block, one CTA, in shared memory;
-//   k_chol_trsm    the panel below it, L_ik = A_ik L_kk^-T, a warp per row;
-//   k_chol_syrk_tc the trailing lower triangle, A_ij -= L_ik L_jk^T, in
-//                  128 x 128 output tiles on the tensor cores (tcgen05,
-//                  TF32 split in hi and lo parts for FP32 accuracy).
-// The trailing update does nearly all of the (3n)^3/3 flops.  The panel
-// kernels sit on the critical path, one panel after the other; they run
-// ahead on a second stream: once the first tile column of the update (which
-// holds the next panel) is done, the next panel is factorised and solved
-// while the rest of the update proceeds.
+// in place, lower triangle, in 128 x 128 tiles.  Tile columns are grouped in
+// outer panels of W tile columns (W = 4 by default):
+//   inside an outer panel, tile column J is brought up to date left-looking
+//     (A_IJ -= sum over the panel's earlier columns, one long-K pass per
+//     tile), then its diagonal tile is factorised in FP64 and the tiles
+//     below it are solved;
+//   after the outer panel, the trailing lower triangle is updated once with
+//     K = the panel's 128 W columns: first the next outer panel's tile
+//     columns (the critical path), then the rest on a second stream beside
+//     the next outer panel's own work.
+// Each C tile is read and written once per outer panel instead of once per
+// 64 columns.  The products run on the 5th-generation tensor cores
+// (tcgen05.mma kind::tf32, accumulator in TMEM) in a warp-specialised
+// pipeline: eight warps load 32-column K chunks of both operands, split each
+// FP32 value p into TF32 p_hi = rn(p) and p_lo = rn(p - p_hi), and store
+// them in shared memory (three stages, mbarrier-tracked); one thread issues
+// hi.hi + hi.lo + lo.hi per K step (the lo.lo term is below FP32 rounding),
+// so the products keep FP32 accuracy; the same eight warps then read the
+// accumulator from TMEM and update C in place.
 // The factor is refreshed every `hi_refresh` steps (an updater; 1 = every
 // step, as the reference).  Every step applies it: (L g)_i by a warp per bead
 // over the bead's three rows, D F by the TEA-style tiles, then the move
@@ -25,19 +32,18 @@
 // All reductions run in a fixed order, so results do not depend on scheduling.
 #pragma once
 
+#include <cuda.h>
+
 #include "sopb_hi.cuh"
 
 namespace sopb {
 
-constexpr int kCholNB = 64;      // panel width
-constexpr int kCholCPL = kCholNB / 32;   // panel columns per lane in the panel solve
-constexpr int kCholLdp = kCholNB + 1;
-constexpr int kCholTile = 128;   // trailing-update output tile
-constexpr int kCholKC = 8;       // K columns staged per round
+constexpr int kCT = 128;                 // tile and panel width
+constexpr int kCholPanelTiles = 4;       // default outer-panel width W, in tile columns
 
 __host__ __device__ inline int chol_ld(int n) { return (3 * n + 31) & ~31; }
-constexpr size_t kCholTrsmSmem = (size_t)(kCholNB * kCholLdp + kCholNB) * 4;
-constexpr int kCholMaxBeads = 16384;   // 3n floats of g in shared memory
+__host__ __device__ inline int chol_tiles(int m) { return (m + kCT - 1) / kCT; }
+constexpr int kCholMaxBeads = 16384;     // 3n floats of g in shared memory
 
 // D, lower block triangle: block (i, q), q <= i, at rows 3i.., columns 3q..
 // (integrateCholesky_D, bdhitea_kernel.cu:89-152, from the step's coordinates).
@@ -64,149 +70,225 @@ k_hi_assemble(const JobDev* __restrict__ Jp, GridAux aux) {
     }
 }
 
-// Cholesky of the diagonal block at (k, k), nb <= 64 rows, in shared memory,
-// by 8-wide sub-panels: warp 0 factors the sub-panel (its diagonal 8 x 8 and
-// the rows below; lane l holds rows l, l+32 of it, the pivots and the L
-// entries of the sub-panel's columns travel by shuffles), then the 256
-// threads subtract its product from the trailing lower triangle, eight terms
-// per entry in column order.  Two barriers per sub-panel, 16 in all (the
-// unblocked form it replaced took one barrier of 1024 threads per column).
-// A pivot that is not positive sets the job's status.
-constexpr int kPotrfThreads = 256;
+// Cholesky of the diagonal tile (J, J), nb <= 128 rows, and the inverse of
+// its factor, in FP64 in shared memory, one CTA of 512 threads.
+// Factor, by 8-wide sub-panels: every thread that solves a row factors the
+// sub-panel's 8 x 8 diagonal block in registers (the same arithmetic in each
+// thread, so nothing but a barrier sits between the pivots of a sub-panel;
+// one FP64 rsqrt per pivot gives both L_cc = d rsqrt(d) and 1 / L_cc), solves
+// its row of the sub-panel below the block, and then the 512 threads share the
+// (row, column) pairs of the trailing lower triangle evenly, eight terms per
+// entry in column order.
+// Inverse X = L^-1, by 8-wide block columns, one warp per block column: the
+// diagonal block by forward substitution, then block row after block row
+// S = sum_k L_ik X_kj (two entries per lane) and L_ii X_ij = -S by forward
+// substitution.  X's strict lower triangle is kept transposed in the unused
+// upper triangle of the tile, its diagonal beside it.
+// Out: the factor (FP32) into the tensor's tile, X (FP32, zero above the
+// diagonal and outside nb) into aux.linv for the tile-column solve.  A
+// pivot that is not positive sets the job's status.
+constexpr int kPotrfThreads = 512;
 constexpr int kPotrfW = 8;                    // sub-panel width
-constexpr int kPotrfRows = kCholNB / 32;      // sub-panel rows per lane
+constexpr int kPotrfLd = kCT + 1;             // doubles
+constexpr size_t kPotrfSmem = (size_t)(kCT * kPotrfLd + 2 * kCT) * sizeof(double);
 
-__global__ void __launch_bounds__(kPotrfThreads)
-k_chol_potrf(JobDev* __restrict__ Jp, GridAux aux, int k) {
-    __shared__ float A[kCholNB][kCholLdp];
-    if (Jp->status) return;
-    const int m = 3 * Jp->n, ld = aux.ld, nb = min(kCholNB, m - k);
-    const int tid = threadIdx.x, lane = tid & 31;
-    float* M = aux.tensor + (size_t)k * ld + k;
-    for (int e = tid; e < nb * nb; e += kPotrfThreads) {
-        const int r = e / nb, c = e - r * nb;
-        if (c <= r) A[r][c] = M[(size_t)r * ld + c];
-    }
-    __syncthreads();
-    int bad = 0;
-    for (int c0 = 0; c0 < nb; c0 += kPotrfW) {
-        const int w = min(kPotrfW, nb - c0);
-        if (tid < 32) {
-            // rows c0 + lane + 32 h of the sub-panel
-            float v[kPotrfRows][kPotrfW];
-#pragma unroll
-            for (int h = 0; h < kPotrfRows; ++h) {
-                const int r = c0 + lane + 32 * h;
-#pragma unroll
-                for (int c = 0; c < kPotrfW; ++c) v[h][c] = (r < nb && c < w) ? A[r][c0 + c] : 0.f;
-            }
-#pragma unroll
-            for (int c = 0; c < kPotrfW; ++c) {
-                if (c >= w) break;
-                const float d = __shfl_sync(0xffffffffu, v[0][c], c);
-                if (!(d > 0.f)) bad = 1;
-                const float rsd = rsqrtf(d), sd = sqrtf(d);
-#pragma unroll
-                for (int h = 0; h < kPotrfRows; ++h) {
-                    const int r = lane + 32 * h;   // row within the sub-panel
-                    if (r == c) v[h][c] = sd;
-                    else if (r > c) v[h][c] *= rsd;
-                }
-#pragma unroll
-                for (int t = c + 1; t < kPotrfW; ++t) {
-                    const float lt = __shfl_sync(0xffffffffu, v[0][c], t);   // L of row c0+t, column c
-#pragma unroll
-                    for (int h = 0; h < kPotrfRows; ++h)
-                        if (lane + 32 * h >= t) v[h][t] -= v[h][c] * lt;
-                }
-            }
-#pragma unroll
-            for (int h = 0; h < kPotrfRows; ++h) {
-                const int r = c0 + lane + 32 * h;
-#pragma unroll
-                for (int c = 0; c < kPotrfW; ++c)
-                    if (r < nb && c < w && c0 + c <= r) A[r][c0 + c] = v[h][c];
-            }
-        }
-        __syncthreads();
-        // trailing lower triangle: rows and columns c0 + w .. nb - 1
-        const int t0 = c0 + w, R = nb - t0;
-        for (int e = tid; e < R * R; e += kPotrfThreads) {
-            const int r = t0 + e / R, q = t0 + e % R;
-            if (q > r) continue;
-            float acc = A[r][q];
-#pragma unroll
-            for (int c = 0; c < kPotrfW; ++c)
-                if (c < w) acc -= A[r][c0 + c] * A[q][c0 + c];
-            A[r][q] = acc;
-        }
-        __syncthreads();
-    }
-    for (int e = tid; e < nb * nb; e += kPotrfThreads) {
-        const int r = e / nb, c = e - r * nb;
-        if (c <= r) M[(size_t)r * ld + c] = A[r][c];
-    }
-    if (bad) atomicMax(&Jp->status, SOPB_ERR_HI);
+// 1 / sqrt(d) in FP64 for d > 0: the FP32 estimate refined by two steps of
+// the Newton-Raphson iteration y <- y (3 - d y^2) / 2, each of which roughly
+// squares the relative error (2^-22 -> 2^-44 -> below FP64 rounding).
+__device__ __forceinline__ double rsqrt_nr(double d) {
+    double y = (double)rsqrtf((float)d);
+    y = y * (1.5 - 0.5 * d * y * y);
+    y = y * (1.5 - 0.5 * d * y * y);
+    return y;
 }
 
-// Panel solve below the diagonal block: row r of A[k+nb.., k..k+nb) becomes
-// x with x L_kk^T = a, by forward substitution.  A warp takes four rows at
-// once (independent chains, one shared read of L per column); lane l holds
-// columns l and l+32 of each.  L_kk and its reciprocal diagonal are
-// staged in shared memory once per CTA.
-constexpr int kTrsmRows = 4;
+// rows c0 .. c0 + 7 of the sub-panel's diagonal block, factorised in registers
+__device__ __forceinline__ void diag8_factor(const double* P, int c0, int w, double (&d8)[kPotrfW][kPotrfW],
+                                             double (&rinv)[kPotrfW], int& bad) {
+#pragma unroll
+    for (int i = 0; i < kPotrfW; ++i)
+#pragma unroll
+        for (int jj = 0; jj < kPotrfW; ++jj)
+            d8[i][jj] = (jj <= i && i < w) ? P[(c0 + i) * kPotrfLd + c0 + jj] : (i == jj ? 1.0 : 0.0);
+#pragma unroll
+    for (int c = 0; c < kPotrfW; ++c) {
+        const double piv = d8[c][c];
+        if (c < w && !(piv > 0.0)) bad = 1;
+        const double rs = rsqrt_nr(piv);
+        d8[c][c] = piv * rs;
+        rinv[c] = rs;
+#pragma unroll
+        for (int i = c + 1; i < kPotrfW; ++i) d8[i][c] *= rs;
+#pragma unroll
+        for (int i = c + 1; i < kPotrfW; ++i)
+#pragma unroll
+            for (int jj = c + 1; jj <= i; ++jj) d8[i][jj] -= d8[i][c] * d8[jj][c];
+    }
+}
 
-__global__ void __launch_bounds__(256)
-k_chol_trsm(JobDev* __restrict__ Jp, GridAux aux, int k) {
-    extern __shared__ float L[];   // [kCholNB][kCholLdp] + inverse diagonal
-    if (Jp->status) return;
-    const int m = 3 * Jp->n, ld = aux.ld, nb = min(kCholNB, m - k);
-    const int tid = threadIdx.x, lane = tid & 31;
-    float* dinv = L + kCholNB * kCholLdp;
-    const float* D = aux.tensor + (size_t)k * ld + k;
-    for (int r = tid >> 5; r < nb; r += 8)
-        for (int s = lane; s <= r; s += 32) L[r * kCholLdp + s] = D[(size_t)r * ld + s];
+__global__ void __launch_bounds__(kPotrfThreads)
+k_chol_potrf64(JobDev* __restrict__ Jp, GridAux aux, int J) {
+    extern __shared__ double P64[];   // [kCT][kPotrfLd], the diagonal of X [kCT], 1 / L_cc [kCT]
+    __shared__ int stop;
+    if (threadIdx.x == 0) stop = Jp->status;
     __syncthreads();
-    for (int c = tid; c < nb; c += 256) dinv[c] = 1.0f / L[c * kCholLdp + c];
+    if (stop) return;
+    double* xd = P64 + kCT * kPotrfLd;
+    double* rdiag = xd + kCT;
+    const int m = 3 * Jp->n, ld = aux.ld, k = J * kCT, nb = min(kCT, m - k);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float* M = aux.tensor + (size_t)k * ld + k;
+    for (int r = warp; r < nb; r += kPotrfThreads / 32)
+        for (int c = lane; c <= r; c += 32) P64[r * kPotrfLd + c] = (double)M[(size_t)r * ld + c];
     __syncthreads();
-    const int groups = gridDim.x * 8;
-    for (int r0 = k + nb + (blockIdx.x * 8 + (tid >> 5)) * kTrsmRows; r0 < m; r0 += groups * kTrsmRows) {
-        float a[kTrsmRows][kCholCPL];
+    int bad = 0;
+    // ---- factor ----
+    for (int c0 = 0; c0 < nb; c0 += kPotrfW) {
+        const int w = min(kPotrfW, nb - c0), t0 = c0 + w;
+        const int r = t0 + tid;              // this thread's row of the sub-panel below its block
+        if (tid == 0 || r < nb) {
+            double d8[kPotrfW][kPotrfW], rinv[kPotrfW];
+            diag8_factor(P64, c0, w, d8, rinv, bad);
+            if (tid == 0)
 #pragma unroll
-        for (int q = 0; q < kTrsmRows; ++q)
+                for (int i = 0; i < kPotrfW; ++i) {
 #pragma unroll
-            for (int u = 0; u < kCholCPL; ++u)
-                a[q][u] = (r0 + q < m && lane + 32 * u < nb) ? aux.tensor[(size_t)(r0 + q) * ld + k + lane + 32 * u] : 0.f;
-        for (int c = 0; c < nb; ++c) {
-            const int owner = c & 31, slot = c >> 5;
-            float lc[kCholCPL];
-#pragma unroll
-            for (int u = 0; u < kCholCPL; ++u) {
-                const int cc = lane + 32 * u;
-                lc[u] = (cc > c && cc < nb) ? L[cc * kCholLdp + c] : 0.f;
-            }
-            const float di = dinv[c];
-#pragma unroll
-            for (int q = 0; q < kTrsmRows; ++q) {
-                float mine = a[q][0];
-#pragma unroll
-                for (int u = 1; u < kCholCPL; ++u)
-                    if (slot == u) mine = a[q][u];
-                const float x = __shfl_sync(0xffffffffu, mine, owner) * di;
-#pragma unroll
-                for (int u = 0; u < kCholCPL; ++u) {
-                    if (lane + 32 * u == c) a[q][u] = x;
-                    else a[q][u] -= x * lc[u];
+                    for (int jj = 0; jj <= i; ++jj)
+                        if (i < w) P64[(c0 + i) * kPotrfLd + c0 + jj] = d8[i][jj];
+                    if (i < w) rdiag[c0 + i] = rinv[i];
                 }
+            if (r < nb) {
+                double x[kPotrfW];
+#pragma unroll
+                for (int c = 0; c < kPotrfW; ++c) x[c] = c < w ? P64[r * kPotrfLd + c0 + c] : 0.0;
+#pragma unroll
+                for (int c = 0; c < kPotrfW; ++c) {
+                    double v = x[c];
+#pragma unroll
+                    for (int q = 0; q < c; ++q) v -= x[q] * d8[c][q];
+                    x[c] = v * rinv[c];
+                }
+#pragma unroll
+                for (int c = 0; c < kPotrfW; ++c)
+                    if (c < w) P64[r * kPotrfLd + c0 + c] = x[c];
             }
         }
+        __syncthreads();
+        // trailing lower triangle, rows and columns t0 .. nb - 1: pair p is
+        // (row t0 + a, column t0 + b) with p = a (a + 1) / 2 + b, b <= a
+        const int R = nb - t0, npairs = R * (R + 1) / 2;
+        for (int p = tid; p < npairs; p += kPotrfThreads) {
+            int a = (int)((sqrtf(8.f * (float)p + 1.f) - 1.f) * 0.5f);
+            while ((a + 1) * (a + 2) / 2 <= p) ++a;
+            while (a * (a + 1) / 2 > p) --a;
+            const int rr = t0 + a, q = t0 + (p - a * (a + 1) / 2);
+            double acc = P64[rr * kPotrfLd + q];
 #pragma unroll
-        for (int q = 0; q < kTrsmRows; ++q)
-            if (r0 + q < m)
-#pragma unroll
-                for (int u = 0; u < kCholCPL; ++u)
-                    if (lane + 32 * u < nb) aux.tensor[(size_t)(r0 + q) * ld + k + lane + 32 * u] = a[q][u];
+            for (int c = 0; c < kPotrfW; ++c)
+                if (c < w) acc -= P64[rr * kPotrfLd + c0 + c] * P64[q * kPotrfLd + c0 + c];
+            P64[rr * kPotrfLd + q] = acc;
+        }
+        __syncthreads();
     }
+    // ---- inverse: warp j owns block column j (columns 8 j .. 8 j + 7) ----
+    // X[a][b], a > b, lives at P64[b][a]; X[a][a] at xd[a]
+    const int nblk = (nb + kPotrfW - 1) / kPotrfW;
+    if (warp < nblk) {
+        const int j0 = warp * kPotrfW, wj = min(kPotrfW, nb - j0);
+        // diagonal block: lane c < wj solves L_jj x = e_c (column c of X_jj)
+        if (lane < kPotrfW) {
+            const int c = lane;
+            double x[kPotrfW];
+#pragma unroll
+            for (int r = 0; r < kPotrfW; ++r) {
+                double v = (r == c) ? 1.0 : 0.0;
+#pragma unroll
+                for (int q = 0; q < r; ++q)
+                    if (q >= c) v -= P64[(j0 + r) * kPotrfLd + j0 + q] * x[q];
+                x[r] = (r >= c && r < wj && c < wj) ? v * rdiag[j0 + r] : 0.0;
+            }
+#pragma unroll
+            for (int r = 0; r < kPotrfW; ++r)
+                if (c < wj && r < wj) {
+                    if (r == c) xd[j0 + r] = x[r];
+                    else if (r > c) P64[(j0 + c) * kPotrfLd + j0 + r] = x[r];
+                }
+        }
+        __syncwarp();
+        // block rows below: S = sum_{k = j..i-1} L_ik X_kj, then L_ii X_ij = -S
+        const int er = lane >> 2, ec = 2 * (lane & 3);   // this lane's entries (er, ec), (er, ec + 1) of the block
+        for (int i0 = j0 + kPotrfW; i0 < nb; i0 += kPotrfW) {
+            const int wi = min(kPotrfW, nb - i0);
+            double s0 = 0.0, s1 = 0.0;
+            if (er < wi) {
+                const double* Lr = P64 + (i0 + er) * kPotrfLd;
+                const int c0x = j0 + ec, c1x = c0x + 1;
+                // the diagonal block's rows of X: diagonal, below it (stored transposed), or zero
+                for (int q = j0; q < j0 + wj; ++q) {
+                    const double x0 = q == c0x ? xd[q] : (q > c0x && c0x < j0 + wj ? P64[c0x * kPotrfLd + q] : 0.0);
+                    const double x1 = q == c1x ? xd[q] : (q > c1x && c1x < j0 + wj ? P64[c1x * kPotrfLd + q] : 0.0);
+                    s0 += Lr[q] * x0;
+                    s1 += Lr[q] * x1;
+                }
+                // block rows j+1 .. i-1 of X, below the diagonal: four partial sums each
+                if (c0x < j0 + wj) {
+                    const double* X0 = P64 + c0x * kPotrfLd;
+                    const double* X1 = P64 + c1x * kPotrfLd;
+                    const bool has1 = c1x < j0 + wj;
+                    double a0[4] = {0.0, 0.0, 0.0, 0.0}, a1[4] = {0.0, 0.0, 0.0, 0.0};
+                    int q = j0 + kPotrfW;
+                    for (; q + 4 <= i0; q += 4) {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            a0[u] += Lr[q + u] * X0[q + u];
+                            if (has1) a1[u] += Lr[q + u] * X1[q + u];
+                        }
+                    }
+                    for (; q < i0; ++q) {
+                        a0[0] += Lr[q] * X0[q];
+                        if (has1) a1[0] += Lr[q] * X1[q];
+                    }
+                    s0 += (a0[0] + a0[1]) + (a0[2] + a0[3]);
+                    s1 += (a1[0] + a1[1]) + (a1[2] + a1[3]);
+                }
+            }
+            // stage -S in the block's transposed slots, then solve column by column
+            if (er < wi) {
+                if (ec < wj) P64[(j0 + ec) * kPotrfLd + i0 + er] = -s0;
+                if (ec + 1 < wj) P64[(j0 + ec + 1) * kPotrfLd + i0 + er] = -s1;
+            }
+            __syncwarp();
+            if (lane < wj) {
+                const int c = j0 + lane;
+                double x[kPotrfW];
+#pragma unroll
+                for (int r = 0; r < kPotrfW; ++r) {
+                    if (r < wi) {
+                        double v = P64[c * kPotrfLd + i0 + r];
+#pragma unroll
+                        for (int q = 0; q < r; ++q) v -= P64[(i0 + r) * kPotrfLd + i0 + q] * x[q];
+                        x[r] = v * rdiag[i0 + r];
+                    } else {
+                        x[r] = 0.0;
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kPotrfW; ++r)
+                    if (r < wi) P64[c * kPotrfLd + i0 + r] = x[r];
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int r = warp; r < nb; r += kPotrfThreads / 32)
+        for (int c = lane; c <= r; c += 32) M[(size_t)r * ld + c] = (float)P64[r * kPotrfLd + c];
+    for (int e = tid; e < kCT * kCT; e += kPotrfThreads) {
+        const int r = e >> 7, c = e & (kCT - 1);
+        float v = 0.f;
+        if (r < nb && c < nb) v = r == c ? (float)xd[r] : (r > c ? (float)P64[c * kPotrfLd + r] : 0.f);
+        aux.linv[e] = v;
+    }
+    if (bad) atomicMax(&Jp->status, SOPB_ERR_HI);
 }
 
 // D F tiles: partial sums over one slice of j of D_ij F_j, j != i
@@ -290,31 +372,43 @@ k_chol_apply_rows(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
     (void)m;
 }
 
-}  // namespace sopb
-
-namespace sopb {
-
-// ---- trailing update on the tensor cores (tcgen05, TF32 x3) -----------------
-// A_ij -= P_i P_j^T for one 128 x 128 lower tile, K = the 64 panel columns,
-// on the 5th-generation tensor cores: each FP32 panel value p is split into
-// TF32 p_hi = rn(p) and p_lo = rn(p - p_hi), and P_i P_j^T is accumulated in
-// TMEM as hi.hi + hi.lo + lo.hi (the lo.lo term is below FP32 rounding), so
-// the product keeps FP32 accuracy.  256 threads stage the two 128 x 64
-// operands (hi and lo) into shared memory in the canonical K-major layout
-// without swizzle (8-row x 16-byte core matrices, the 16 K-chunks of a row
-// group 128 B apart, row groups 2048 B apart); one elected thread issues the
-// 24 MMAs (M = N = 128, K = 8 each) and commits them to an mbarrier; the
-// warps read the accumulator from TMEM (warp w: lanes 32 (w mod 4), columns
-// 64 (w / 4) onwards) into shared memory.  The C tile is loaded into
-// registers at the start (16 coalesced float4 loads per thread, in flight
-// while the operands are staged and multiplied) and written back once.
-constexpr int kTcTile = 128;
-constexpr int kTcThreads = 256;
-constexpr int kTcOperandBytes = kTcTile * kCholNB * 4;          // 32 KB
-constexpr int kTcStageLd = kTcTile + 4;                          // accumulator rows in shared memory (float4 aligned)
-constexpr size_t kTcSmem = 4 * (size_t)kTcOperandBytes + 2048;   // + alignment, barrier, TMEM address
+// ---- tile products on the tensor cores (tcgen05, TF32 x3, TMA-fed) ---------
+// One CTA per 128 x 128 output tile.  kTcUpdate: C_IJ -= sum over k in
+// [k0, k1) of P_Ik P_Jk^T for the lower tiles (I, J) of the tile columns
+// jc0, jc0 + 1, ... (I >= J, gridDim.x tiles in column order), P the factor's
+// columns k0..k1, lower entries of diagonal tiles only.  kTcSolve: C_IJ =
+// A_IJ X^T for the tiles below the diagonal tile of column jc0 (I = jc0 + 1 +
+// blockIdx.x), X = L_JJ^-1 from its own tensor map (the tile-column solve as
+// a product).
+// Pipeline over 32-column K chunks, three stages of 64 KB in shared memory:
+//   warp 9 (one thread) loads the chunk of both operands with two TMA tile
+//     loads (128 rows x 32 FP32, 128-byte swizzle) onto the stage's "loaded"
+//     mbarrier;
+//   warps 0-7 split each value p into TF32 p_hi = rn(p), written back in
+//     place, and p_lo = rn(p - p_hi), written beside it in the same swizzled
+//     layout, then arrive on the stage's "converted" mbarrier;
+//   warp 8 (one thread) issues 12 MMAs per chunk (4 K steps of 8; hi.hi into
+//     one of three accumulator banks in turn, hi.lo + lo.hi into a fourth,
+//     so that no bank accumulates a long K: the tensor cores' FP32
+//     accumulation truncates) and commits them to the stage's "empty"
+//     mbarrier, which releases it to the TMA thread; after the last chunk it
+//     commits to the "done" mbarrier.
+// Operands are K-major with 128-byte swizzle (descriptor layout type 2,
+// 8-row groups 1024 B apart).  Every wait is bounded: on expiry the CTA stops
+// loading and issuing, skips its C update and the job reports
+// SOPB_ERR_TIMEOUT.  The epilogue: warp w reads TMEM lanes 32 (w mod 4),
+// columns 64 (w / 4) onwards of every bank, sums the banks in FP32 and
+// updates 32 consecutive entries of one C row.
+enum { kTcUpdate = 0, kTcSolve = 1 };
+constexpr int kTcKC = 32;                                 // K columns per stage (128 B of FP32)
+constexpr int kTcStages = 3;
+constexpr int kTcPart = kCT * kTcKC * 4;                  // 16 KB: one operand's chunk
+constexpr int kTcStage = 4 * kTcPart;                     // A hi, B hi (TMA destinations), A lo, B lo
+constexpr int kTcConverters = 256;                        // warps 0-7
+constexpr int kTcThreads = kTcConverters + 64;            // + warp 8 (MMA) + warp 9 (TMA)
+constexpr size_t kTcSmem = (size_t)kTcStages * kTcStage + 1024 + 256;
 constexpr uint32_t kTcWaitLimit = 1u << 24;
-static_assert(kTcTile * kTcStageLd * 4 <= 4 * kTcOperandBytes, "staged accumulator fits the operand buffers");
+constexpr uint32_t kTcTmemCols = 512;                     // four 128-column accumulator banks
 
 __device__ __forceinline__ uint32_t tf32_rn(float x) {
     uint32_t r;
@@ -322,195 +416,253 @@ __device__ __forceinline__ uint32_t tf32_rn(float x) {
     return r;
 }
 
-__device__ __forceinline__ uint64_t umma_desc_kmajor(uint32_t smem_addr) {
-    // start address >> 4 [0,14); leading byte offset 128 >> 4 [16,30);
-    // stride byte offset 2048 >> 4 [32,46); version 1 [46,48); no swizzle
-    return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)(2048 >> 4) << 32) |
-           ((uint64_t)1 << 46);
+// K-major shared-memory matrix descriptor, 128-byte swizzle: start address
+// >> 4 [0,14), leading byte offset 16 >> 4 [16,30) (unused with swizzle),
+// stride byte offset 1024 >> 4 [32,46) (8-row groups), version 1 [46,48),
+// layout type 2 = SWIZZLE_128B [61,64).  K steps inside the 128-byte row
+// advance the start address.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t smem_addr) {
+    return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
 // kind::tf32, D = F32, A = B = TF32, both K-major, N = 128, M = 128
 constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
 
-// `part`: 0 every lower tile, 1 the first tile column only (it holds the
-// next panels, which the panel kernels need first), 2 the other columns.
-__global__ void __launch_bounds__(kTcThreads, 1)
-k_chol_syrk_tc(JobDev* __restrict__ Jp, GridAux aux, int k, int part) {
-    extern __shared__ __align__(1024) unsigned char tc_smem[];
-    if (Jp->status) return;
-    const int m = 3 * Jp->n, ld = aux.ld, t0 = k + kCholNB;
-    const int b = blockIdx.x;
-    int I, Jt;
-    if (part == 1) {
-        I = b;
-        Jt = 0;
-    } else {
-        I = (int)((sqrtf(8.f * (float)b + 1.f) - 1.f) * 0.5f);
-        while ((I + 1) * (I + 2) / 2 <= b) ++I;
-        while (I * (I + 1) / 2 > b) --I;
-        Jt = b - I * (I + 1) / 2;
-        if (part == 2) {   // lower tiles of the grid without its first column
-            ++I;
-            ++Jt;
-        }
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort_flag) {
+    for (uint32_t it = 0; it < kTcWaitLimit; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (abort_flag && *abort_flag) return false;
     }
-    const int r0 = t0 + I * kTcTile, c0 = t0 + Jt * kTcTile;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    return false;
+}
 
-    // 1024-aligned operand buffers: A hi, A lo, B hi, B lo
+// One TMA tile load (no multicast) of the box at column x, row y into
+// shared memory, completing on mbarrier `bar`.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_b,
+          JobDev* __restrict__ Jp, GridAux aux, int jc0, int k0, int k1, int mode) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ int stop;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) stop = Jp->status;
+    __syncthreads();
+    if (stop) return;
+    const int m = 3 * Jp->n, ld = aux.ld, T = chol_tiles(m);
+    int I, J;
+    if (mode == kTcSolve) {
+        J = jc0;
+        I = jc0 + 1 + blockIdx.x;
+    } else {
+        int b = blockIdx.x;
+        J = jc0;
+        while (J < T - 1 && b >= T - J) {
+            b -= T - J;
+            ++J;
+        }
+        I = J + b;
+    }
+    const int r0 = I * kCT, c0 = J * kCT;
+    // B operand rows and the column of its first chunk
+    const int b_row = mode == kTcSolve ? 0 : c0, b_col = mode == kTcSolve ? 0 : k0;
+    const int nk = (k1 - k0 + kTcKC - 1) / kTcKC;
+
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tc_smem);
     const uint32_t pad = (1024u - (sbase & 1023u)) & 1023u;
     unsigned char* buf = tc_smem + pad;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(buf + 4 * kTcOperandBytes + 16);
     const uint32_t sbuf = sbase + pad;
-    const uint32_t s_mbar = sbuf + 4 * kTcOperandBytes;
+    const uint32_t bars = sbuf + kTcStages * kTcStage;   // loaded[s], converted[s], empty[s], done
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(buf + kTcStages * kTcStage + 8 * (3 * kTcStages + 1));
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    auto loaded = [&](int s) { return bars + 8u * (uint32_t)s; };
+    auto converted = [&](int s) { return bars + 8u * (uint32_t)(kTcStages + s); };
+    auto empty = [&](int s) { return bars + 8u * (uint32_t)(2 * kTcStages + s); };
+    const uint32_t done_bar = bars + 8u * (uint32_t)(3 * kTcStages);
 
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbuf + 4 * kTcOperandBytes + 16),
-                     "r"(128));
+    if (warp == 8) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         (uint32_t)__cvta_generic_to_shared(tmem_slot)),
+                     "r"(kTcTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s_mbar), "r"(1));
+        for (int s = 0; s < kTcStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(loaded(s)), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(converted(s)), "r"(kTcConverters));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty(s)), "r"(1));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(done_bar), "r"(1));
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-
-    // the C tile: thread (warp w, lane l) holds rows w + 8 i, columns 4 l .. 4 l + 3
-    float4 cv[kTcTile / 8];
-#pragma unroll
-    for (int i = 0; i < kTcTile / 8; ++i) {
-        const int gr = r0 + warp + 8 * i, gcol = c0 + 4 * lane;
-        // gcol and ld are multiples of 4: gcol < m keeps the float4 inside the row
-        cv[i] = (gr < m && gcol < m) ? *reinterpret_cast<const float4*>(aux.tensor + (size_t)gr * ld + gcol)
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    // stage the operands: lane = r + 8 cc covers 8 rows x 4 chunks of 16 B;
-    // all of a thread's loads are issued before the conversions
-    const float* P = aux.tensor + k;
-    const int r = lane & 7, cc = lane >> 3;
-    constexpr int kPer = 16 * 4 / (kTcThreads / 32);   // (row group, chunk quad) items per warp
-#pragma unroll
-    for (int op = 0; op < 2; ++op) {
-        const int row0 = op == 0 ? r0 : c0;
-        unsigned char* hi = buf + (2 * op) * kTcOperandBytes;
-        unsigned char* lo = hi + kTcOperandBytes;
-        float4 v[kPer];
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int it = warp + u * (kTcThreads / 32);
-            const int g = it >> 2, q = it & 3;
-            const int gr = row0 + 8 * g + r;
-            v[u] = gr < m ? *reinterpret_cast<const float4*>(P + (size_t)gr * ld + 4 * (4 * q + cc))
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int it = warp + u * (kTcThreads / 32);
-            const int g = it >> 2, q = it & 3;
-            const uint32_t h0 = tf32_rn(v[u].x), h1 = tf32_rn(v[u].y), h2 = tf32_rn(v[u].z), h3 = tf32_rn(v[u].w);
-            const uint32_t l0 = tf32_rn(v[u].x - __uint_as_float(h0)), l1 = tf32_rn(v[u].y - __uint_as_float(h1)),
-                           l2 = tf32_rn(v[u].z - __uint_as_float(h2)), l3 = tf32_rn(v[u].w - __uint_as_float(h3));
-            const int off = g * 2048 + (4 * q + cc) * 128 + r * 16;
-            *reinterpret_cast<uint4*>(hi + off) = make_uint4(h0, h1, h2, h3);
-            *reinterpret_cast<uint4*>(lo + off) = make_uint4(l0, l1, l2, l3);
-        }
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    if (tid == 0) {
-        const uint32_t a_hi = sbuf, a_lo = sbuf + kTcOperandBytes, b_hi = sbuf + 2 * kTcOperandBytes,
-                       b_lo = sbuf + 3 * kTcOperandBytes;
-        const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-        for (int s = 0; s < kCholNB / 8; ++s) {
-            const uint32_t step = 256u * (uint32_t)s;    // two 16-byte K chunks per K = 8
-            const uint64_t da[3] = {umma_desc_kmajor(a_hi + step), umma_desc_kmajor(a_hi + step),
-                                    umma_desc_kmajor(a_lo + step)};
-            const uint64_t db[3] = {umma_desc_kmajor(b_hi + step), umma_desc_kmajor(b_lo + step),
-                                    umma_desc_kmajor(b_hi + step)};
-            for (int t = 0; t < 3; ++t) {
-                const uint32_t acc = (s > 0 || t > 0) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                    "l"(da[t]), "l"(db[t]), "r"(kTcIdesc), "r"(acc), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+    if (warp == 9) {
+        if (lane == 0) {
+            for (int c = 0; c < nk; ++c) {
+                const int s = c % kTcStages, round = c / kTcStages;
+                if (round > 0 && !mbar_wait(empty(s), (uint32_t)((round - 1) & 1), abort_flag)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                const uint32_t st = sbuf + s * kTcStage;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(loaded(s)),
+                             "r"(2 * kTcPart)
+                             : "memory");
+                tma_load_2d(st, &tmap_a, k0 + c * kTcKC, r0, loaded(s));
+                tma_load_2d(st + kTcPart, &tmap_b, b_col + c * kTcKC, b_row, loaded(s));
             }
         }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s_mbar)
-                     : "memory");
+    } else if (warp == 8) {
+        if (lane == 0) {
+            for (int c = 0; c < nk; ++c) {
+                const int s = c % kTcStages, round = c / kTcStages;
+                if (!mbar_wait(converted(s), (uint32_t)(round & 1), abort_flag)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t a_hi = sbuf + s * kTcStage, b_hi = a_hi + kTcPart, a_lo = a_hi + 2 * kTcPart,
+                               b_lo = a_hi + 3 * kTcPart;
+                const uint32_t d_hh = tmem + 128u * (uint32_t)(c % 3), d_x = tmem + 384u;
+                for (int ks = 0; ks < kTcKC / 8; ++ks) {
+                    const uint32_t kb = 32u * (uint32_t)ks;   // 8 TF32 = 32 bytes of each row
+                    const uint64_t da[3] = {umma_desc_sw128(a_hi + kb), umma_desc_sw128(a_hi + kb),
+                                            umma_desc_sw128(a_lo + kb)};
+                    const uint64_t db[3] = {umma_desc_sw128(b_hi + kb), umma_desc_sw128(b_lo + kb),
+                                            umma_desc_sw128(b_hi + kb)};
+#pragma unroll
+                    for (int t = 0; t < 3; ++t) {
+                        const uint32_t dacc = t == 0 ? d_hh : d_x;
+                        const uint32_t acc = t == 0 ? (c >= 3 || ks > 0 ? 1u : 0u) : (c > 0 || ks > 0 || t > 1 ? 1u : 0u);
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(dacc),
+                            "l"(da[t]), "l"(db[t]), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(empty(s))
+                             : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(done_bar)
+                         : "memory");
+        }
+    } else {
+        // converters: item u of thread tid covers row 8 g + r, 16-byte chunk q
+        // (swizzled position q ^ r); lanes r = 0..7 of one chunk hit eight banks
+        for (int c = 0; c < nk; ++c) {
+            const int s = c % kTcStages, round = c / kTcStages;
+            if (!mbar_wait(loaded(s), (uint32_t)(round & 1), abort_flag)) {
+                *abort_flag = 1;
+                break;
+            }
+            unsigned char* st = buf + s * kTcStage;
+#pragma unroll
+            for (int u = 0; u < kCT * kTcKC / 4 / kTcConverters; ++u) {
+                const int idx = tid + kTcConverters * u;
+                const int r = idx & 7, q = (idx >> 3) & 7, g = idx >> 6;
+                const int off = (8 * g + r) * 128 + ((q ^ r) << 4);
+#pragma unroll
+                for (int op = 0; op < 2; ++op) {
+                    unsigned char* hi = st + op * kTcPart + off;
+                    const float4 v = *reinterpret_cast<const float4*>(hi);
+                    const uint32_t h0 = tf32_rn(v.x), h1 = tf32_rn(v.y), h2 = tf32_rn(v.z), h3 = tf32_rn(v.w);
+                    const uint32_t l0 = tf32_rn(v.x - __uint_as_float(h0)), l1 = tf32_rn(v.y - __uint_as_float(h1)),
+                                   l2 = tf32_rn(v.z - __uint_as_float(h2)), l3 = tf32_rn(v.w - __uint_as_float(h3));
+                    *reinterpret_cast<uint4*>(hi) = make_uint4(h0, h1, h2, h3);
+                    *reinterpret_cast<uint4*>(hi + 2 * kTcPart) = make_uint4(l0, l1, l2, l3);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(converted(s)) : "memory");
+        }
     }
-    // wait for the MMAs (bounded; on expiry the tile is skipped and the job
-    // reports SOPB_ERR_TIMEOUT)
-    uint32_t done = 0;
-    for (uint32_t it = 0; it < kTcWaitLimit && !done; ++it) {
-        asm volatile(
-            "{\n\t.reg .pred P1;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, P1;\n\t}\n"
-            : "=r"(done)
-            : "r"(s_mbar), "r"(0u)
-            : "memory");
-    }
-    // one verdict for the whole CTA, so the warp-wide TMEM reads below run
-    // in every lane or in none
-    done = __syncthreads_and((int)done) ? 1u : 0u;
+    // epilogue: wait for the MMAs (every thread, bounded), then update C
+    const bool done = mbar_wait(done_bar, 0u, nullptr);
+    const bool ok = __syncthreads_and(done && !*abort_flag) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // accumulator -> shared memory (the A operands are no longer read)
-    float* acc_s = reinterpret_cast<float*>(buf);
-    if (done) {
-        const int lrow = 32 * (warp & 3) + lane;       // TMEM lane = tile row
+    if (ok && warp < 8) {
+        const int hh = nk < 3 ? nk : 3;
+        const int lrow = 32 * (warp & 3) + lane, gr = r0 + lrow;
+        const int cmax = mode == kTcSolve ? min(m, c0 + kCT) : m;
         for (int ch = 0; ch < 2; ++ch) {
             const int col = 64 * (warp >> 2) + 32 * ch;
-            uint32_t v[32];
-            const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)col;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float sum[32];
+            for (int bq = 0; bq <= hh; ++bq) {
+                const int bk = bq < hh ? bq : 3;   // the cross-term bank last
+                uint32_t v[32];
+                const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 * bk + col);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int e = 0; e < 32; e += 4)
-                *reinterpret_cast<float4*>(acc_s + lrow * kTcStageLd + col + e) =
-                    make_float4(__uint_as_float(v[e]), __uint_as_float(v[e + 1]), __uint_as_float(v[e + 2]),
-                                __uint_as_float(v[e + 3]));
+                for (int e = 0; e < 32; ++e) sum[e] = bq == 0 ? __uint_as_float(v[e]) : sum[e] + __uint_as_float(v[e]);
+            }
+            if (gr < m) {
+                const int gc = c0 + col;
+                float* dst = aux.tensor + (size_t)gr * ld + gc;
+                if (mode == kTcSolve) {
+#pragma unroll
+                    for (int e = 0; e < 32; e += 4) {
+                        if (gc + e + 3 < cmax) {
+                            *reinterpret_cast<float4*>(dst + e) = make_float4(sum[e], sum[e + 1], sum[e + 2], sum[e + 3]);
+                        } else {
+#pragma unroll
+                            for (int w = 0; w < 4; ++w)
+                                if (gc + e + w < cmax) dst[e + w] = sum[e + w];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 32; e += 4) {
+                        if (gc + e + 3 <= gr && gc + e + 3 < m) {
+                            float4 x = *reinterpret_cast<float4*>(dst + e);
+                            x.x -= sum[e];
+                            x.y -= sum[e + 1];
+                            x.z -= sum[e + 2];
+                            x.w -= sum[e + 3];
+                            *reinterpret_cast<float4*>(dst + e) = x;
+                        } else {
+#pragma unroll
+                            for (int w = 0; w < 4; ++w)
+                                if (gc + e + w <= gr && gc + e + w < m) dst[e + w] -= sum[e + w];
+                        }
+                    }
+                }
+            }
         }
-    } else if (tid == 0) {
-        Jp->status = SOPB_ERR_TIMEOUT;
     }
+    if (!ok && tid == 0) atomicMax(&Jp->status, SOPB_ERR_TIMEOUT);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
-    if (!done) return;
-    // C tile update from the registers, lower entries only
-    const int gc = c0 + 4 * lane;
-#pragma unroll
-    for (int i = 0; i < kTcTile / 8; ++i) {
-        const int R = warp + 8 * i, gr = r0 + R;
-        if (gr >= m) continue;
-        const float4 a = *reinterpret_cast<const float4*>(acc_s + R * kTcStageLd + 4 * lane);
-        float4 x = cv[i];
-        x.x -= a.x;
-        x.y -= a.y;
-        x.z -= a.z;
-        x.w -= a.w;
-        float* dst = aux.tensor + (size_t)gr * ld + gc;
-        if (gc + 3 <= gr && gc + 3 < m) {
-            *reinterpret_cast<float4*>(dst) = x;
-        } else {
-            const float xs[4] = {x.x, x.y, x.z, x.w};
-            for (int w = 0; w < 4; ++w)
-                if (gc + w <= gr && gc + w < m) dst[w] = xs[w];
-        }
-    }
+    if (warp == 8) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols));
 }
 
 }  // namespace sopb

@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
             "sopb_context_destroy": ([vp], C.c_int),
             "sopb_context_sync": ([vp], C.c_int),
             "sopb_context_set_shape_policy": ([vp, i32, C.c_float, i32], C.c_int),
+            "sopb_context_set_hi_policy": ([vp, i32, i32], C.c_int),
             "sopb_job_footprint": ([vp, vp], C.c_int),
             "sopb_job_create": ([vp, vp, vp], C.c_int),
             "sopb_job_destroy": ([vp], C.c_int),
@@ -339,6 +340,13 @@ class Context:
         """Resident-kernel shape for jobs created from now on (autotuner knob)."""
         check(lib().sopb_context_set_shape_policy(self.handle, int(lanes_per_bead), float(beads_per_group),
                                                   int(max_block)), "set_shape_policy")
+
+    def set_hi_policy(self, chol_panel_tiles: int = 4, hi_ctas_per_sm: int = 4) -> None:
+        """HI launch policy for jobs created from now on (autotuner knob):
+        exact-HI outer-panel width in 128-column tiles, and the CTAs per SM
+        the O(N^2) HI sums are sliced for."""
+        check(lib().sopb_context_set_hi_policy(self.handle, int(chol_panel_tiles), int(hi_ctas_per_sm)),
+              "set_hi_policy")
 
     def upload_coords(self, jobs: Sequence[Job], xyzw: np.ndarray) -> None:
         arr = self._handles(jobs)

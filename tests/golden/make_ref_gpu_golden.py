@@ -32,7 +32,8 @@ def main():
     if pack_only:
         args = args[1:]
     out = os.path.abspath(args[0] if args else "refgold")
-    names = args[1:] or [c for c in ref_cases.CASES if not ref_cases.CASES[c].get("speed")]
+    names = args[1:] or [c for c in ref_cases.CASES
+                         if not ref_cases.CASES[c].get("speed") and not ref_cases.CASES[c].get("longrun")]
     for name in names:
         c = ref_cases.CASES[name]
         d = os.path.join(out, name)

@@ -122,6 +122,16 @@ CASES = {
         "indentationSurfaceN": "0.0 1.0 0.0", "indentationTipZeta": "5000", "indentationSurfA": "1.0",
         "indentationSurfB": "-2.0", "indentationSurfSigma": "10.0", "indentationSurfEl": "0.2",
         "indentationFixTrans": "yes"}),
+    # long-run statistics: 256 runs of the plain 200-bead force-ramp pull for
+    # 1e5 steps (cantilever 1.4 A per 200 steps, 700 A in all), pulling lines
+    # every 200 steps and .dat lines every 1000; made by
+    # make_ref_longrun_golden.py, compared by tests/test_gpu_longrun.py
+    "longpull": dict(n=200, sys_seed=2024, runs=256, total=100000, dumps=[], longrun=True, cfg={
+        "runnum": "256", "firstrun": "1", "seed": "1119726", "nav": "1000", "max_pairs": "256",
+        "max_possiblePairs": "256", "pulling": "on", "deltax": "1.4", "k_trans": "0.05", "pullFreq": "200",
+        "fixed": "0", "pulled": "199", "fixedEnd": "0", "pulledEnd": "199", "pullDirection": "endToEnd",
+        "pullOutput": "<name>_<run>_pull.dat", "outputtiming": "1000", "dcdfreq": "100000000",
+        "restartfreq": "100000000"}),
     "heat": dict(n=100, sys_seed=6, runs=1, total=45, dumps=[45], cfg={
         "run": "1", "seed": "5", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
         "heating": "on", "initialT": "0.1", "deltaT": "0.2", "tempFreq": "10"}),

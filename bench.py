@@ -71,18 +71,37 @@ def alg_bytes_per_bead_step(st, pairs_freq):
             + (4 * st["n_possible"] + 4 * st["n_pair"]) / pairs_freq)
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) that ncu measured
-# over every launch of one bench step, per bead-step, for the bench's own
-# command lines: batch512 (--policy 4,1,1024), 200 Langevin steps per step
-# over three launch classes; the values scale with the bead-steps of a step.
-NCU_DRAM_BYTES_PER_BEAD_STEP = {
-    "batch512": (71.892736e6 + 18.4832e6 + 5.900544e6 + 0.024064e6 + 0.466432e6 + 0.002048e6) / (113612 * 200),
-}
+# Figures of ncu captures of the shipped kernels (profiles/ncu_figures.json):
+# DRAM bytes per bead-step and SM-side counters per workload, each recorded
+# with a hash of the CUDA sources it was captured from.  A figure whose hash
+# no longer matches the sources is stale and not reported.
+FIGURES = os.path.join(REPO, "profiles", "ncu_figures.json")
+
+
+def source_hash():
+    import hashlib
+    h = hashlib.sha256()
+    d = os.path.join(REPO, "sop-gpu_b200", "csrc")
+    for f in sorted(os.listdir(d)):
+        if f.endswith((".cu", ".cuh", ".cpp", ".h")):
+            h.update(f.encode())
+            with open(os.path.join(d, f), "rb") as fh:
+                h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def ncu_figures(workload):
+    try:
+        with open(FIGURES) as f:
+            e = json.load(f).get(workload)
+    except (OSError, ValueError):
+        return None
+    return e if e and e.get("source_sha") == source_hash() else None
 
 
 def traffic_per_step(workload, bead_steps):
-    b = NCU_DRAM_BYTES_PER_BEAD_STEP.get(workload)
-    return None if b is None else b * bead_steps
+    e = ncu_figures(workload)
+    return None if e is None else e["dram_bytes_per_bead_step"] * bead_steps
 
 
 def peaks():
@@ -217,6 +236,27 @@ def reduce_over_ranks(dist, bead_steps, seconds, device):
     return float(s[0].item()), float(t[1].item())
 
 
+def roofline_batch(achieved, peak, peak_kind, bps, stats, bead_steps):
+    """The batch512 roofline entry: the reference data model's bytes against
+    the HBM peak (frac), the DRAM traffic an ncu capture of the shipped
+    kernel measured, and what limits the kernel per that capture: the SM
+    (issue slots and shared-memory wavefronts), not HBM."""
+    fig = ncu_figures("batch512")
+    r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+         "traffic": traffic_per_step("batch512", bead_steps),
+         "traffic_scope": "DRAM bytes of one bench step (all launch classes), ncu capture of the shipped kernel",
+         "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats}
+    if fig:
+        r["limiter"] = "sm"
+        r["sm_side"] = {k: fig[k] for k in ("issue_active_pct", "shared_wavefronts_per_bead_step",
+                                            "shared_bank_conflict_frac", "warps_active_pct") if k in fig}
+        r["ncu_capture"] = {"date": fig.get("date"), "source_sha": fig.get("source_sha")}
+    else:
+        r["limiter"] = None
+        r["traffic_note"] = "no ncu capture of the current kernel sources in profiles/ncu_figures.json"
+    return r
+
+
 def run_gpu(args):
     import torch
     import sopb
@@ -246,7 +286,7 @@ def run_gpu(args):
     elif args.autotune:
         import sopb_autotune
         t0 = time.perf_counter()
-        tuned = sopb_autotune.autotune(ctx, specs, steps=100, log=log if rank == 0 else None)
+        tuned = sopb_autotune.autotune(ctx, specs, steps=1000, log=log if rank == 0 else None)
         log("rank %d: autotuned shape policy %s in %.1fs" % (rank, tuned["policy"], time.perf_counter() - t0))
     jobs = [ctx.job(sp) for sp in specs]
     beads = sum(sp.n for sp in specs)
@@ -354,15 +394,19 @@ def run_gpu(args):
             "shape_policy": None if tuned is None else {"lanes_per_bead": tuned["policy"][0],
                                                         "beads_per_group": tuned["policy"][1],
                                                         "max_block": tuned["policy"][2]},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic_per_step("batch512", beads * chunk),
-                         "traffic_scope": "DRAM bytes of one bench step (all launch classes), ncu",
-                         "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats},
+            "roofline": roofline_batch(achieved, peak, peak_kind, bps, stats, beads * chunk),
             "plain": plain,
             "batched_over_plain": value / plain["value"] if plain else None,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }
+    if rank == 0 and world == 1 and not args.batch_only:
+        # compact lines of the other single-GPU workloads: the 198k-bead
+        # capsid indentation and exact HI / TEA at 4000 beads
+        ctx.sync()
+        out["capsid"] = measure_capsid(dev, 3, 1, chunk, None if args.no_cpu else args.ref_seconds)
+        out["hi"] = measure_hi(dev, 4000, 2, 1, 10)
+    if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
     if dist:
@@ -371,33 +415,54 @@ def run_gpu(args):
     return 0
 
 
-def run_capsid(args):
-    """Large-assembly workload: one 198k-bead job on the grid path."""
+def capsid_cpu_rate(target_s=10.0):
+    """The oracle on a bounded sample of the capsid workload: the 18 000-bead
+    shell of 180 copies of a 100-bead chain (same lattice, indentation and
+    cell-list parameters), one job, one thread."""
+    import oracle_py as O
+    sp, _ = capsid_spec(copies_per_unit=3, chain_n=100, cell_list=1)
+    o = O.OracleJob(sp)
+    t0 = time.perf_counter()
+    o.advance(10)                                  # includes the step-0 list builds
+    probe = time.perf_counter() - t0
+    steps = max(10, min(2000, int(target_s / max(probe / 10, 1e-9))))
+    t0 = time.perf_counter()
+    o.advance(steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": sp.n * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "CPU restatement, one job: the 18000-bead shell (180 copies of a 100-bead chain) x %d steps" % steps}
+
+
+def measure_capsid(dev, steps, warmup, chunk, cpu_seconds=None, copies_per_unit=3, chain_n=1100):
+    """The 198k-bead capsid indentation job on the grid path: device-timed
+    bead-steps/s (L2 flushed between timed steps), end to end through the C
+    ABI with host buffers, the roofline against HBM, clocks."""
     import torch
     import sopb
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
     ctx = sopb.Context(dev, stream=stream.cuda_stream)
     t0 = time.perf_counter()
-    spec, info = capsid_spec()
-    log("capsid: generated %d beads in %.1fs (%s)" % (spec.n, time.perf_counter() - t0, info))
+    spec, info = capsid_spec(copies_per_unit=copies_per_unit, chain_n=chain_n,
+                             cell_list=1 if copies_per_unit * 60 * chain_n <= 16384 else 0)
+    log("capsid: generated %d beads in %.1fs (shell radius %.1f A)" % (spec.n, time.perf_counter() - t0,
+                                                                       info["radius_A"]))
     job = ctx.job(spec)
-    chunk = args.chunk
     with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             ctx.run([job], chunk)
     ctx.sync()
     if job.status() != 0:
         raise RuntimeError("capsid job failed in warm-up: status %d" % job.status())
     stats = list_stats([job], [spec])
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
         with torch.cuda.stream(stream):
-            for k in range(args.steps):
+            for k in range(steps):
                 flush.fill_(float(k))
                 starts[k].record(stream)
                 ctx.run([job], chunk)
@@ -406,33 +471,50 @@ def run_capsid(args):
     total_ms = sum(s_.elapsed_time(e) for s_, e in zip(starts, ends))
     if job.status() != 0:
         raise RuntimeError("capsid job failed: status %d" % job.status())
-    value = spec.n * chunk * args.steps / (total_ms / 1e3)
+    value = spec.n * chunk * steps / (total_ms / 1e3)
     host = torch.empty((spec.n, 4), dtype=torch.float32, pin_memory=True).numpy()
     ctx.download_coords([job], host)
     t0 = time.perf_counter()
-    for k in range(args.steps):
+    for k in range(steps):
         ctx.upload_coords([job], host)
         ctx.run([job], chunk)
         ctx.download_coords([job], host)
     torch.cuda.synchronize()
-    e2e = spec.n * chunk * args.steps / (time.perf_counter() - t0)
+    e2e = spec.n * chunk * steps / (time.perf_counter() - t0)
     peak, peak_kind = peaks()
     bps = alg_bytes_per_bead_step(stats, 10)
-    achieved = bps * spec.n * chunk / ((total_ms / 1e3) / args.steps) / 1e9
-    out = {"metric": "bead-steps/s (198k-bead capsid indentation)", "value": value, "unit": UNIT, "n_gpus": 1,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-           "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded shell of chain copies)",
-           "config": {"workload": "capsid198k_indentation", "beads": spec.n, "langevin_steps_per_step": chunk,
-                      "pairs_threshold_A": 40.0, "pairlist": "cell list, every 10 steps", "shell": info,
+    achieved = bps * spec.n * chunk / ((total_ms / 1e3) / steps) / 1e9
+    traffic = traffic_per_step("capsid198k", spec.n * chunk)
+    out = {"workload": "capsid198k_indentation", "value": value, "unit": UNIT, "steps": steps, "warmup": warmup,
+           "ms_per_step": total_ms / steps,
+           "config": {"beads": spec.n, "langevin_steps_per_step": chunk, "pairs_threshold_A": 40.0,
+                      "pairlist": "cell list, every 10 steps", "shell_radius_A": info["radius_A"],
+                      "copies": info["copies"], "chain_n": info["chain_n"], "inter_natives": info["inter_natives"],
                       "l2": "flushed between timed steps"},
            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": spec.n * 16, "d2h_bytes_per_step": spec.n * 16},
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                        "traffic": traffic_per_step("capsid", spec.n * chunk),
-                        "traffic_scope": "DRAM bytes of one bench step (every launch of the step), ncu",
+                        "traffic": traffic,
+                        "traffic_scope": "DRAM bytes of one bench step (every launch of the step), scaled from an "
+                                         "ncu capture of the 18000-bead shell by bead-steps",
                         "peak_kind": peak_kind, "alg_bytes_per_bead_step": bps, "lists": stats},
            "tip": job.read(sopb.TIPSTATE)[:11].tolist(), "clocks": clk.summary()}
-    print(json.dumps(out), flush=True)
     ctx.close()
+    if cpu_seconds:
+        out["cpu_baseline"] = capsid_cpu_rate(cpu_seconds)
+    return out
+
+
+def run_capsid(args):
+    """Large-assembly workload: one 198k-bead job on the grid path."""
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    r = measure_capsid(dev, args.steps, args.warmup, args.chunk, None if args.no_cpu else args.ref_seconds,
+                       args.capsid_copies, args.capsid_chain)
+    out = {"metric": "bead-steps/s (198k-bead capsid indentation)", "value": r["value"], "unit": UNIT,
+           "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+           "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded shell of chain copies)",
+           "config": dict(r["config"], workload="capsid198k_indentation"), "e2e": r["e2e"],
+           "roofline": r["roofline"], "tip": r["tip"], "clocks": r["clocks"], "cpu_baseline": r.get("cpu_baseline")}
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -468,35 +550,45 @@ def factor_error(job, ctx, spec):
     return err
 
 
-def run_hi(args):
-    """HI workload: one 4000-bead job with exact hydrodynamics (blocked
-    Cholesky of the 12 000 x 12 000 tensor, refreshed every 10 steps) and the
-    same job with TEA, on the grid path."""
+def tf32_peak():
+    """TF32 dense tensor peak: half the measured BF16 GEMM burst (TF32 runs at
+    half the BF16 rate on B200), else half the fallback."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"]) / 2.0, "measured bf16 burst / 2"
+    return 1590.0 / 2.0, "fallback bf16 / 2"
+
+
+def measure_hi(dev, n, steps, warmup, chunk, check_factor=True):
+    """One n-bead globule with exact HI (blocked Cholesky of the 3n x 3n
+    tensor, refreshed every 10 steps) and with TEA, on the grid path.  The
+    exact path's roofline counts the (3n)^3/3 useful flops of a refresh
+    against the TF32 tensor peak (the TF32 x3 split issues three times as
+    many)."""
     import torch
-    import sopb
-    dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
+    import sopb
     ctx = sopb.Context(dev, stream=stream.cuda_stream)
-    n = args.hi_beads
-    chunk = args.chunk
     res = {}
     clocks = None
+    e2e = None
     for kind in ("exact", "tea"):
         spec = hi_spec(n, kind == "exact")
         job = ctx.job(spec)
         with torch.cuda.stream(stream):
-            for _ in range(args.warmup):
+            for _ in range(warmup):
                 ctx.run([job], chunk)
         ctx.sync()
         if job.status() != 0:
             raise RuntimeError("hi %s job failed in warm-up: status %d" % (kind, job.status()))
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
         torch.cuda.synchronize()
         with ClockSampler(dev) as clk:
             with torch.cuda.stream(stream):
-                for k in range(args.steps):
+                for k in range(steps):
                     starts[k].record(stream)
                     ctx.run([job], chunk)
                     ends[k].record(stream)
@@ -504,45 +596,66 @@ def run_hi(args):
         total_ms = sum(s_.elapsed_time(e) for s_, e in zip(starts, ends))
         if job.status() != 0:
             raise RuntimeError("hi %s job failed: status %d" % (kind, job.status()))
-        res[kind] = {"value": n * chunk * args.steps / (total_ms / 1e3), "ms_per_langevin_step": total_ms / (chunk * args.steps)}
+        res[kind] = {"value": n * chunk * steps / (total_ms / 1e3), "ms_per_langevin_step": total_ms / (chunk * steps)}
         if kind == "exact":
             clocks = clk.summary()
             host = torch.empty((n, 4), dtype=torch.float32, pin_memory=True).numpy()
             ctx.download_coords([job], host)
             t0 = time.perf_counter()
-            for k in range(args.steps):
+            for k in range(steps):
                 ctx.upload_coords([job], host)
                 ctx.run([job], chunk)
                 ctx.download_coords([job], host)
             torch.cuda.synchronize()
-            e2e = n * chunk * args.steps / (time.perf_counter() - t0)
-            # land on a refresh boundary, then measure the factor made there
-            left = (-job.step()) % 10
-            if left:
-                ctx.run([job], left)
-            res["exact"]["factor_rel_error_fp64"] = factor_error(job, ctx, spec)
+            e2e = n * chunk * steps / (time.perf_counter() - t0)
+            if check_factor:
+                left = (-job.step()) % 10      # land on a refresh boundary, measure the factor made there
+                if left:
+                    ctx.run([job], left)
+                res["exact"]["factor_rel_error_fp64"] = factor_error(job, ctx, spec)
         job.destroy()
+    ctx.close()
     m = 3 * n
     refresh_flop = m ** 3 / 3.0
-    out = {"metric": "bead-steps/s (exact HI, %d beads)" % n, "value": res["exact"]["value"], "unit": UNIT,
+    peak, peak_kind = tf32_peak()
+    # refreshes every 10 steps: the useful factorisation flops per Langevin step
+    achieved = refresh_flop / 10.0 / (res["exact"]["ms_per_langevin_step"] / 1e3) / 1e12
+    return {"workload": "hi%d_exact_refresh10" % n, "value": res["exact"]["value"], "unit": UNIT,
+            "steps": steps, "warmup": warmup,
+            "config": {"beads": n, "langevin_steps_per_step": chunk, "hi_a_A": 3.8, "hi_refresh": 10,
+                       "tensor": "%d x %d FP32" % (m, m), "chol_panel_tiles": 4},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": n * 16},
+            "exact": res["exact"], "tea": res["tea"], "flop_per_refresh": refresh_flop,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "note": "useful (3n)^3/3 flops per refresh, one refresh per 10 steps, over the whole step "
+                                 "time (apply and D F included); TF32 x3 issues 3x these"},
+            "clocks": clocks}
+
+
+def run_hi(args):
+    """HI workload: one 4000-bead job with exact hydrodynamics (blocked
+    Cholesky of the 12 000 x 12 000 tensor, refreshed every 10 steps) and the
+    same job with TEA, on the grid path."""
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    r = measure_hi(dev, args.hi_beads, args.steps, args.warmup, args.chunk)
+    out = {"metric": "bead-steps/s (exact HI, %d beads)" % args.hi_beads, "value": r["value"], "unit": UNIT,
            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
-           "data": "synthetic (seeded globule)",
-           "config": {"workload": "hi%d_exact_refresh10" % n, "beads": n, "langevin_steps_per_step": chunk,
-                      "hi_a_A": 3.8, "hi_refresh": 10, "tensor": "%d x %d FP32" % (m, m)},
-           "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": n * 16},
-           "exact": res["exact"], "tea": res["tea"],
-           "flop_per_refresh": refresh_flop,
-           "clocks": clocks}
+           "data": "synthetic (seeded globule)", "config": dict(r["config"], workload=r["workload"]),
+           "e2e": r["e2e"], "exact": r["exact"], "tea": r["tea"], "flop_per_refresh": r["flop_per_refresh"],
+           "roofline": r["roofline"], "clocks": r["clocks"]}
     print(json.dumps(out), flush=True)
-    ctx.close()
     return 0
 
 
 def run_serve(args):
     """Serving workload: a seeded Poisson stream of pulling, clamp and
     indentation jobs (sizes log-normal in [50, 5000], 30% with HI: exact for
-    n <= 1500, TEA above), served by continuous batching; throughput and
-    p50/p99 completion latency, next to each sampled job's time alone."""
+    n <= 1500, TEA above, steps log-uniform in [1e4, 1e5] times
+    --serve-step-scale), served by continuous batching.  Reports the served
+    throughput and p50/p99 completion latency, and the plain path on the same
+    request set: every job alone, one at a time, its rate timed over
+    min(steps, 2000) of its steps and its alone time scaled to its steps."""
     import torch
     import sopb
     import sopb_serve
@@ -551,44 +664,80 @@ def run_serve(args):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
     ctx = sopb.Context(dev)
+    lo_steps, hi_steps = int(1e4 * args.serve_step_scale), int(1e5 * args.serve_step_scale)
     t0 = time.perf_counter()
-    reqs = poisson_stream(args.serve_jobs, args.serve_rate, 2024, steps_lo=int(1e4 * args.serve_step_scale),
-                          steps_hi=int(1e5 * args.serve_step_scale))
+    reqs = poisson_stream(args.serve_jobs, args.serve_rate, 2024, steps_lo=lo_steps, steps_hi=hi_steps)
     log("serve: generated %d requests in %.1fs" % (len(reqs), time.perf_counter() - t0))
-    # warm-up: one small job of each path
-    for r in reqs[:4]:
+    for r in reqs[:4]:                     # warm-up: one small job of each path
         j = ctx.job(r.spec)
         ctx.run([j], 20)
         j.destroy()
     ctx.sync()
     srv = sopb_serve.Server(ctx, quantum=args.serve_quantum)
-    t0 = time.perf_counter()
-    res = srv.serve(reqs)
-    wall = time.perf_counter() - t0
+    with ClockSampler(dev) as clk:
+        t0 = time.perf_counter()
+        res = srv.serve(reqs)
+        wall = time.perf_counter() - t0
     summ = sopb_serve.summarize(res, wall)
-    # the same jobs alone (a sample): latency without the mix
-    alone, slow = [], []
     served = {x.rid: x for x in res}
-    for r in reqs[:: max(1, len(reqs) // 16)]:
+    # the plain path: each job alone
+    alone_s, slow, bead_steps = [], [], 0.0
+    for r in reqs:
         j = ctx.job(r.spec)
+        ctx.run([j], 10)                   # step-0 updaters outside the timed part
         ctx.sync()
+        k = min(r.steps, 2000)
         ta = time.perf_counter()
-        ctx.run([j], r.steps)
+        ctx.run([j], k)
         ctx.sync()
-        alone.append(time.perf_counter() - ta)
-        slow.append(served[r.rid].latency / alone[-1])
+        t_alone = (time.perf_counter() - ta) * r.steps / k
         j.destroy()
+        alone_s.append(t_alone)
+        bead_steps += r.spec.n * r.steps
+        if served[r.rid].status == 0:
+            slow.append(served[r.rid].latency / t_alone)
+    plain = bead_steps / sum(alone_s)
+    by_kind = {}
+    for x in res:
+        by_kind.setdefault(x.kind, []).append(x.latency)
     out = {"metric": "bead-steps/s (served Poisson stream)", "value": summ["throughput"], "unit": UNIT,
            "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
            "config": {"workload": "serve_poisson", "jobs": len(reqs), "rate_per_s": args.serve_rate,
                       "sizes": "lognormal [50, 5000]", "hi_fraction": 0.3,
-                      "steps": "log-uniform [%d, %d]" % (int(1e4 * args.serve_step_scale), int(1e5 * args.serve_step_scale)),
-                      "quantum": args.serve_quantum},
-           "serve": summ, "peak_inflight": srv.peak_inflight,
-           "alone_sample": {"jobs": len(alone), "p50_s": float(np.percentile(alone, 50)),
-                            "p99_s": float(np.percentile(alone, 99)),
-                            "slowdown_p50": float(np.percentile(slow, 50)),
-                            "slowdown_p99": float(np.percentile(slow, 99))}}
+                      "steps": "log-uniform [%d, %d]" % (lo_steps, hi_steps), "quantum": args.serve_quantum},
+           "serve": summ, "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_used,
+           "plain": {"value": plain, "unit": UNIT, "method": "each job alone, one at a time; rate over "
+                                                              "min(steps, 2000) steps scaled to the job's steps",
+                     "total_s": float(sum(alone_s)), "p50_s": float(np.percentile(alone_s, 50)),
+                     "p99_s": float(np.percentile(alone_s, 99))},
+           "served_over_plain": summ["throughput"] / plain,
+           "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)), "p99": float(np.percentile(slow, 99))},
+           "latency_by_kind_p50_s": {k: float(np.percentile(v, 50)) for k, v in sorted(by_kind.items())},
+           "clocks": clk.summary()}
+    print(json.dumps(out), flush=True)
+    ctx.close()
+    return 0
+
+
+def run_autotune(args):
+    """The tuner's tables: the resident shape on the 512-replica batch
+    (1000-step trials, best of two) and the HI policy on the 4000-bead exact
+    and TEA jobs (20-step trials, best of two)."""
+    import torch
+    import sopb
+    import sopb_autotune
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    ctx = sopb.Context(dev)
+    specs = batch_specs()
+    beads = sum(sp.n for sp in specs)
+    r = sopb_autotune.autotune(ctx, specs, steps=args.autotune_steps, log=log)
+    h = sopb_autotune.autotune(ctx, [hi_spec(4000, True), hi_spec(4000, False)], log=log)
+    fmt = lambda t: [{"policy": list(p), "seconds": dt, "bead_steps_per_s": v} for p, dt, v in t]
+    out = {"workload": "autotune", "resident": {"jobs": len(specs), "beads": beads, "steps": args.autotune_steps,
+                                                "best": list(r["policy"]), "table": fmt(r["table"])},
+           "hi": {"jobs": "exact + TEA at 4000 beads", "steps": 20, "best": list(h["hi_policy"]),
+                  "table": fmt(h["hi_table"])}}
     print(json.dumps(out), flush=True)
     ctx.close()
     return 0
@@ -603,14 +752,19 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="the batch512 line without the capsid and HI sub-objects")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the shape policy by short timed runs instead of --policy")
-    ap.add_argument("--workload", default="batch512", choices=["batch512", "serve", "capsid", "hi"])
+    ap.add_argument("--workload", default="batch512", choices=["batch512", "serve", "capsid", "hi", "autotune"])
+    ap.add_argument("--autotune-steps", type=int, default=1000)
     ap.add_argument("--hi-beads", type=int, default=4000)
+    ap.add_argument("--capsid-copies", type=int, default=3, help="copies per icosahedral unit (60 units)")
+    ap.add_argument("--capsid-chain", type=int, default=1100, help="beads per chain copy")
     ap.add_argument("--serve-jobs", type=int, default=200)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-quantum", type=int, default=1000)
-    ap.add_argument("--serve-step-scale", type=float, default=0.1)
+    ap.add_argument("--serve-step-scale", type=float, default=1.0)
     # 4 lanes per bead, one bead per lane group, CTAs of up to 1024 threads:
     # the fastest policy on this workload in full-length runs (the autotuner's
     # 100-step trials cannot separate it from its neighbours reliably)
@@ -624,6 +778,8 @@ def main():
         return run_capsid(args)
     if args.workload == "hi":
         return run_hi(args)
+    if args.workload == "autotune":
+        return run_autotune(args)
     return run_gpu(args)
 
 

@@ -10,19 +10,15 @@ Two kinds of job share the GPU:
   - replica-resident jobs (no HI, up to 2048 beads): one CTA holds a whole
     job, so they run best together, many jobs per launch;
   - grid-path jobs (HI or above 2048 beads): chains of small launches.
-A resident CTA needs an empty SM, which a GPU kept busy by small CTAs
-rarely offers, so the two kinds alternate in phases:
-  - batch phase: every resident job with steps left runs up to
-    `batch_quantum` steps in one ragged launch on the batch stream (each
-    job's CTA stops at its own count), started when no grid quantum is in
-    flight so that its CTAs find empty SMs; grid quanta then fill the SMs it
-    leaves free;
-  - grid phase: grid jobs run quanta of about `slice_us` of device time on
-    `grid_lanes` streams (sopb_run_on), one quantum per lane at a time, the
-    jobs with the least remaining work first; a lane takes the next quantum
-    as soon as its previous one finished.  When resident jobs are waiting
-    and no batch launch runs, no new quanta start, and the next batch launch
-    begins once the running ones drain.
+Resident jobs run in ragged launches of up to `batch_quantum` steps (each
+job's CTA stops at its own count) on a pool of highest-priority streams:
+as soon as resident jobs are waiting and a pool stream is free, they start,
+beside any batch already running, and the block scheduler hands their CTAs
+the next SMs that the short grid-path kernels free.  Grid jobs run quanta of
+about `slice_us` of device time on `grid_lanes` lowest-priority streams
+(sopb_run_on), one quantum per lane at a time, the jobs with the least
+remaining work first; a lane takes the next quantum as soon as its previous
+one finished.
 State stays on the device for a job's whole life, and a job's result does
 not depend on what it shares the GPU with (its launch shape is a function
 of the job alone).
@@ -50,15 +46,16 @@ def on_grid_path(spec: "sopb.JobSpec") -> bool:
 def step_cost(spec: "sopb.JobSpec") -> float:
     """Device time of one step of a grid-path job alone, microseconds, on
     B200 (sizes quanta and orders jobs): a per-step launch chain, all-pairs
-    O(n^2) sums for HI and the amortised O((3n)^3) factorisation for exact
-    HI (fitted to 87 us per TEA step and 3.6 ms per exact step, refresh 10,
-    at 4000 beads), O(n) otherwise."""
+    O(n^2) sums for HI and, for exact HI, the factorisation amortised over
+    its refresh period, whose time is set by the chain of 3n/128 tile
+    columns (fitted to 85 us per TEA step and 2.1 ms per exact step with
+    refresh 10 at 4000 beads, 0.2 ms at 451 beads), O(n) otherwise."""
     p, n = spec.params, float(spec.n)
     if not p.hi_on:
         return 20.0 + 5e-4 * n
     cost = 40.0 + 3e-6 * n * n
     if p.hi_exact:
-        cost += 20.0 + 5.6e-7 * n ** 3 / max(1, int(p.hi_refresh))
+        cost += 5.2 * n / max(1, int(p.hi_refresh))
     return cost
 
 
@@ -91,7 +88,7 @@ class Result:
 class Server:
     def __init__(self, ctx: "sopb.Context", hbm_budget: int = 64 << 30, max_inflight: int = 2048,
                  quantum: int = 1000, keep_coords: bool = False, slice_us: float = 1.0e4, grid_lanes: int = 16,
-                 batch_quantum: int = 2000):
+                 batch_quantum: int = 2000, batch_streams: int = 4):
         import torch
         self.torch = torch
         self.ctx = ctx
@@ -100,13 +97,13 @@ class Server:
         self.quantum = quantum          # upper bound of a grid job's quantum, steps
         self.slice_us = slice_us
         self.keep_coords = keep_coords
-        self.batch_stream = torch.cuda.Stream()
-        self.lanes = [torch.cuda.Stream() for _ in range(grid_lanes)]
+        lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
+        self.batch_streams = [torch.cuda.Stream(priority=hi) for _ in range(batch_streams)]
+        self.lanes = [torch.cuda.Stream(priority=lo) for _ in range(grid_lanes)]
         self.waiting: Deque[Request] = collections.deque()
         self.inflight: Dict[int, dict] = {}
-        self.chain: Deque[tuple] = collections.deque()   # batch phase: (event, finishing rids)
+        self.chain: List[tuple] = []    # running batch launches: (event, stream, rids)
         self.batch_quantum = batch_quantum
-        self.grid_turn = False          # a grid round is due after a batch phase
         self.used = 0
         self.peak_used = 0
         self.peak_inflight = 0
@@ -155,30 +152,36 @@ class Server:
 
     def _poll_chain(self) -> bool:
         moved = False
-        while self.chain and self.chain[0][0].query():
-            _, rids = self.chain.popleft()
-            for rid in rids:
+        for item in [c for c in self.chain if c[0].query()]:
+            self.chain.remove(item)
+            for rid in item[2]:
                 st = self.inflight[rid]
                 if st["done"] >= st["req"].steps:
                     self._retire(rid)
                 else:
-                    st["queued"] = False      # more steps in a later batch phase
+                    st["queued"] = False      # more steps in a later batch launch
             moved = True
         return moved
 
-    def _start_batch(self) -> None:
+    def _start_batch(self) -> bool:
         """Up to `batch_quantum` more steps of every waiting resident job in
-        one ragged launch (sopb_run_ragged: each job its own step count)."""
+        one ragged launch (sopb_run_ragged: each job its own step count) on a
+        free batch stream, beside the batch launches already running."""
         members = [rid for rid, st in self.inflight.items() if not st["grid"] and not st["queued"]]
+        busy = {id(c[1]) for c in self.chain}
+        free = [b for b in self.batch_streams if id(b) not in busy]
+        if not members or not free:
+            return False
+        stream = free[0]
         left = [min(self.batch_quantum, self.inflight[r]["req"].steps - self.inflight[r]["done"]) for r in members]
         for rid, n in zip(members, left):
             self.inflight[rid]["queued"] = True
             self.inflight[rid]["done"] += n
-        self.ctx.run([self.inflight[r]["job"] for r in members], left, stream=self.batch_stream.cuda_stream)
+        self.ctx.run([self.inflight[r]["job"] for r in members], left, stream=stream.cuda_stream)
         ev = self.torch.cuda.Event()
-        ev.record(self.batch_stream)
-        self.chain.append((ev, members))
-        self.grid_turn = True            # grid quanta fill the SMs the batch leaves free
+        ev.record(stream)
+        self.chain.append((ev, stream, members))
+        return True
 
     def _poll_grid(self, launch: bool) -> bool:
         """Retires grid jobs whose last quantum finished; with `launch`, starts
@@ -216,23 +219,13 @@ class Server:
         return moved
 
     def step(self) -> bool:
-        """One pass of the loop: admit, poll, and start whatever may start."""
+        """One pass of the loop: admit, retire what finished, start the
+        resident jobs that wait and the grid quanta that fit the lanes."""
         self._admit()
         moved = self._poll_chain()
-        if self.grid_turn:                   # grid quanta beside the placed batch launch
-            self.grid_turn = False
-            moved |= self._poll_grid(launch=True)
-        if self.chain:                       # batch launch running: keep the lanes busy
-            return self._poll_grid(launch=True) or moved
-        waiting_resident = any(not st["grid"] and not st["queued"] for st in self.inflight.values())
-        if waiting_resident:
-            # drain the grid quanta in flight, then the batch phase
-            moved |= self._poll_grid(launch=False)
-            if all(st["event"] is None for st in self.inflight.values() if st["grid"]):
-                self._start_batch()
-                moved = True
-            return moved
-        return self._poll_grid(launch=True) or moved
+        moved |= self._start_batch()
+        moved |= self._poll_grid(launch=True)
+        return moved
 
     def serve(self, arrivals: List[Request], until_idle: bool = True) -> List[Result]:
         """Replays `arrivals` (sorted by arrival time, seconds) on the real

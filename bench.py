@@ -673,7 +673,7 @@ def run_serve(args):
         ctx.run([j], 20)
         j.destroy()
     ctx.sync()
-    srv = sopb_serve.Server(ctx, quantum=args.serve_quantum)
+    srv = sopb_serve.Server(ctx, quantum=args.serve_quantum, grid_lanes=args.serve_lanes)
     with ClockSampler(dev) as clk:
         t0 = time.perf_counter()
         res = srv.serve(reqs)
@@ -682,7 +682,7 @@ def run_serve(args):
     served = {x.rid: x for x in res}
     # the plain path: each job alone
     alone_s, slow, bead_steps = [], [], 0.0
-    for r in reqs:
+    for r in ([] if args.serve_no_plain else reqs):
         j = ctx.job(r.spec)
         ctx.run([j], 10)                   # step-0 updaters outside the timed part
         ctx.sync()
@@ -696,6 +696,8 @@ def run_serve(args):
         bead_steps += r.spec.n * r.steps
         if served[r.rid].status == 0:
             slow.append(served[r.rid].latency / t_alone)
+    if args.serve_no_plain:
+        alone_s, slow, bead_steps = [float("nan")], [float("nan")], float("nan")
     plain = bead_steps / sum(alone_s)
     by_kind = {}
     for x in res:
@@ -704,7 +706,8 @@ def run_serve(args):
            "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded)",
            "config": {"workload": "serve_poisson", "jobs": len(reqs), "rate_per_s": args.serve_rate,
                       "sizes": "lognormal [50, 5000]", "hi_fraction": 0.3,
-                      "steps": "log-uniform [%d, %d]" % (lo_steps, hi_steps), "quantum": args.serve_quantum},
+                      "steps": "log-uniform [%d, %d]" % (lo_steps, hi_steps), "quantum": args.serve_quantum,
+                      "grid_lanes": args.serve_lanes},
            "serve": summ, "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_used,
            "plain": {"value": plain, "unit": UNIT, "method": "each job alone, one at a time; rate over "
                                                               "min(steps, 2000) steps scaled to the job's steps",
@@ -765,6 +768,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-quantum", type=int, default=1000)
     ap.add_argument("--serve-step-scale", type=float, default=1.0)
+    ap.add_argument("--serve-lanes", type=int, default=16, help="grid-path streams of the serving loop")
+    ap.add_argument("--serve-no-plain", action="store_true", help="skip the one-at-a-time comparison")
     # 4 lanes per bead, one bead per lane group, CTAs of up to 1024 threads:
     # the fastest policy on this workload in full-length runs (the autotuner's
     # 100-step trials cannot separate it from its neighbours reliably)

@@ -186,8 +186,12 @@ struct sopb_job {
     // its first step (kDue* bits)
     std::map<int, cudaGraphExec_t> chunks;
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
-    cudaStream_t la = nullptr;         // exact HI: the trailing updates (lowest priority)
-    cudaStream_t hp = nullptr;         // exact HI: the panel chain (highest priority)
+    // exact HI: streams of the factorisation, one per stream priority level
+    // (created on first use): the panel chain runs one level above the
+    // caller's stream, the trailing updates at the caller's level
+    static constexpr int kPrioLevels = 8;
+    cudaStream_t prio_st[kPrioLevels] = {};
+    bool hi_streams = false;
     cudaEvent_t la_fork = nullptr, la_join = nullptr, hp_fork = nullptr, hp_join = nullptr;
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
     int chol_w = kCholPanelTiles;      // exact HI: outer-panel width of the factorisation, tile columns
@@ -481,9 +485,8 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     for (sopb_job* j : c->slots)
         if (j) {
             for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
-            if (j->la) {
-                cudaStreamDestroy(j->la);
-                cudaStreamDestroy(j->hp);
+            if (j->hi_streams) {
+                for (cudaStream_t q : j->prio_st) if (q) cudaStreamDestroy(q);
                 for (cudaEvent_t e : {j->la_fork, j->la_join, j->hp_fork, j->hp_join}) cudaEventDestroy(e);
             }
             if (j->amem) cudaFree(j->amem);
@@ -771,10 +774,13 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, in
             a.linv = (float*)(b + L.linv);
             SOPB_TRY(encode_tmap_f32(&j->tmap_ten, a.tensor, m, m, a.ld));
             SOPB_TRY(encode_tmap_f32(&j->tmap_linv, a.linv, kCT, kCT, kCT));
+            // one stream per priority level, made here rather than during a
+            // stream capture
+            j->hi_streams = true;
             int lo = 0, hi = 0;
             CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-            CUDA_TRY(cudaStreamCreateWithPriority(&j->la, cudaStreamNonBlocking, lo));
-            CUDA_TRY(cudaStreamCreateWithPriority(&j->hp, cudaStreamNonBlocking, hi));
+            for (int k = 0; k <= std::min(lo - hi, sopb_job::kPrioLevels - 1); ++k)
+                CUDA_TRY(cudaStreamCreateWithPriority(&j->prio_st[k], cudaStreamNonBlocking, lo - k));
             for (cudaEvent_t* e : {&j->la_fork, &j->la_join, &j->hp_fork, &j->hp_join})
                 CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
         }
@@ -825,15 +831,15 @@ int grid_possible(sopb_job* j, JobDev* Jp, cudaStream_t st, int force) {
 // `steps` Langevin steps, then the step counter moves by `steps`.
 // Exact HI of a job above 128 beads: assemble D and factorise it in place in
 // 128 x 128 tiles, outer panel by outer panel (chol_w tile columns each).
-// The panel chain runs on the job's highest-priority stream: inside an outer
+// The panel chain runs one stream priority above the caller's: inside an outer
 // panel, each tile column is brought up to date from the panel's earlier
 // columns (one long-K tensor-core pass per tile), its diagonal tile is
 // factorised in FP64 with the inverse of its factor, and the tiles below are
 // solved as a tensor-core product; then the trailing update of the next outer
 // panel's tile columns (K = this panel's columns).  The rest of the trailing
-// update runs on the lowest-priority stream beside the next outer panel's
-// chain, and the chain waits for it before it touches columns that rest
-// updated.  The caller's stream waits for both at the end.
+// update runs at the caller's priority beside the next outer panel's chain,
+// and the chain waits for it before it touches columns that rest updated.
+// The caller's stream waits for both at the end.
 int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     GridAux& a = j->aux;
     const int n = j->n, m = 3 * n, T = chol_tiles(m), W = std::max(1, j->chol_w);
@@ -843,7 +849,15 @@ int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
         if (tiles > 0 && k1 > k0)
             k_chol_tc<<<tiles, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_ten, Jp, a, jc0, k0, k1, kTcUpdate);
     };
-    cudaStream_t hp = j->hp, la = j->la;
+    // priorities relative to the caller's stream (numerically smaller is
+    // higher): the chain one level above it, the trailing updates at it
+    int lo = 0, hi = 0, p = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    CUDA_TRY(cudaStreamGetPriority(st, &p));
+    p = std::min(lo, std::max(hi, p));
+    auto level = [&](int prio) { return j->prio_st[std::min(sopb_job::kPrioLevels - 1, lo - prio)]; };
+    cudaStream_t hp = level(std::max(hi, p - 1)), la = level(p);
+    if (!hp || !la) return SOPB_ERR_CUDA;
     CUDA_TRY(cudaEventRecord(j->hp_fork, st));
     CUDA_TRY(cudaStreamWaitEvent(hp, j->hp_fork, 0));
     k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, hp>>>(Jp, a);
@@ -1438,9 +1452,8 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     // nothing waits here: graphs and memory are released after the job's
     // last work on its stream, the bead range and slot once it has finished
     for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
-    if (j->la) {   // released by the runtime once its work is done
-        cudaStreamDestroy(j->la);
-        cudaStreamDestroy(j->hp);
+    if (j->hi_streams) {   // released by the runtime once their work is done
+        for (cudaStream_t q : j->prio_st) if (q) cudaStreamDestroy(q);
         for (cudaEvent_t e : {j->la_fork, j->la_join, j->hp_fork, j->hp_join}) cudaEventDestroy(e);
     }
     SOPB_TRY(job_ev(j));

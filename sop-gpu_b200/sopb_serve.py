@@ -16,9 +16,10 @@ as soon as resident jobs are waiting and a pool stream is free, they start,
 beside any batch already running, and the block scheduler hands their CTAs
 the next SMs that the short grid-path kernels free.  Grid jobs run quanta of
 about `slice_us` of device time on `grid_lanes` lowest-priority streams
-(sopb_run_on), one quantum per lane at a time, the jobs with the least
-remaining work first; a lane takes the next quantum as soon as its previous
-one finished.
+(sopb_run_on), one quantum per lane at a time; a lane takes the next quantum
+as soon as its previous one finished.  The jobs with the most work left (they
+set when the stream is done) get the `long_lanes` lanes, one priority level
+above the others; the rest go least remaining work first.
 State stays on the device for a job's whole life, and a job's result does
 not depend on what it shares the GPU with (its launch shape is a function
 of the job alone).
@@ -88,7 +89,7 @@ class Result:
 class Server:
     def __init__(self, ctx: "sopb.Context", hbm_budget: int = 64 << 30, max_inflight: int = 2048,
                  quantum: int = 1000, keep_coords: bool = False, slice_us: float = 1.0e4, grid_lanes: int = 16,
-                 batch_quantum: int = 2000, batch_streams: int = 4):
+                 batch_quantum: int = 2000, batch_streams: int = 4, long_lanes: int = 4):
         import torch
         self.torch = torch
         self.ctx = ctx
@@ -99,7 +100,13 @@ class Server:
         self.keep_coords = keep_coords
         lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
         self.batch_streams = [torch.cuda.Stream(priority=hi) for _ in range(batch_streams)]
-        self.lanes = [torch.cuda.Stream(priority=lo) for _ in range(grid_lanes)]
+        # the first `long_lanes` lanes run one level above the rest and take
+        # the grid jobs with the most work left (they set the makespan); the
+        # library runs an exact-HI factorisation's chain one level above its
+        # lane
+        self.long_lanes = min(long_lanes, grid_lanes)
+        self.lanes = [torch.cuda.Stream(priority=max(hi, lo - 1) if k < self.long_lanes else lo)
+                      for k in range(grid_lanes)]
         self.waiting: Deque[Request] = collections.deque()
         self.inflight: Dict[int, dict] = {}
         self.chain: List[tuple] = []    # running batch launches: (event, stream, rids)
@@ -185,8 +192,9 @@ class Server:
 
     def _poll_grid(self, launch: bool) -> bool:
         """Retires grid jobs whose last quantum finished; with `launch`, starts
-        quanta on free lanes, least remaining work first (a lane runs one
-        quantum at a time, so the GPU holds at most one per lane)."""
+        quanta on free lanes: the jobs with the most work left on the long
+        lanes, the others least work first (a lane runs one quantum at a
+        time, so the GPU holds at most one per lane)."""
         moved = False
         idle = []
         busy = set()
@@ -204,9 +212,16 @@ class Server:
             idle.append(rid)
         if not launch:
             return moved
-        free = [ln for ln in self.lanes if id(ln) not in busy]
-        idle.sort(key=lambda r: (self.inflight[r]["req"].steps - self.inflight[r]["done"]) * self.inflight[r]["cost"])
-        for rid, lane in zip(idle, free):
+        work = lambda r: (self.inflight[r]["req"].steps - self.inflight[r]["done"]) * self.inflight[r]["cost"]
+        # the jobs with the most work left go to free long lanes, the others
+        # (least work first) to free ordinary lanes
+        long_free = [ln for ln in self.lanes[:self.long_lanes] if id(ln) not in busy]
+        rest_free = [ln for ln in self.lanes[self.long_lanes:] if id(ln) not in busy]
+        idle.sort(key=work, reverse=True)
+        pairs = list(zip(idle, long_free))
+        rest = sorted(idle[len(pairs):], key=work)
+        pairs += list(zip(rest, rest_free))
+        for rid, lane in pairs:
             st = self.inflight[rid]
             n = min(st["q"], st["req"].steps - st["done"])
             st["lane"] = lane

@@ -673,7 +673,8 @@ def run_serve(args):
         ctx.run([j], 20)
         j.destroy()
     ctx.sync()
-    srv = sopb_serve.Server(ctx, quantum=args.serve_quantum, grid_lanes=args.serve_lanes)
+    srv = sopb_serve.Server(ctx, quantum=args.serve_quantum, grid_lanes=args.serve_lanes,
+                            slice_us=args.serve_slice_us, long_lanes=args.serve_long_lanes)
     with ClockSampler(dev) as clk:
         t0 = time.perf_counter()
         res = srv.serve(reqs)
@@ -707,7 +708,8 @@ def run_serve(args):
            "config": {"workload": "serve_poisson", "jobs": len(reqs), "rate_per_s": args.serve_rate,
                       "sizes": "lognormal [50, 5000]", "hi_fraction": 0.3,
                       "steps": "log-uniform [%d, %d]" % (lo_steps, hi_steps), "quantum": args.serve_quantum,
-                      "grid_lanes": args.serve_lanes},
+                      "grid_lanes": args.serve_lanes, "slice_us": args.serve_slice_us,
+                      "long_lanes": args.serve_long_lanes},
            "serve": summ, "peak_inflight": srv.peak_inflight, "peak_hbm_bytes": srv.peak_used,
            "plain": {"value": plain, "unit": UNIT, "method": "each job alone, one at a time; rate over "
                                                               "min(steps, 2000) steps scaled to the job's steps",
@@ -716,6 +718,9 @@ def run_serve(args):
            "served_over_plain": summ["throughput"] / plain,
            "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)), "p99": float(np.percentile(slow, 99))},
            "latency_by_kind_p50_s": {k: float(np.percentile(v, 50)) for k, v in sorted(by_kind.items())},
+           "slowest": [{"rid": x.rid, "n": x.n, "kind": x.kind, "steps": x.steps, "latency_s": x.latency,
+                        "queued_s": x.admitted - x.arrival}
+                       for x in sorted(res, key=lambda x: -x.latency)[:5]],
            "clocks": clk.summary()}
     print(json.dumps(out), flush=True)
     ctx.close()
@@ -770,6 +775,8 @@ def main():
     ap.add_argument("--serve-step-scale", type=float, default=1.0)
     ap.add_argument("--serve-lanes", type=int, default=16, help="grid-path streams of the serving loop")
     ap.add_argument("--serve-no-plain", action="store_true", help="skip the one-at-a-time comparison")
+    ap.add_argument("--serve-slice-us", type=float, default=1.0e4, help="device time of a grid quantum")
+    ap.add_argument("--serve-long-lanes", type=int, default=4, help="lanes for the jobs with the most work left")
     # 4 lanes per bead, one bead per lane group, CTAs of up to 1024 threads:
     # the fastest policy on this workload in full-length runs (the autotuner's
     # 100-step trials cannot separate it from its neighbours reliably)

@@ -17,9 +17,11 @@ beside any batch already running, and the block scheduler hands their CTAs
 the next SMs that the short grid-path kernels free.  Grid jobs run quanta of
 about `slice_us` of device time on `grid_lanes` lowest-priority streams
 (sopb_run_on), one quantum per lane at a time; a lane takes the next quantum
-as soon as its previous one finished.  The jobs with the most work left (they
-set when the stream is done) get the `long_lanes` lanes, one priority level
-above the others; the rest go least remaining work first.
+as soon as its previous one finished.  The jobs with the most time left (by
+the measured device time of their last quantum, the cost model before
+that; they set when the stream is done) get the `long_lanes` lanes at the
+greatest priority, one level above the resident batches; the rest go least
+remaining work first.
 State stays on the device for a job's whole life, and a job's result does
 not depend on what it shares the GPU with (its launch shape is a function
 of the job alone).
@@ -99,14 +101,14 @@ class Server:
         self.slice_us = slice_us
         self.keep_coords = keep_coords
         lo, hi = torch.cuda.Stream.priority_range() if hasattr(torch.cuda.Stream, "priority_range") else (0, -1)
-        self.batch_streams = [torch.cuda.Stream(priority=hi) for _ in range(batch_streams)]
-        # the first `long_lanes` lanes run one level above the rest and take
-        # the grid jobs with the most work left (they set the makespan); the
-        # library runs an exact-HI factorisation's chain one level above its
-        # lane
+        # the first `long_lanes` lanes take the grid jobs with the most time
+        # left (they set when the stream is done) at the greatest priority;
+        # resident batches one level below; the other lanes at the least
+        # (the library runs an exact-HI factorisation's chain one level above
+        # its lane where there is one)
+        self.batch_streams = [torch.cuda.Stream(priority=min(lo, hi + 1)) for _ in range(batch_streams)]
         self.long_lanes = min(long_lanes, grid_lanes)
-        self.lanes = [torch.cuda.Stream(priority=max(hi, lo - 1) if k < self.long_lanes else lo)
-                      for k in range(grid_lanes)]
+        self.lanes = [torch.cuda.Stream(priority=hi if k < self.long_lanes else lo) for k in range(grid_lanes)]
         self.waiting: Deque[Request] = collections.deque()
         self.inflight: Dict[int, dict] = {}
         self.chain: List[tuple] = []    # running batch launches: (event, stream, rids)
@@ -139,7 +141,7 @@ class Server:
             self.used += fp
             self.peak_used = max(self.peak_used, self.used)
             st = dict(req=req, job=job, done=0, fp=fp, admitted=self.now(), grid=on_grid_path(req.spec),
-                      event=None, lane=None, q=0, queued=False)
+                      event=None, start=None, qn=0, lane=None, q=0, queued=False, meas=None)
             if st["grid"]:
                 st["cost"] = step_cost(req.spec)
                 q = int(self.slice_us / st["cost"]) // 10 * 10
@@ -192,7 +194,7 @@ class Server:
 
     def _poll_grid(self, launch: bool) -> bool:
         """Retires grid jobs whose last quantum finished; with `launch`, starts
-        quanta on free lanes: the jobs with the most work left on the long
+        quanta on free lanes: the jobs with the most time left on the long
         lanes, the others least work first (a lane runs one quantum at a
         time, so the GPU holds at most one per lane)."""
         moved = False
@@ -204,6 +206,10 @@ class Server:
                 if not st["event"].query():
                     busy.add(id(st["lane"]))
                     continue
+                # measured time per step of this job (device time of its last
+                # quantum on its lane), which ranks the jobs by time left
+                us = st["start"].elapsed_time(st["event"]) * 1e3 / max(1, st["qn"])
+                st["meas"] = us if st["meas"] is None else 0.5 * (st["meas"] + us)
                 st["event"] = None
                 moved = True
             if st["done"] >= st["req"].steps:
@@ -212,7 +218,10 @@ class Server:
             idle.append(rid)
         if not launch:
             return moved
-        work = lambda r: (self.inflight[r]["req"].steps - self.inflight[r]["done"]) * self.inflight[r]["cost"]
+        def work(r):
+            st = self.inflight[r]
+            per = st["meas"] if st["meas"] is not None else st["cost"]
+            return (st["req"].steps - st["done"]) * per
         # the jobs with the most work left go to free long lanes, the others
         # (least work first) to free ordinary lanes
         long_free = [ln for ln in self.lanes[:self.long_lanes] if id(ln) not in busy]
@@ -225,11 +234,13 @@ class Server:
             st = self.inflight[rid]
             n = min(st["q"], st["req"].steps - st["done"])
             st["lane"] = lane
+            t0 = self.torch.cuda.Event(enable_timing=True)
+            t0.record(lane)
             self.ctx.run([st["job"]], n, stream=lane.cuda_stream)
             st["done"] += n
-            ev = self.torch.cuda.Event()
+            ev = self.torch.cuda.Event(enable_timing=True)
             ev.record(lane)
-            st["event"] = ev
+            st["start"], st["event"], st["qn"] = t0, ev, n
             moved = True
         return moved
 

@@ -75,22 +75,26 @@ k_hi_assemble(const JobDev* __restrict__ Jp, GridAux aux) {
 // Factor, by 8-wide sub-panels: every thread that solves a row factors the
 // sub-panel's 8 x 8 diagonal block in registers (the same arithmetic in each
 // thread, so nothing but a barrier sits between the pivots of a sub-panel;
-// one FP64 rsqrt per pivot gives both L_cc = d rsqrt(d) and 1 / L_cc), solves
-// its row of the sub-panel below the block, and then the 512 threads share the
-// (row, column) pairs of the trailing lower triangle evenly, eight terms per
-// entry in column order.
-// Inverse X = L^-1, by 8-wide block columns, one warp per block column: the
-// diagonal block by forward substitution, then block row after block row
-// S = sum_k L_ik X_kj (two entries per lane) and L_ii X_ij = -S by forward
-// substitution.  X's strict lower triangle is kept transposed in the unused
-// upper triangle of the tile, its diagonal beside it.
+// one FP64 rsqrt per pivot gives both L_cc = d rsqrt(d) and 1 / L_cc),
+// solves its row of the sub-panel below the block (kept column-major beside
+// the tile as well); then the trailing lower triangle is updated by warps in
+// strips of 32 rows x 4 columns, a row per lane (eight terms per entry, in
+// column order).
+// Inverse X = L^-1 by recursive doubling: the sixteen 8 x 8 diagonal blocks
+// by forward substitution (a thread per column), then four levels that
+// merge pairs of diagonal blocks of size B = 8 .. 64, X_UT = -X_UU (L_UT
+// X_TT), two triangular products per level with all 512 threads (its
+// critical path is about 2B dependent FMAs per level instead of the 128 of
+// a forward substitution).  X's strict lower triangle is kept transposed in
+// the unused upper triangle of the tile, its diagonal beside it.  Tile loads
+// are issued unconditionally (clamped addresses), 32 per thread in flight.
 // Out: the factor (FP32) into the tensor's tile, X (FP32, zero above the
 // diagonal and outside nb) into aux.linv for the tile-column solve.  A
 // pivot that is not positive sets the job's status.
 constexpr int kPotrfThreads = 512;
 constexpr int kPotrfW = 8;                    // sub-panel width
 constexpr int kPotrfLd = kCT + 1;             // doubles
-constexpr size_t kPotrfSmem = (size_t)(kCT * kPotrfLd + 2 * kCT) * sizeof(double);
+constexpr size_t kPotrfSmem = (size_t)(kCT * kPotrfLd + 2 * kCT + kPotrfW * kCT + kCT * kCT / 4) * sizeof(double);
 
 // 1 / sqrt(d) in FP64 for d > 0: the FP32 estimate refined by two steps of
 // the Newton-Raphson iteration y <- y (3 - d y^2) / 2, each of which roughly
@@ -126,20 +130,90 @@ __device__ __forceinline__ void diag8_factor(const double* P, int c0, int w, dou
     }
 }
 
+// One level of the recursive inverse: pairs of diagonal blocks of size B
+// (top T, bottom U) merge as X_UT = -X_UU (L_UT X_TT), two triangular
+// products.  Thread: row i of its pair's block, R = B / 8 consecutive
+// columns j0 ..; the rows vary fastest within a warp, so the row-dependent
+// operand is read row-parallel and the other one is a broadcast.  X[a][c],
+// a > c, at P64[c][a]; X[a][a] at xd[a].  Ends with a barrier.
+template <int B>
+__device__ __forceinline__ void inv_level(double* P64, double* xd, double* ybuf) {
+    constexpr int R = B / 8;
+    const int tid = threadIdx.x, i = tid % B, j0 = ((tid / B) % 8) * R, pr = tid / (8 * B);
+    const int i0 = 2 * B * pr;                 // the pair's first row / column
+    double* Y = ybuf + pr * B * B;             // L_UT X_TT of this pair, row-major
+    {
+        double y[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) y[t] = 0.0;
+        const double* Lr = P64 + (i0 + B + i) * kPotrfLd + i0;
+        // X_TT[k][j] is zero for k < j: the first R values of k are triangular
+#pragma unroll
+        for (int dk = 0; dk < R; ++dk) {
+            const int kk = j0 + dk;
+            const double a = Lr[kk];
+#pragma unroll
+            for (int t = 0; t <= dk; ++t) {
+                const int j = j0 + t;
+                y[t] += a * (t == dk ? xd[i0 + j] : P64[(i0 + j) * kPotrfLd + i0 + kk]);
+            }
+        }
+        for (int kk = j0 + R; kk < B; ++kk) {
+            const double a = Lr[kk];
+#pragma unroll
+            for (int t = 0; t < R; ++t) y[t] += a * P64[(i0 + j0 + t) * kPotrfLd + i0 + kk];
+        }
+#pragma unroll
+        for (int t = 0; t < R; ++t) Y[i * B + j0 + t] = y[t];
+    }
+    __syncthreads();
+    {
+        double x[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = 0.0;
+        const int a = i0 + B + i;
+        for (int kk = 0; kk < i; ++kk) {
+            const double xuu = P64[(i0 + B + kk) * kPotrfLd + a];
+#pragma unroll
+            for (int t = 0; t < R; ++t) x[t] -= xuu * Y[kk * B + j0 + t];
+        }
+        const double xaa = xd[a];
+#pragma unroll
+        for (int t = 0; t < R; ++t) P64[(i0 + j0 + t) * kPotrfLd + a] = x[t] - xaa * Y[i * B + j0 + t];
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kPotrfThreads)
 k_chol_potrf64(JobDev* __restrict__ Jp, GridAux aux, int J) {
-    extern __shared__ double P64[];   // [kCT][kPotrfLd], the diagonal of X [kCT], 1 / L_cc [kCT]
+    // [kCT][kPotrfLd] tile, the diagonal of X [kCT], 1 / L_cc [kCT], the
+    // current sub-panel column-major [kPotrfW][kCT], inverse products
+    extern __shared__ double P64[];
     __shared__ int stop;
     if (threadIdx.x == 0) stop = Jp->status;
     __syncthreads();
     if (stop) return;
     double* xd = P64 + kCT * kPotrfLd;
     double* rdiag = xd + kCT;
+    double* panel = rdiag + kCT;
+    double* ybuf = panel + kPotrfW * kCT;     // [kCT * kCT / 4]: the products of one inverse level
     const int m = 3 * Jp->n, ld = aux.ld, k = J * kCT, nb = min(kCT, m - k);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kPer = kCT * kCT / kPotrfThreads;     // tile entries per thread
     float* M = aux.tensor + (size_t)k * ld + k;
-    for (int r = warp; r < nb; r += kPotrfThreads / 32)
-        for (int c = lane; c <= r; c += 32) P64[r * kPotrfLd + c] = (double)M[(size_t)r * ld + c];
+    {
+        float v[kPer];
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int e = tid + u * kPotrfThreads, r = min(e >> 7, nb - 1), c = min(e & (kCT - 1), nb - 1);
+            v[u] = M[(size_t)r * ld + c];
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int e = tid + u * kPotrfThreads, r = e >> 7, c = e & (kCT - 1);
+            if (r < nb && c <= r) P64[r * kPotrfLd + c] = (double)v[u];
+        }
+    }
     __syncthreads();
     int bad = 0;
     // ---- factor ----
@@ -170,123 +244,108 @@ k_chol_potrf64(JobDev* __restrict__ Jp, GridAux aux, int J) {
                 }
 #pragma unroll
                 for (int c = 0; c < kPotrfW; ++c)
-                    if (c < w) P64[r * kPotrfLd + c0 + c] = x[c];
+                    if (c < w) {
+                        P64[r * kPotrfLd + c0 + c] = x[c];
+                        panel[c * kCT + r] = x[c];
+                    }
             }
         }
         __syncthreads();
-        // trailing lower triangle, rows and columns t0 .. nb - 1: pair p is
-        // (row t0 + a, column t0 + b) with p = a (a + 1) / 2 + b, b <= a
-        const int R = nb - t0, npairs = R * (R + 1) / 2;
-        for (int p = tid; p < npairs; p += kPotrfThreads) {
-            int a = (int)((sqrtf(8.f * (float)p + 1.f) - 1.f) * 0.5f);
-            while ((a + 1) * (a + 2) / 2 <= p) ++a;
-            while (a * (a + 1) / 2 > p) --a;
-            const int rr = t0 + a, q = t0 + (p - a * (a + 1) / 2);
-            double acc = P64[rr * kPotrfLd + q];
+        // trailing lower triangle, rows and columns t0 .. nb - 1: a warp
+        // takes a strip of 32 rows (a row per lane) by 4 columns at a time,
+        // the sub-panel read column-major (each lane its row's value, the
+        // four columns' values as broadcasts); eight terms per entry in
+        // column order
+        const int R = nb - t0, nstrips = (R + 31) >> 5;
+        int ntasks = 0;
+        for (int st = 0; st < nstrips; ++st) ntasks += (min(R, 32 * st + 32) + 3) >> 2;
+        for (int task = warp; task < ntasks; task += kPotrfThreads / 32) {
+            int st = 0, g = task;
+            while (g >= ((min(R, 32 * st + 32) + 3) >> 2)) {
+                g -= (min(R, 32 * st + 32) + 3) >> 2;
+                ++st;
+            }
+            const int row = t0 + 32 * st + lane, q0 = t0 + 4 * g;
+            double acc[4];
 #pragma unroll
-            for (int c = 0; c < kPotrfW; ++c)
-                if (c < w) acc -= P64[rr * kPotrfLd + c0 + c] * P64[q * kPotrfLd + c0 + c];
-            P64[rr * kPotrfLd + q] = acc;
+            for (int v = 0; v < 4; ++v)
+                acc[v] = (row < nb && q0 + v <= row) ? P64[row * kPotrfLd + q0 + v] : 0.0;
+#pragma unroll
+            for (int c = 0; c < kPotrfW; ++c) {
+                if (c < w) {
+                    const double x = row < nb ? panel[c * kCT + row] : 0.0;
+                    const double2 y01 = *reinterpret_cast<const double2*>(panel + c * kCT + q0);
+                    const double2 y23 = *reinterpret_cast<const double2*>(panel + c * kCT + q0 + 2);
+                    acc[0] -= x * y01.x;
+                    acc[1] -= x * y01.y;
+                    acc[2] -= x * y23.x;
+                    acc[3] -= x * y23.y;
+                }
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+                if (row < nb && q0 + v <= row) P64[row * kPotrfLd + q0 + v] = acc[v];
         }
         __syncthreads();
     }
-    // ---- inverse: warp j owns block column j (columns 8 j .. 8 j + 7) ----
-    // X[a][b], a > b, lives at P64[b][a]; X[a][a] at xd[a]
-    const int nblk = (nb + kPotrfW - 1) / kPotrfW;
-    if (warp < nblk) {
-        const int j0 = warp * kPotrfW, wj = min(kPotrfW, nb - j0);
-        // diagonal block: lane c < wj solves L_jj x = e_c (column c of X_jj)
-        if (lane < kPotrfW) {
-            const int c = lane;
-            double x[kPotrfW];
+    // ---- inverse X = L^-1 by recursive doubling of diagonal blocks ----
+    // X[a][c], a > c, lives at P64[c][a]; X[a][a] at xd[a].  Rows and columns
+    // from nb to 127 are made the identity first, so every level is full.
+    for (int e = tid; e < (kCT - nb) * kCT; e += kPotrfThreads) {
+        const int r = nb + e / kCT, c = e % kCT;
+        if (c <= r) P64[r * kPotrfLd + c] = r == c ? 1.0 : 0.0;
+        if (c == 0) rdiag[r] = 1.0;
+    }
+    __syncthreads();
+    if (tid < kCT) {
+        // the sixteen 8 x 8 diagonal blocks: thread (block, column cc)
+        // solves L_bb x = e_cc by forward substitution
+        const int b0 = tid & ~(kPotrfW - 1), cc = tid & (kPotrfW - 1);
+        double x[kPotrfW];
 #pragma unroll
-            for (int r = 0; r < kPotrfW; ++r) {
-                double v = (r == c) ? 1.0 : 0.0;
+        for (int r = 0; r < kPotrfW; ++r) {
+            double v = r == cc ? 1.0 : 0.0;
 #pragma unroll
-                for (int q = 0; q < r; ++q)
-                    if (q >= c) v -= P64[(j0 + r) * kPotrfLd + j0 + q] * x[q];
-                x[r] = (r >= c && r < wj && c < wj) ? v * rdiag[j0 + r] : 0.0;
-            }
-#pragma unroll
-            for (int r = 0; r < kPotrfW; ++r)
-                if (c < wj && r < wj) {
-                    if (r == c) xd[j0 + r] = x[r];
-                    else if (r > c) P64[(j0 + c) * kPotrfLd + j0 + r] = x[r];
-                }
+            for (int q = 0; q < r; ++q)
+                if (q >= cc) v -= P64[(b0 + r) * kPotrfLd + b0 + q] * x[q];
+            x[r] = r < cc ? 0.0 : v * rdiag[b0 + r];
         }
-        __syncwarp();
-        // block rows below: S = sum_{k = j..i-1} L_ik X_kj, then L_ii X_ij = -S
-        const int er = lane >> 2, ec = 2 * (lane & 3);   // this lane's entries (er, ec), (er, ec + 1) of the block
-        for (int i0 = j0 + kPotrfW; i0 < nb; i0 += kPotrfW) {
-            const int wi = min(kPotrfW, nb - i0);
-            double s0 = 0.0, s1 = 0.0;
-            if (er < wi) {
-                const double* Lr = P64 + (i0 + er) * kPotrfLd;
-                const int c0x = j0 + ec, c1x = c0x + 1;
-                // the diagonal block's rows of X: diagonal, below it (stored transposed), or zero
-                for (int q = j0; q < j0 + wj; ++q) {
-                    const double x0 = q == c0x ? xd[q] : (q > c0x && c0x < j0 + wj ? P64[c0x * kPotrfLd + q] : 0.0);
-                    const double x1 = q == c1x ? xd[q] : (q > c1x && c1x < j0 + wj ? P64[c1x * kPotrfLd + q] : 0.0);
-                    s0 += Lr[q] * x0;
-                    s1 += Lr[q] * x1;
-                }
-                // block rows j+1 .. i-1 of X, below the diagonal: four partial sums each
-                if (c0x < j0 + wj) {
-                    const double* X0 = P64 + c0x * kPotrfLd;
-                    const double* X1 = P64 + c1x * kPotrfLd;
-                    const bool has1 = c1x < j0 + wj;
-                    double a0[4] = {0.0, 0.0, 0.0, 0.0}, a1[4] = {0.0, 0.0, 0.0, 0.0};
-                    int q = j0 + kPotrfW;
-                    for (; q + 4 <= i0; q += 4) {
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
-                            a0[u] += Lr[q + u] * X0[q + u];
-                            if (has1) a1[u] += Lr[q + u] * X1[q + u];
-                        }
-                    }
-                    for (; q < i0; ++q) {
-                        a0[0] += Lr[q] * X0[q];
-                        if (has1) a1[0] += Lr[q] * X1[q];
-                    }
-                    s0 += (a0[0] + a0[1]) + (a0[2] + a0[3]);
-                    s1 += (a1[0] + a1[1]) + (a1[2] + a1[3]);
-                }
-            }
-            // stage -S in the block's transposed slots, then solve column by column
-            if (er < wi) {
-                if (ec < wj) P64[(j0 + ec) * kPotrfLd + i0 + er] = -s0;
-                if (ec + 1 < wj) P64[(j0 + ec + 1) * kPotrfLd + i0 + er] = -s1;
-            }
-            __syncwarp();
-            if (lane < wj) {
-                const int c = j0 + lane;
-                double x[kPotrfW];
-#pragma unroll
-                for (int r = 0; r < kPotrfW; ++r) {
-                    if (r < wi) {
-                        double v = P64[c * kPotrfLd + i0 + r];
-#pragma unroll
-                        for (int q = 0; q < r; ++q) v -= P64[(i0 + r) * kPotrfLd + i0 + q] * x[q];
-                        x[r] = v * rdiag[i0 + r];
-                    } else {
-                        x[r] = 0.0;
-                    }
-                }
-#pragma unroll
-                for (int r = 0; r < kPotrfW; ++r)
-                    if (r < wi) P64[c * kPotrfLd + i0 + r] = x[r];
-            }
-            __syncwarp();
+        for (int r = 0; r < kPotrfW; ++r) {
+            if (r == cc) xd[b0 + r] = x[r];
+            else if (r > cc) P64[(b0 + cc) * kPotrfLd + b0 + r] = x[r];
         }
     }
     __syncthreads();
-    for (int r = warp; r < nb; r += kPotrfThreads / 32)
-        for (int c = lane; c <= r; c += 32) M[(size_t)r * ld + c] = (float)P64[r * kPotrfLd + c];
-    for (int e = tid; e < kCT * kCT; e += kPotrfThreads) {
-        const int r = e >> 7, c = e & (kCT - 1);
-        float v = 0.f;
-        if (r < nb && c < nb) v = r == c ? (float)xd[r] : (r > c ? (float)P64[c * kPotrfLd + r] : 0.f);
-        aux.linv[e] = v;
+    // merge pairs of diagonal blocks of size B = 8, 16, 32, 64
+    inv_level<8>(P64, xd, ybuf);
+    inv_level<16>(P64, xd, ybuf);
+    inv_level<32>(P64, xd, ybuf);
+    inv_level<64>(P64, xd, ybuf);
+    // out: the factor's rows (zero above the diagonal) and X, four columns
+    // per store; a chunk that would pass column nb - 1 of the last tile
+    // column (and reach the next row) is stored column by column
+#pragma unroll 4
+    for (int u = 0; u < kPer / 4; ++u) {
+        const int e = tid + u * kPotrfThreads, r = e >> 5, c = (e & 31) * 4;
+        float lv[4], xv[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const int q = c + t;
+            lv[t] = (r < nb && q <= r) ? (float)P64[r * kPotrfLd + q] : 0.f;
+            xv[t] = (r < nb && q < nb) ? (r == q ? (float)xd[r] : (r > q ? (float)P64[q * kPotrfLd + r] : 0.f)) : 0.f;
+        }
+        *reinterpret_cast<float4*>(aux.linv + r * kCT + c) = make_float4(xv[0], xv[1], xv[2], xv[3]);
+        if (r < nb) {
+            float* dst = M + (size_t)r * ld + c;
+            if (c + 4 <= nb) {
+                *reinterpret_cast<float4*>(dst) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+            } else {
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (c + t < nb) dst[t] = lv[t];
+            }
+        }
     }
     if (bad) atomicMax(&Jp->status, SOPB_ERR_HI);
 }

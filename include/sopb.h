@@ -253,7 +253,7 @@ int sopb_context_set_shape_policy(sopb_context* ctx, int32_t lanes_per_bead, flo
 /* Launch policy of grid-path HI jobs created from now on: the width of the
  * exact-HI factorisation's outer panels, in 128-column tiles (default 4:
  * each trailing tile is updated once per 512 columns), and the CTAs per SM
- * that the O(N^2) TEA and D F sums are sliced for (default 4).  Both change
+ * that the O(N^2) TEA and D F sums are sliced for (default 8).  Both change
  * only the order of floating-point sums; a job keeps the policy it was
  * created with.  The autotuner's knob for HI jobs; no reference counterpart
  * (the reference factorises unblocked, one CTA per trajectory,

@@ -78,6 +78,10 @@ inline int64_t grid_cap_nr(const sopb_params& p, int64_t cap_pp, int64_t cap_pl)
     return near_skin(p) > 0.02f ? std::max<int64_t>(1, std::min<int64_t>(cap_pp, 2 * cap_pl)) : 0;
 }
 
+// Default CTAs per SM that the O(N^2) TEA and D F sums are sliced for (the
+// fastest of 2..32 for TEA and exact HI at 4000 beads on B200).
+constexpr int32_t kHiCtasPerSm = 8;
+
 // Shape policy of the resident kernel (see launch_shape).
 struct ShapePolicy {
     int32_t lpb = 4;
@@ -86,7 +90,7 @@ struct ShapePolicy {
     // grid-path HI jobs: outer-panel width of the exact-HI factorisation (tile
     // columns) and the CTAs per SM the O(N^2) sums are sliced for
     int32_t chol_panel_tiles = kCholPanelTiles;
-    int32_t hi_ctas_per_sm = 4;
+    int32_t hi_ctas_per_sm = kHiCtasPerSm;
 };
 
 struct LaunchClass {
@@ -700,7 +704,8 @@ struct GridLayout {
     size_t total = 0;
 };
 
-GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl, int hi_cps = 4) {
+GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl,
+                       int hi_cps = kHiCtasPerSm) {
     GridLayout L;
     L.npart = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)sms * 8);
     L.cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);

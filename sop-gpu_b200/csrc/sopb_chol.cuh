@@ -359,6 +359,7 @@ k_hi_df_partial(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
     if (J.status) return;
     const int n = J.n, i = blockIdx.x * kHiTile + threadIdx.x, s = blockIdx.y;
     const float4 xi = aux.xc[i < n ? i : 0];
+    const float a = J.hi_a, inv_a = 1.f / J.hi_a;
     float3 f = make_float3(0.f, 0.f, 0.f);
     const int span = ((n + jsplit - 1) / jsplit + kHiTile - 1) / kHiTile * kHiTile;
     const int j0 = s * span, j1 = min(n, j0 + span);
@@ -371,15 +372,22 @@ k_hi_df_partial(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
         }
         __syncthreads();
         const int cnt = min(kHiTile, j1 - t0);
-        if (i < n)
-            for (int kk = 0; kk < cnt; ++kk) {
-                if (t0 + kk == i) continue;
-                const Blk6 d = rpy_between(xi, xs[kk], J.hi_a);
-                const float4 fq = ms[kk];
-                f.x += d.xx * fq.x + d.xy * fq.y + d.xz * fq.z;
-                f.y += d.xy * fq.x + d.yy * fq.y + d.yz * fq.z;
-                f.z += d.xz * fq.x + d.yz * fq.y + d.zz * fq.z;
+        auto term = [&](int kk) {
+            const Blk6 d = rpy_fast(xi, xs[kk], a, inv_a);
+            const float4 fq = ms[kk];
+            f.x += d.xx * fq.x + d.xy * fq.y + d.xz * fq.z;
+            f.y += d.xy * fq.x + d.yy * fq.y + d.yz * fq.z;
+            f.z += d.xz * fq.x + d.yz * fq.y + d.zz * fq.z;
+        };
+        if (i < n) {
+            if (t0 == blockIdx.x * kHiTile) {   // the tile of this CTA's own beads
+                for (int kk = 0; kk < cnt; ++kk)
+                    if (t0 + kk != i) term(kk);
+            } else {
+#pragma unroll 4
+                for (int kk = 0; kk < cnt; ++kk) term(kk);
             }
+        }
     }
     if (i < n) aux.part[(size_t)s * n + i] = make_float4(f.x, f.y, f.z, 0.f);
 }

@@ -51,6 +51,22 @@ __device__ __forceinline__ Blk6 rpy_between(float4 xi, float4 xj, float a) {
     return rpy_block(dx, dy, dz, r, a);
 }
 
+// The same block for the per-step O(n^2) sums, with one reciprocal square
+// root per pair: e = d rsqrt(r^2), u = a / r = a rsqrt(r^2), and the far
+// field (r > 2a) tested as r^2 > 4a^2; both branches are formed and one is
+// selected, so a warp does not diverge on the pair distance.
+__device__ __forceinline__ Blk6 rpy_fast(float4 xi, float4 xj, float a, float inv_a) {
+    const float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float ir = rsqrtf(r2);
+    const float ex = dx * ir, ey = dy * ir, ez = dz * ir;
+    const float u = a * ir, u2 = u * u, ra = r2 * ir * inv_a;
+    const bool far = r2 > 4.f * a * a;
+    const float crr = far ? 0.75f * u * (1.f - 2.f * u2) : (3.f / 32.f) * ra;
+    const float cii = far ? 0.75f * u * (1.f + (2.f / 3.f) * u2) : 1.f - (9.f / 32.f) * ra;
+    return {ex * ex * crr + cii, ex * ey * crr, ex * ez * crr, ey * ey * crr + cii, ey * ez * crr, ez * ez * crr + cii};
+}
+
 // integrateTea_epsilon_local (bdhitea_kernel.cu:192-210): squared row sums
 // (x, y, z) and the sum of all nine entries (w).
 __device__ __forceinline__ void eps_stats(float4 xi, float4 xj, float a, float4& s) {
@@ -62,8 +78,9 @@ __device__ __forceinline__ void eps_stats(float4 xi, float4 xj, float a, float4&
 }
 
 // integrateTea_force (bdhitea_kernel.cu:252-301): D_ij (F_j + beta C_i o g_j).
-__device__ __forceinline__ void tea_pair(float4 xi, float4 xj, float4 mj, float4 rj, float3 bci, float a, float3& f) {
-    const Blk6 d = rpy_between(xi, xj, a);
+__device__ __forceinline__ void tea_pair(float4 xi, float4 xj, float4 mj, float4 rj, float3 bci, float a, float inv_a,
+                                         float3& f) {
+    const Blk6 d = rpy_fast(xi, xj, a, inv_a);
     const float f0 = mj.x + rj.x * bci.x, f1 = mj.y + rj.y * bci.y, f2 = mj.z + rj.z * bci.z;
     f.x += d.xx * f0 + d.xy * f1 + d.xz * f2;
     f.y += d.xy * f0 + d.yy * f1 + d.yz * f2;
@@ -209,6 +226,7 @@ k_tea_force_partial(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
     const int n = J.n, i = blockIdx.x * kHiTile + threadIdx.x, s = blockIdx.y;
     const float4 xi = aux.xc[i < n ? i : 0];
     const float3 bci = tea_bci(J, aux, i < n ? i : 0, nullptr);
+    const float a = J.hi_a, inv_a = 1.f / J.hi_a;
     float3 f = make_float3(0.f, 0.f, 0.f);
     if (J.hi_unlisted) {
         const int span = ((n + jsplit - 1) / jsplit + kHiTile - 1) / kHiTile * kHiTile;
@@ -223,24 +241,30 @@ k_tea_force_partial(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
             }
             __syncthreads();
             const int cnt = min(kHiTile, j1 - t0);
-            if (i < n)
-                for (int k = 0; k < cnt; ++k)
-                    if (t0 + k != i) tea_pair(xi, xs[k], ms[k], rs[k], bci, J.hi_a, f);
+            if (i < n) {
+                if (t0 == blockIdx.x * kHiTile) {   // the tile of this CTA's own beads
+                    for (int k = 0; k < cnt; ++k)
+                        if (t0 + k != i) tea_pair(xi, xs[k], ms[k], rs[k], bci, a, inv_a, f);
+                } else {
+#pragma unroll 4
+                    for (int k = 0; k < cnt; ++k) tea_pair(xi, xs[k], ms[k], rs[k], bci, a, inv_a, f);
+                }
+            }
         }
     } else if (s == 0 && i < n) {
         // integrateTea_kernel: covalent, native and Verlet partners
         for (int k = J.cov_off[i]; k < J.cov_off[i + 1]; ++k) {
             const int q = J.cov_j[k];
-            tea_pair(xi, aux.xc[q], aux.mf[q], aux.rf[q], bci, J.hi_a, f);
+            tea_pair(xi, aux.xc[q], aux.mf[q], aux.rf[q], bci, a, inv_a, f);
         }
         for (int k = J.nat_off[i]; k < J.nat_off[i + 1]; ++k) {
             const int q = J.nat_j[k];
-            tea_pair(xi, aux.xc[q], aux.mf[q], aux.rf[q], bci, J.hi_a, f);
+            tea_pair(xi, aux.xc[q], aux.mf[q], aux.rf[q], bci, a, inv_a, f);
         }
         const int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
         for (int k = 0; k < J.pl_cnt[i]; ++k) {
             const int q = row[k];
-            tea_pair(xi, aux.xc[q], aux.mf[q], aux.rf[q], bci, J.hi_a, f);
+            tea_pair(xi, aux.xc[q], aux.mf[q], aux.rf[q], bci, a, inv_a, f);
         }
     }
     if (i < n) aux.part[(size_t)s * n + i] = make_float4(f.x, f.y, f.z, 0.f);

@@ -341,7 +341,7 @@ class Context:
         check(lib().sopb_context_set_shape_policy(self.handle, int(lanes_per_bead), float(beads_per_group),
                                                   int(max_block)), "set_shape_policy")
 
-    def set_hi_policy(self, chol_panel_tiles: int = 4, hi_ctas_per_sm: int = 4) -> None:
+    def set_hi_policy(self, chol_panel_tiles: int = 4, hi_ctas_per_sm: int = 8) -> None:
         """HI launch policy for jobs created from now on (autotuner knob):
         exact-HI outer-panel width in 128-column tiles, and the CTAs per SM
         the O(N^2) HI sums are sliced for."""

@@ -242,32 +242,50 @@ __device__ void build_verlet(const JobDev& J, const float4* __restrict__ xs, int
 // skin since the near list was built, every pair now closer than
 // pairlist_cutoff was closer than pairlist_cutoff + skin then, so filtering
 // the near rows (increasing j) with the same exact test gives the same rows
-// as the full scan.  A warp per bead, lanes over 32 near entries at a time.
+// as the full scan.  A warp per bead, lanes over 32 near entries at a time;
+// the warp fetches its next bead's row length while it filters the current
+// row, and a row's first kNearAhead x 32 entries are loaded before any of
+// them is tested, so a row costs one global round trip, not one per 32.
+constexpr int kNearAhead = 8;
 template <int BLOCK>
 __device__ void build_verlet_near(const JobDev& J, const float4* __restrict__ xs, int& err) {
     const int n = J.n, lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
-    for (int i = threadIdx.x >> 5; i < n; i += BLOCK / 32) {
-        const float4 xi = xs[i];
+    int i = threadIdx.x >> 5;
+    int ncnt = i < n ? J.nr_cnt[i] : 0;
+    for (; i < n; i += BLOCK / 32) {
+        const int ncnt_next = i + BLOCK / 32 < n ? J.nr_cnt[i + BLOCK / 32] : 0;
         const uint16_t* nrow = J.nr_j + (size_t)i * J.cap_nr;
-        const int ncnt = J.nr_cnt[i];
+        int q[kNearAhead];
+#pragma unroll
+        for (int u = 0; u < kNearAhead; ++u) {
+            const int k = 32 * u + lane;
+            q[u] = k < ncnt ? nrow[k] : 0;
+        }
+        const float4 xi = xs[i];
         int32_t* row = J.pl_j + (size_t)i * J.cap_pl;
         int cnt = 0;
-        for (int kb = 0; kb < ncnt; kb += 32) {
-            const int k = kb + lane;
-            const int q = k < ncnt ? nrow[k] : 0;
-            const bool ok = k < ncnt && within_cutoff(xi, xs[q], J.pl_t);
+        auto take = [&](int k, int qk) {
+            const bool ok = k < ncnt && within_cutoff(xi, xs[qk], J.pl_t);
             const uint32_t hit = __ballot_sync(0xffffffffu, ok);
             if (ok) {
                 const int pos = cnt + __popc(hit & below);
-                if (pos < J.cap_pl) row[pos] = q;
+                if (pos < J.cap_pl) row[pos] = qk;
             }
             cnt += __popc(hit);
+        };
+#pragma unroll
+        for (int u = 0; u < kNearAhead; ++u)
+            if (32 * u < ncnt) take(32 * u + lane, q[u]);   // the same for the warp's lanes
+        for (int kb = 32 * kNearAhead; kb < ncnt; kb += 32) {
+            const int k = kb + lane;
+            take(k, k < ncnt ? nrow[k] : 0);
         }
         if (lane == 0) {
             if (cnt > J.cap_pl) err = SOPB_STATUS_CAPACITY;
             J.pl_cnt[i] = cnt < J.cap_pl ? cnt : J.cap_pl;
         }
+        ncnt = ncnt_next;
     }
 }
 
@@ -474,23 +492,31 @@ __device__ void fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap
     if (tid == 0) off[n] = *tot_smem;
     __syncthreads();
     {
-        for (int i = w; i < n; i += BLOCK / 32) {
+        // two beads per warp at a time, so that the loads of both rows are
+        // in flight together
+        for (int i = w; i < n; i += 2 * (BLOCK / 32)) {
+            const int i2 = i + BLOCK / 32;
+            const bool in1 = off[i + 1] <= cap, in2 = i2 < n && off[i2 + 1] <= cap;
+            const int k0 = off[i], cnt = in1 ? off[i + 1] - k0 : 0;
+            const int k02 = in2 ? off[i2] : 0, cnt2 = in2 ? off[i2 + 1] - k02 : 0;
             const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
-            const int k0 = off[i], cnt = off[i + 1] - k0;
-            if (off[i + 1] > cap) break;
-            for (int kb = 0; kb < cnt; kb += 128) {
-                int v[4];
+            const int32_t* r2 = J.pl_j + (size_t)(in2 ? i2 : i) * J.cap_pl;
+            for (int kb = 0; kb < max(cnt, cnt2); kb += 128) {
+                int v[4], v2[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = kb + 32 * u + lane;
                     v[u] = k < cnt ? r[k] : 0;
+                    v2[u] = k < cnt2 ? r2[k] : 0;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = kb + 32 * u + lane;
                     if (k < cnt) nbr[k0 + k] = (uint16_t)v[u];
+                    if (k < cnt2) nbr[k02 + k] = (uint16_t)v2[u];
                 }
             }
+            if (!in2) break;   // every later bead ends beyond the cache as well
         }
     }
     __syncthreads();

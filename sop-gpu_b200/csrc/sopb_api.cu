@@ -190,13 +190,20 @@ struct sopb_job {
     // its first step (kDue* bits)
     std::map<int, cudaGraphExec_t> chunks;
     int bead_blocks = 1;               // CTAs of the per-bead grid kernels
-    // exact HI: streams of the factorisation, one per stream priority level
-    // (created on first use): the panel chain runs one level above the
-    // caller's stream, the trailing updates at the caller's level
+    // exact HI: streams of the factorisation, two per stream priority level
+    // (made at job creation): the single-tile chain runs two levels above
+    // the caller's stream, the rest of each tile column one level above it,
+    // the bulk trailing updates at the caller's level
     static constexpr int kPrioLevels = 8;
     cudaStream_t prio_st[kPrioLevels] = {};
+    cudaStream_t mid_st[kPrioLevels] = {};
     bool hi_streams = false;
-    cudaEvent_t la_fork = nullptr, la_join = nullptr, hp_fork = nullptr, hp_join = nullptr;
+    cudaEvent_t la_join = nullptr, hp_fork = nullptr, hp_join = nullptr;
+    // hand-offs between the chain and the tile-column stream: rings of four
+    // (factor done, first tile solved, column updated, rest solved), then
+    // the next-panel updates and the column stream's join
+    static constexpr int kLkRing = 4;
+    cudaEvent_t lk_ev[4 * kLkRing + 3] = {};
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
     int chol_w = kCholPanelTiles;      // exact HI: outer-panel width of the factorisation, tile columns
     CUtensorMap tmap_ten{};            // exact HI: TMA maps of the tensor and of the diagonal tile's
@@ -222,6 +229,14 @@ struct sopb_job {
     } while (0)
 
 namespace {
+
+// Streams and events of an exact-HI job's factorisation.
+void hi_streams_destroy(sopb_job* j) {
+    for (cudaStream_t q : j->prio_st) if (q) cudaStreamDestroy(q);
+    for (cudaStream_t q : j->mid_st) if (q) cudaStreamDestroy(q);
+    for (cudaEvent_t e : {j->la_join, j->hp_fork, j->hp_join}) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : j->lk_ev) if (e) cudaEventDestroy(e);
+}
 
 // Opt the resident kernel in to the largest dynamic shared memory the device
 // allows next to the kernel's static shared memory.
@@ -489,10 +504,7 @@ extern "C" int sopb_context_destroy(sopb_context* c) {
     for (sopb_job* j : c->slots)
         if (j) {
             for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
-            if (j->hi_streams) {
-                for (cudaStream_t q : j->prio_st) if (q) cudaStreamDestroy(q);
-                for (cudaEvent_t e : {j->la_fork, j->la_join, j->hp_fork, j->hp_join}) cudaEventDestroy(e);
-            }
+            if (j->hi_streams) hi_streams_destroy(j);
             if (j->amem) cudaFree(j->amem);
             cudaFree(j->dmem);
             cudaEventDestroy(j->ev);
@@ -727,7 +739,7 @@ GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp,
         if (L.exact) {
             L.ld = L.blocked ? chol_ld((int)n) : (int)(3 * n);
             L.ten = take((size_t)3 * n * L.ld * 4);
-            if (L.blocked) L.linv = take((size_t)kCT * kCT * 4);
+            if (L.blocked) L.linv = take((size_t)2 * kCT * kCT * 4);
         }
     }
     L.geo = take(8 * sizeof(float));
@@ -778,16 +790,19 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, in
             const int m = 3 * n;
             a.linv = (float*)(b + L.linv);
             SOPB_TRY(encode_tmap_f32(&j->tmap_ten, a.tensor, m, m, a.ld));
-            SOPB_TRY(encode_tmap_f32(&j->tmap_linv, a.linv, kCT, kCT, kCT));
-            // one stream per priority level, made here rather than during a
-            // stream capture
+            SOPB_TRY(encode_tmap_f32(&j->tmap_linv, a.linv, 2 * kCT, kCT, kCT));
+            // two streams per priority level, made here rather than during
+            // a stream capture
             j->hi_streams = true;
             int lo = 0, hi = 0;
             CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-            for (int k = 0; k <= std::min(lo - hi, sopb_job::kPrioLevels - 1); ++k)
+            for (int k = 0; k <= std::min(lo - hi, sopb_job::kPrioLevels - 1); ++k) {
                 CUDA_TRY(cudaStreamCreateWithPriority(&j->prio_st[k], cudaStreamNonBlocking, lo - k));
-            for (cudaEvent_t* e : {&j->la_fork, &j->la_join, &j->hp_fork, &j->hp_join})
+                CUDA_TRY(cudaStreamCreateWithPriority(&j->mid_st[k], cudaStreamNonBlocking, lo - k));
+            }
+            for (cudaEvent_t* e : {&j->la_join, &j->hp_fork, &j->hp_join})
                 CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            for (cudaEvent_t& e : j->lk_ev) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         }
     }
     a.cell_geo = (float*)(b + L.geo);
@@ -835,63 +850,123 @@ int grid_possible(sopb_job* j, JobDev* Jp, cudaStream_t st, int force) {
 // Updaters of a stride boundary (each gated on the device step), then
 // `steps` Langevin steps, then the step counter moves by `steps`.
 // Exact HI of a job above 128 beads: assemble D and factorise it in place in
-// 128 x 128 tiles, outer panel by outer panel (chol_w tile columns each).
-// The panel chain runs one stream priority above the caller's: inside an outer
-// panel, each tile column is brought up to date from the panel's earlier
-// columns (one long-K tensor-core pass per tile), its diagonal tile is
-// factorised in FP64 with the inverse of its factor, and the tiles below are
-// solved as a tensor-core product; then the trailing update of the next outer
-// panel's tile columns (K = this panel's columns).  The rest of the trailing
-// update runs at the caller's priority beside the next outer panel's chain,
-// and the chain waits for it before it touches columns that rest updated.
-// The caller's stream waits for both at the end.
+// 128 x 128 tiles (T tile columns), outer panel by outer panel (chol_w tile
+// columns each), on three streams by priority relative to the caller's:
+//   hp, two levels above: the chain of single tiles.  Per tile column J: the
+//     diagonal tile is brought up to date from the outer panel's earlier
+//     columns, factorised in FP64 with the inverse X_J of its factor (into
+//     the inverse buffer of J's parity), and the tile just below it is
+//     solved (L = A X_J^T on the tensor cores);
+//   ms, one level above: the rest of each tile column beside the chain --
+//     the tiles below the diagonal from the panel's earlier columns, then,
+//     once X_J is there, their solve;
+//   la, the caller's level: after an outer panel, the trailing update with
+//     K = its columns of every tile column beyond the next outer panel.
+// After an outer panel, the next one's tile columns get the finished panel's
+// K: the first diagonal tile on hp, the rest of the first tile column on ms
+// (the first solve waits for it), then the panel's other tile columns on ms.
+// Each tile receives the same updates (same tile kernel, same K ranges, same
+// order) as a serial sweep of the same outer panels gives it, so the factor
+// does not depend on how the streams interleave.  The caller's stream waits
+// for all three at the end.
 int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     GridAux& a = j->aux;
     const int n = j->n, m = 3 * n, T = chol_tiles(m), W = std::max(1, j->chol_w);
-    auto update = [&](cudaStream_t s, int jc0, int jc1, int k0, int k1) {
-        int tiles = 0;
-        for (int J = jc0; J < jc1; ++J) tiles += T - J;
+    // `tiles` tiles from (i0, jc0) in column order (column jc0 from row tile
+    // i0, then the following tile columns from their diagonal tiles)
+    auto update = [&](cudaStream_t s, int tiles, int jc0, int i0, int k0, int k1) {
         if (tiles > 0 && k1 > k0)
-            k_chol_tc<<<tiles, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_ten, Jp, a, jc0, k0, k1, kTcUpdate);
+            k_chol_tc<<<tiles, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_ten, Jp, a, jc0, i0, k0, k1, kTcUpdate);
+    };
+    auto tiles_from = [&](int jc0, int i0, int jc1) {   // column jc0 from i0, then whole columns up to jc1
+        int t = T - i0;
+        for (int J = jc0 + 1; J < jc1; ++J) t += T - J;
+        return t;
+    };
+    auto solve = [&](cudaStream_t s, int J, int i0, int i1) {
+        if (i1 > i0)
+            k_chol_tc<<<i1 - i0, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_linv, Jp, a, J, i0, J * kCT,
+                                                           (J + 1) * kCT, kTcSolve);
     };
     // priorities relative to the caller's stream (numerically smaller is
-    // higher): the chain one level above it, the trailing updates at it
+    // higher)
     int lo = 0, hi = 0, p = 0;
     CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     CUDA_TRY(cudaStreamGetPriority(st, &p));
     p = std::min(lo, std::max(hi, p));
-    auto level = [&](int prio) { return j->prio_st[std::min(sopb_job::kPrioLevels - 1, lo - prio)]; };
-    cudaStream_t hp = level(std::max(hi, p - 1)), la = level(p);
-    if (!hp || !la) return SOPB_ERR_CUDA;
-    CUDA_TRY(cudaEventRecord(j->hp_fork, st));
-    CUDA_TRY(cudaStreamWaitEvent(hp, j->hp_fork, 0));
+    auto idx = [&](int prio) { return std::min(sopb_job::kPrioLevels - 1, lo - std::max(hi, prio)); };
+    cudaStream_t hp = j->prio_st[idx(p - 2)], ms = j->mid_st[idx(p - 1)], la = j->prio_st[idx(p)];
+    if (!hp || !ms || !la) return SOPB_ERR_CUDA;
+    constexpr int R = sopb_job::kLkRing;
+    cudaEvent_t* e_pot = j->lk_ev;            // X_J written
+    cudaEvent_t* e_s1 = j->lk_ev + R;         // tile (J + 1, J) solved
+    cudaEvent_t* e_cu = j->lk_ev + 2 * R;     // tiles below (J, J) updated from the panel
+    cudaEvent_t* e_sr = j->lk_ev + 3 * R;     // tiles (J + 2.., J) solved
+    cudaEvent_t e_np1 = j->lk_ev[4 * R], e_np2 = j->lk_ev[4 * R + 1], ms_join = j->lk_ev[4 * R + 2];
+    auto rec = [](cudaEvent_t e, cudaStream_t s) { return cudaEventRecord(e, s); };
+    auto wait = [](cudaStream_t s, cudaEvent_t e) { return cudaStreamWaitEvent(s, e, 0); };
+
+    CUDA_TRY(rec(j->hp_fork, st));
+    CUDA_TRY(wait(hp, j->hp_fork));
+    CUDA_TRY(wait(ms, j->hp_fork));
     k_hi_assemble<<<dim3((n + 255) / 256, n), 256, 0, hp>>>(Jp, a);
-    bool rest_pending = false;   // a rest update on `la` that the next part must follow
+    bool rest_pending = false;   // a trailing update on la that the next outer panel must follow
     for (int P0 = 0; P0 < T; P0 += W) {
         const int P1 = std::min(T, P0 + W);
         for (int J = P0; J < P1; ++J) {
-            update(hp, J, J + 1, P0 * kCT, J * kCT);
+            // row J of the columns before J - 1 (solved on ms), and the
+            // inverse buffer of J's parity free again
+            if (J >= 2) CUDA_TRY(wait(hp, e_sr[(J - 2) % R]));
+            if (J > P0) {
+                if (J == P0 + 1 && P0 > 0) CUDA_TRY(wait(hp, e_np2));   // (J, J) got the last panel's K on ms
+                update(hp, 1, J, J, P0 * kCT, J * kCT);
+                if (J + 1 < T) {
+                    CUDA_TRY(wait(ms, e_s1[(J - 1) % R]));               // row J of column J - 1
+                    update(ms, T - J - 1, J, J + 1, P0 * kCT, J * kCT);
+                    CUDA_TRY(rec(e_cu[J % R], ms));
+                }
+            }
             k_chol_potrf64<<<1, kPotrfThreads, kPotrfSmem, hp>>>(Jp, a, J);
-            if (J + 1 < T)   // the tiles below: L_IJ = A_IJ X^T on the tensor cores
-                k_chol_tc<<<T - J - 1, kTcThreads, kTcSmem, hp>>>(j->tmap_ten, j->tmap_linv, Jp, a, J, J * kCT,
-                                                                    (J + 1) * kCT, kTcSolve);
+            CUDA_TRY(rec(e_pot[J % R], hp));
+            if (J + 1 < T) {
+                if (J > P0) CUDA_TRY(wait(hp, e_cu[J % R]));
+                else if (P0 > 0) CUDA_TRY(wait(hp, e_np1));             // (J + 1, J) got the last panel's K on ms
+                solve(hp, J, J + 1, J + 2);
+                CUDA_TRY(rec(e_s1[J % R], hp));
+            }
+            if (J + 2 < T) {
+                CUDA_TRY(wait(ms, e_pot[J % R]));
+                solve(ms, J, J + 2, T);
+                CUDA_TRY(rec(e_sr[J % R], ms));
+            }
         }
         if (P1 < T) {
+            // the finished panel's K for the next panel's tile columns, the
+            // earlier trailing update of those columns (on la) first
             const int Q1 = std::min(T, P1 + W);
-            CUDA_TRY(cudaEventRecord(j->la_fork, hp));                       // this outer panel is final
-            if (rest_pending) CUDA_TRY(cudaStreamWaitEvent(hp, j->la_join, 0));
-            update(hp, P1, Q1, P0 * kCT, P1 * kCT);                         // the next outer panel's columns
-            if (Q1 < T) {
-                CUDA_TRY(cudaStreamWaitEvent(la, j->la_fork, 0));
-                update(la, Q1, T, P0 * kCT, P1 * kCT);                      // the rest, beside the chain
-                CUDA_TRY(cudaEventRecord(j->la_join, la));
+            if (P1 >= 2) CUDA_TRY(wait(hp, e_sr[(P1 - 2) % R]));
+            if (rest_pending) CUDA_TRY(wait(hp, j->la_join));
+            update(hp, 1, P1, P1, P0 * kCT, P1 * kCT);
+            CUDA_TRY(wait(ms, e_s1[(P1 - 1) % R]));
+            if (rest_pending) CUDA_TRY(wait(ms, j->la_join));
+            update(ms, T - P1 - 1, P1, P1 + 1, P0 * kCT, P1 * kCT);
+            CUDA_TRY(rec(e_np1, ms));
+            if (Q1 > P1 + 1) update(ms, tiles_from(P1 + 1, P1 + 1, Q1), P1 + 1, P1 + 1, P0 * kCT, P1 * kCT);
+            CUDA_TRY(rec(e_np2, ms));
+            if (Q1 < T) {   // the tile columns beyond the next panel, beside it
+                CUDA_TRY(wait(la, e_s1[(P1 - 1) % R]));
+                CUDA_TRY(wait(la, e_sr[(P1 - 1) % R]));
+                update(la, tiles_from(Q1, Q1, T), Q1, Q1, P0 * kCT, P1 * kCT);
+                CUDA_TRY(rec(j->la_join, la));
                 rest_pending = true;
             }
         }
     }
-    CUDA_TRY(cudaEventRecord(j->hp_join, hp));
-    CUDA_TRY(cudaStreamWaitEvent(st, j->hp_join, 0));
-    if (rest_pending) CUDA_TRY(cudaStreamWaitEvent(st, j->la_join, 0));
+    CUDA_TRY(rec(j->hp_join, hp));
+    CUDA_TRY(rec(ms_join, ms));
+    CUDA_TRY(wait(st, j->hp_join));
+    CUDA_TRY(wait(st, ms_join));
+    if (rest_pending) CUDA_TRY(wait(st, j->la_join));
     CUDA_TRY(cudaGetLastError());
     return SOPB_OK;
 }
@@ -1457,10 +1532,7 @@ extern "C" int sopb_job_destroy(sopb_job* j) {
     // nothing waits here: graphs and memory are released after the job's
     // last work on its stream, the bead range and slot once it has finished
     for (auto& g : j->chunks) if (g.second) cudaGraphExecDestroy(g.second);
-    if (j->hi_streams) {   // released by the runtime once their work is done
-        for (cudaStream_t q : j->prio_st) if (q) cudaStreamDestroy(q);
-        for (cudaEvent_t e : {j->la_fork, j->la_join, j->hp_fork, j->hp_join}) cudaEventDestroy(e);
-    }
+    if (j->hi_streams) hi_streams_destroy(j);   // released by the runtime once their work is done
     SOPB_TRY(job_ev(j));
     CUDA_TRY(cudaStreamWaitEvent(c->io, j->ev, 0));
     if (j->amem) CUDA_TRY(cudaFreeAsync(j->amem, c->io));

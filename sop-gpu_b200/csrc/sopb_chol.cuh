@@ -89,7 +89,8 @@ k_hi_assemble(const JobDev* __restrict__ Jp, GridAux aux) {
 // the unused upper triangle of the tile, its diagonal beside it.  Tile loads
 // are issued unconditionally (clamped addresses), 32 per thread in flight.
 // Out: the factor (FP32) into the tensor's tile, X (FP32, zero above the
-// diagonal and outside nb) into aux.linv for the tile-column solve.  A
+// diagonal and outside nb) into the inverse buffer of J's parity (aux.linv
+// holds two) for the tile-column solves.  A
 // pivot that is not positive sets the job's status.
 constexpr int kPotrfThreads = 512;
 constexpr int kPotrfW = 8;                    // sub-panel width
@@ -201,6 +202,7 @@ k_chol_potrf64(JobDev* __restrict__ Jp, GridAux aux, int J) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int kPer = kCT * kCT / kPotrfThreads;     // tile entries per thread
     float* M = aux.tensor + (size_t)k * ld + k;
+    float* xout = aux.linv + (size_t)(J & 1) * kCT * kCT;   // two buffers: a solve may still read J - 1's
     {
         float v[kPer];
 #pragma unroll
@@ -335,7 +337,7 @@ k_chol_potrf64(JobDev* __restrict__ Jp, GridAux aux, int J) {
             lv[t] = (r < nb && q <= r) ? (float)P64[r * kPotrfLd + q] : 0.f;
             xv[t] = (r < nb && q < nb) ? (r == q ? (float)xd[r] : (r > q ? (float)P64[q * kPotrfLd + r] : 0.f)) : 0.f;
         }
-        *reinterpret_cast<float4*>(aux.linv + r * kCT + c) = make_float4(xv[0], xv[1], xv[2], xv[3]);
+        *reinterpret_cast<float4*>(xout + r * kCT + c) = make_float4(xv[0], xv[1], xv[2], xv[3]);
         if (r < nb) {
             float* dst = M + (size_t)r * ld + c;
             if (c + 4 <= nb) {
@@ -441,12 +443,12 @@ k_chol_apply_rows(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
 
 // ---- tile products on the tensor cores (tcgen05, TF32 x3, TMA-fed) ---------
 // One CTA per 128 x 128 output tile.  kTcUpdate: C_IJ -= sum over k in
-// [k0, k1) of P_Ik P_Jk^T for the lower tiles (I, J) of the tile columns
-// jc0, jc0 + 1, ... (I >= J, gridDim.x tiles in column order), P the factor's
-// columns k0..k1, lower entries of diagonal tiles only.  kTcSolve: C_IJ =
-// A_IJ X^T for the tiles below the diagonal tile of column jc0 (I = jc0 + 1 +
-// blockIdx.x), X = L_JJ^-1 from its own tensor map (the tile-column solve as
-// a product).
+// [k0, k1) of P_Ik P_Jk^T for lower tiles (I, J) in column order: column jc0
+// from row tile i0 down, then the tile columns jc0 + 1, ... from their
+// diagonal tiles down (gridDim.x tiles in all), P the factor's columns
+// k0..k1, lower entries of diagonal tiles only.  kTcSolve: C_IJ = A_IJ X^T
+// for the tiles I = i0 + blockIdx.x of column J = jc0, X = L_JJ^-1 from the
+// inverse buffer of J's parity (the tile-column solve as a product).
 // Pipeline over 32-column K chunks, three stages of 64 KB in shared memory:
 //   warp 9 (one thread) loads the chunk of both operands with two TMA tile
 //     loads (128 rows x 32 FP32, 128-byte swizzle) onto the stage's "loaded"
@@ -465,7 +467,8 @@ k_chol_apply_rows(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
 // loading and issuing, skips its C update and the job reports
 // SOPB_ERR_TIMEOUT.  The epilogue: warp w reads TMEM lanes 32 (w mod 4),
 // columns 64 (w / 4) onwards of every bank, sums the banks in FP32 and
-// updates 32 consecutive entries of one C row.
+// updates 64 consecutive entries of one C row, which an update loads into
+// registers before it waits for the last MMAs.
 enum { kTcUpdate = 0, kTcSolve = 1 };
 constexpr int kTcKC = 32;                                 // K columns per stage (128 B of FP32)
 constexpr int kTcStages = 3;
@@ -524,7 +527,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_b,
-          JobDev* __restrict__ Jp, GridAux aux, int jc0, int k0, int k1, int mode) {
+          JobDev* __restrict__ Jp, GridAux aux, int jc0, int i0, int k0, int k1, int mode) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ int stop;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -535,19 +538,21 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
     int I, J;
     if (mode == kTcSolve) {
         J = jc0;
-        I = jc0 + 1 + blockIdx.x;
+        I = i0 + blockIdx.x;
     } else {
-        int b = blockIdx.x;
+        int b = blockIdx.x, top = i0;
         J = jc0;
-        while (J < T - 1 && b >= T - J) {
-            b -= T - J;
+        while (J < T - 1 && b >= T - top) {
+            b -= T - top;
             ++J;
+            top = J;
         }
-        I = J + b;
+        I = top + b;
     }
     const int r0 = I * kCT, c0 = J * kCT;
-    // B operand rows and the column of its first chunk
-    const int b_row = mode == kTcSolve ? 0 : c0, b_col = mode == kTcSolve ? 0 : k0;
+    // B operand rows and the column of its first chunk (the solve: the
+    // inverse buffer of J's parity, rows 128 (J & 1) of its map)
+    const int b_row = mode == kTcSolve ? (J & 1) * kCT : c0, b_col = mode == kTcSolve ? 0 : k0;
     const int nk = (k1 - k0 + kTcKC - 1) / kTcKC;
 
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tc_smem);
@@ -664,6 +669,19 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
             asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(converted(s)) : "memory");
         }
     }
+    // an update's C entries of this thread, loaded while the last MMAs run
+    // (C is neither operand: the K columns lie left of the tile)
+    float4 cpre[16];
+    if (warp < 8 && mode == kTcUpdate) {
+        const int gr = r0 + 32 * (warp & 3) + lane;
+        const float* src = aux.tensor + (size_t)min(gr, m - 1) * ld + c0 + 64 * (warp >> 2);
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            const int gc = c0 + 64 * (warp >> 2) + 4 * q;
+            cpre[q] = (gr < m && gc + 3 <= gr && gc + 3 < m) ? *reinterpret_cast<const float4*>(src + 4 * q)
+                                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
     // epilogue: wait for the MMAs (every thread, bounded), then update C
     const bool done = mbar_wait(done_bar, 0u, nullptr);
     const bool ok = __syncthreads_and(done && !*abort_flag) != 0;
@@ -672,6 +690,7 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
         const int hh = nk < 3 ? nk : 3;
         const int lrow = 32 * (warp & 3) + lane, gr = r0 + lrow;
         const int cmax = mode == kTcSolve ? min(m, c0 + kCT) : m;
+#pragma unroll
         for (int ch = 0; ch < 2; ++ch) {
             const int col = 64 * (warp >> 2) + 32 * ch;
             float sum[32];
@@ -710,7 +729,7 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
 #pragma unroll
                     for (int e = 0; e < 32; e += 4) {
                         if (gc + e + 3 <= gr && gc + e + 3 < m) {
-                            float4 x = *reinterpret_cast<float4*>(dst + e);
+                            float4 x = cpre[8 * ch + e / 4];
                             x.x -= sum[e];
                             x.y -= sum[e + 1];
                             x.z -= sum[e + 2];

@@ -37,7 +37,7 @@ struct GridAux {
     double* beta;        // beta' of the job (TEA), FP64
     float* tensor;       // Cholesky: (3n)^2 matrix, row-major
     int32_t ld;          // leading dimension of `tensor`
-    float* linv;         // blocked Cholesky: inverse of the last diagonal tile's factor, 128 x 128
+    float* linv;         // blocked Cholesky: inverses of the last two diagonal tiles' factors, 2 x 128 x 128
     // reductions
     float4* part;        // per-CTA partial sums
     int32_t npart;

@@ -82,6 +82,34 @@ def test_blocked_factor_matches_fp64_cholesky(gpu_ctx, n):
     g.destroy()
 
 
+@pytest.mark.parametrize("w", [1, 2, 3, 4, 8])
+def test_blocked_factor_panel_widths(w):
+    # the factorisation's three streams (single-tile chain, tile-column rest,
+    # trailing updates) for several outer-panel widths at 17 tile columns:
+    # the factor against FP64, and bit-identical when the same job runs
+    # again beside another exact-HI job, so that the streams interleave
+    # differently
+    n = 700
+    sp = hi_spec(n, 47, "free", hi_exact=1)
+    with sopb.Context(0) as ctx:
+        ctx.set_hi_policy(w, 8)
+        g = ctx.job(sp)
+        x0 = g.read(sopb.COORDS)[:, :3].copy()
+        ctx.run([g], 1)                       # step 0 factorises D at x0
+        assert g.status() == 0
+        L1 = np.tril(g.read(sopb.HIFACTOR))
+        g2 = ctx.job(sp)
+        other = ctx.job(hi_spec(900, 5, "free", hi_exact=1))
+        ctx.run([g2, other], 1)
+        assert g2.status() == 0 and other.status() == 0
+        L2 = np.tril(g2.read(sopb.HIFACTOR))
+    assert np.array_equal(L1, L2)
+    L = L1.astype(np.float64)
+    D = O.rpy_tensor(x0, sp.params.hi_a)
+    assert np.max(np.abs(L - np.linalg.cholesky(D))) < 2e-4
+    assert np.linalg.norm(L @ L.T - D) / np.linalg.norm(D) < 2e-6
+
+
 @pytest.mark.parametrize("n,refresh", [(150, 1), (300, 1), (300, 10), (100, 10)])
 def test_exact_hi_with_refresh_tracks_oracle(gpu_ctx, n, refresh):
     # the blocked factorisation above 128 beads and the refresh updater on

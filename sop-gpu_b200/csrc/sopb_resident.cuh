@@ -38,8 +38,10 @@ constexpr int kMaxResidentBeads = 2048;
 constexpr int kResidentSmemPerBead = 57;
 
 // Shared-memory layout of a resident launch (byte offsets, 16-B aligned
-// arrays).  The bonded maps (covalent and native CSR with parameters) are
-// copied in when `bonded` is set; the Verlet cache takes `cache` u16 entries.
+// arrays).  The coordinates are followed by one far-away dummy bead that the
+// padding of the Verlet cache points at.  The bonded maps (covalent and
+// native CSR with parameters) are copied in when `bonded` is set; the Verlet
+// cache takes `cache` u16 entries.
 struct ResidentLayout {
     size_t x, F, sd, nat_par, Ts, off, cov_off, nat_off, cov_r0, cov_j, nat_j, flags, nbr, total;
 };
@@ -48,7 +50,7 @@ __host__ __device__ inline ResidentLayout resident_layout(int n, int ncov, int n
     ResidentLayout L;
     const size_t b = bonded ? 1 : 0;
     size_t o = 0;
-    L.x = o;        o = align16(o + (size_t)n * 16);
+    L.x = o;        o = align16(o + (size_t)(n + 1) * 16);
     L.F = o;        o = align16(o + (size_t)n * 16);
     L.sd = o;       o = align16(o + (size_t)n * 16);
     L.nat_par = o;  o = align16(o + b * (size_t)nnat * 8);
@@ -154,13 +156,46 @@ __device__ __forceinline__ void pair_run(const JobDev& J, const float4* __restri
     for (; k < cnt; k += lpb) pair_term(xi, xs[r[k]], c8, cut2, f);
 }
 
+// The shared-memory cache of a bead's Verlet row: byte offsets of the
+// partners' coordinates (16 j), the row padded to a multiple of four entries
+// with the offset of the dummy bead, whose term is exactly zero (+0 or -0
+// added).  Each full block of 4 lpb entries is stored lane by lane -- the
+// four entries l, l + lpb, l + 2 lpb, l + 3 lpb of lane l side by side -- so
+// that one 8-byte load fetches them; the rest of the row is in row order.
+// A lane therefore visits the same entries in the same order as pair_run.
+__device__ __forceinline__ int cache_pos(int k, int full, int lg) {
+    if (k >= full) return k;
+    const int blk = 4 << lg, b = k & ~(blk - 1), w = k & (blk - 1);
+    return b + 4 * (w & ((1 << lg) - 1)) + (w >> lg);
+}
+__device__ __forceinline__ void pair_run_cached(const JobDev& J, const float4* __restrict__ xs,
+                                                const uint16_t* __restrict__ rb, int cnt, float4 xi, int l, int lpb,
+                                                float3& f) {
+    const float c8 = J.c8, cut2 = J.cut2;
+    const char* xb = reinterpret_cast<const char*>(xs);
+    const int blk = 4 * lpb, full = cnt - cnt % blk;
+    const uint16_t* q = rb + 4 * l;
+    for (int b = 0; b < full; b += blk, q += blk) {
+        const uint2 o = *reinterpret_cast<const uint2*>(q);
+        const float4 x0 = *reinterpret_cast<const float4*>(xb + (o.x & 0xffffu));
+        const float4 x1 = *reinterpret_cast<const float4*>(xb + (o.x >> 16));
+        const float4 x2 = *reinterpret_cast<const float4*>(xb + (o.y & 0xffffu));
+        const float4 x3 = *reinterpret_cast<const float4*>(xb + (o.y >> 16));
+        pair_term(xi, x0, c8, cut2, f);
+        pair_term(xi, x1, c8, cut2, f);
+        pair_term(xi, x2, c8, cut2, f);
+        pair_term(xi, x3, c8, cut2, f);
+    }
+    for (int k = full + l; k < cnt; k += lpb) pair_term(xi, *reinterpret_cast<const float4*>(xb + rb[k]), c8, cut2, f);
+}
+
 __device__ __forceinline__ void pairs_partial(const JobDev& J, const float4* __restrict__ xs, const int32_t* off,
                                               const uint16_t* nbr, int cap, int i, float4 xi, int l, int lpb,
                                               float3& f) {
     const int k1 = off ? off[i + 1] : 0x7fffffff;
     if (k1 <= cap) {
         const int k0 = off[i];
-        pair_run(J, xs, nbr + k0, k1 - k0, xi, l, lpb, f);
+        pair_run_cached(J, xs, nbr + k0, k1 - k0, xi, l, lpb, f);
     } else {
         pair_run(J, xs, J.pl_j + (size_t)i * J.cap_pl, J.pl_cnt[i], xi, l, lpb, f);
     }
@@ -465,14 +500,18 @@ __device__ __noinline__ void tip_update(const JobDev& J, StepScalars& sc, float3
 }
 
 // Shared-memory cache of the Verlet rows as compact CSR: offsets by a CTA
-// scan of the row counts, then the entries as u16 for every bead whose row
-// ends within `cap` entries (the beads after it read their global rows).
+// scan of the row counts padded to multiples of four, then for every bead
+// whose padded row ends within `cap` entries its row in the layout that
+// pair_run_cached reads (the beads after it read their global rows).  The
+// dummy bead sits at index n, far from every bead.
 template <int BLOCK>
-__device__ void fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap, int* tot_smem) {
+__device__ void fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap, int* tot_smem, float4* xs) {
     const int n = J.n, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int per = (n + BLOCK - 1) / BLOCK, b0 = tid * per, b1 = min(n, b0 + per);
+    auto padded = [](int c) { return (c + 3) & ~3; };
+    if (tid == 0) xs[n] = make_float4(1.0e18f, 1.0e18f, 1.0e18f, 0.f);
     int s = 0;
-    for (int i = b0; i < b1; ++i) s += J.pl_cnt[i];
+    for (int i = b0; i < b1; ++i) s += padded(J.pl_cnt[i]);
     int incl = s;
     for (int o = 1; o < 32; o <<= 1) {
         const int t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -488,32 +527,35 @@ __device__ void fill_cache(const JobDev& J, int32_t* off, uint16_t* nbr, int cap
     }
     __syncthreads();
     int run = wsum[w] + incl - s;
-    for (int i = b0; i < b1; ++i) { off[i] = run; run += J.pl_cnt[i]; }
+    for (int i = b0; i < b1; ++i) { off[i] = run; run += padded(J.pl_cnt[i]); }
     if (tid == 0) off[n] = *tot_smem;
     __syncthreads();
     {
+        const int lg = __ffs(J.lpb) - 1, blk = 4 << lg;
+        const uint16_t dummy = (uint16_t)(16 * n);
         // two beads per warp at a time, so that the loads of both rows are
         // in flight together
         for (int i = w; i < n; i += 2 * (BLOCK / 32)) {
             const int i2 = i + BLOCK / 32;
             const bool in1 = off[i + 1] <= cap, in2 = i2 < n && off[i2 + 1] <= cap;
-            const int k0 = off[i], cnt = in1 ? off[i + 1] - k0 : 0;
-            const int k02 = in2 ? off[i2] : 0, cnt2 = in2 ? off[i2 + 1] - k02 : 0;
+            const int k0 = off[i], pc = in1 ? off[i + 1] - k0 : 0, cnt = in1 ? J.pl_cnt[i] : 0;
+            const int k02 = in2 ? off[i2] : 0, pc2 = in2 ? off[i2 + 1] - k02 : 0, cnt2 = in2 ? J.pl_cnt[i2] : 0;
+            const int full = pc - pc % blk, full2 = pc2 - pc2 % blk;
             const int32_t* r = J.pl_j + (size_t)i * J.cap_pl;
             const int32_t* r2 = J.pl_j + (size_t)(in2 ? i2 : i) * J.cap_pl;
-            for (int kb = 0; kb < max(cnt, cnt2); kb += 128) {
+            for (int kb = 0; kb < max(pc, pc2); kb += 128) {
                 int v[4], v2[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = kb + 32 * u + lane;
-                    v[u] = k < cnt ? r[k] : 0;
-                    v2[u] = k < cnt2 ? r2[k] : 0;
+                    v[u] = k < cnt ? r[k] : n;
+                    v2[u] = k < cnt2 ? r2[k] : n;
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int k = kb + 32 * u + lane;
-                    if (k < cnt) nbr[k0 + k] = (uint16_t)v[u];
-                    if (k < cnt2) nbr[k02 + k] = (uint16_t)v2[u];
+                    if (k < pc) nbr[k0 + cache_pos(k, full, lg)] = k < cnt ? (uint16_t)(16 * v[u]) : dummy;
+                    if (k < pc2) nbr[k02 + cache_pos(k, full2, lg)] = k < cnt2 ? (uint16_t)(16 * v2[u]) : dummy;
                 }
             }
             if (!in2) break;   // every later bead ends beyond the cache as well
@@ -650,7 +692,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
     }
     __syncthreads();
     const int cap = J.lcache;
-    fill_cache<BLOCK>(J, off, nbr, cap, &list_total);
+    fill_cache<BLOCK>(J, off, nbr, cap, &list_total, xs);
 
     const int lpb = J.lpb, l = tid % lpb;
     int err = 0;
@@ -661,7 +703,7 @@ k_resident_steps(JobDev* __restrict__ jobs, const int32_t* __restrict__ ids, con
     __syncthreads();
     for (int64_t s = 0; s < nsteps; ++s, ++step) {
         if (phase == 0 && run_updaters<BLOCK>(J, sc, xs, Ts, red, step, err))
-            fill_cache<BLOCK>(J, off, nbr, cap, &list_total);
+            fill_cache<BLOCK>(J, off, nbr, cap, &list_total, xs);
         if (++phase == J.stride) phase = 0;
         int* counter = &next_bead[s & 1];
         // forces: each warp claims one bead per lane group from a shared

@@ -206,8 +206,10 @@ struct sopb_job {
     cudaEvent_t lk_ev[4 * kLkRing + 3] = {};
     int jsplit = 1;                    // j slices of the O(N^2) HI sums
     int chol_w = kCholPanelTiles;      // exact HI: outer-panel width of the factorisation, tile columns
-    CUtensorMap tmap_ten{};            // exact HI: TMA maps of the tensor and of the diagonal tile's
-    CUtensorMap tmap_linv{};           //   inverse (128 x 32 FP32 boxes, 128-byte swizzle)
+    CUtensorMap tmap_ten{};            // exact HI: TMA maps of the tensor, of the diagonal tiles'
+    CUtensorMap tmap_linv{};           //   inverses and of the TF32 hi and lo planes of the solved
+    CUtensorMap tmap_phi{};            //   tiles (128 x 32 FP32 boxes, 128-byte swizzle)
+    CUtensorMap tmap_plo{};
     uint32_t log_tail = 0;             // event-log rows drained so far
     bool ev_lazy = false;              // ev not yet recorded after the work on st (see job_ev)
 };
@@ -711,13 +713,14 @@ int encode_tmap_f32(CUtensorMap* map, float* base, int rows, int cols, int ld) {
 struct GridLayout {
     int npart = 0, jsplit = 1, cap_nr = 0, ld = 0;
     bool cells = false, hi = false, exact = false, blocked = false;
-    size_t part = 0, rf = 0, mf = 0, xc = 0, ci = 0, eps = 0, ten = 0, linv = 0, geo = 0;
+    int plane_rows = 0, plane_ld = 0;
+    size_t part = 0, rf = 0, mf = 0, xc = 0, ci = 0, eps = 0, ten = 0, linv = 0, phi = 0, plo = 0, geo = 0;
     size_t cc = 0, cs = 0, cb = 0, bc = 0, near = 0, nrj = 0, nrc = 0, xref = 0;
     size_t total = 0;
 };
 
 GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp, int64_t cap_pl,
-                       int hi_cps = kHiCtasPerSm) {
+                       int hi_cps = kHiCtasPerSm, int chol_w = kCholPanelTiles) {
     GridLayout L;
     L.npart = (int)std::min<int64_t>((n + kGridBlock - 1) / kGridBlock, (int64_t)sms * 8);
     L.cells = p.cell_list == 1 || (p.cell_list == 0 && n > 16384);
@@ -739,7 +742,16 @@ GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp,
         if (L.exact) {
             L.ld = L.blocked ? chol_ld((int)n) : (int)(3 * n);
             L.ten = take((size_t)3 * n * L.ld * 4);
-            if (L.blocked) L.linv = take((size_t)2 * kCT * kCT * 4);
+            if (L.blocked) {
+                // the inverse buffers, and the TF32 hi and lo planes of two
+                // outer panels (tile rows x 128 rows each, the panel's columns)
+                const int T = chol_tiles((int)(3 * n));
+                L.plane_rows = T * kCT;
+                L.plane_ld = std::min(std::max(1, chol_w), T) * kCT;
+                L.linv = take((size_t)2 * kCT * kCT * 4);
+                L.phi = take((size_t)2 * L.plane_rows * L.plane_ld * 4);
+                L.plo = take((size_t)2 * L.plane_rows * L.plane_ld * 4);
+            }
         }
     }
     L.geo = take(8 * sizeof(float));
@@ -764,7 +776,8 @@ GridLayout grid_layout(const sopb_params& p, int64_t n, int sms, int64_t cap_pp,
 // pool), reduction partials and, for large jobs, the cell list.
 int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, int32_t cap_pp, int32_t cap_pl) {
     GridAux& a = j->aux;
-    const GridLayout L = grid_layout(p, n, c->sm_count, cap_pp, cap_pl, c->policy.hi_ctas_per_sm);
+    const GridLayout L = grid_layout(p, n, c->sm_count, cap_pp, cap_pl, c->policy.hi_ctas_per_sm,
+                                     c->policy.chol_panel_tiles);
     j->bead_blocks = L.npart;
     j->jsplit = L.jsplit;
     j->chol_w = c->policy.chol_panel_tiles;
@@ -789,8 +802,17 @@ int grid_alloc(sopb_context* c, sopb_job* j, const sopb_params& p, int32_t n, in
         if (L.blocked) {
             const int m = 3 * n;
             a.linv = (float*)(b + L.linv);
+            a.plane_hi = (float*)(b + L.phi);
+            a.plane_lo = (float*)(b + L.plo);
+            a.plane_rows = L.plane_rows;
+            a.plane_ld = L.plane_ld;
+            // rows below the matrix in the planes are read (and discarded)
+            // by the last tile row's updates: zero from the start
+            CUDA_TRY(cudaMemsetAsync(b + L.phi, 0, L.plo + (size_t)2 * L.plane_rows * L.plane_ld * 4 - L.phi, c->upload));
             SOPB_TRY(encode_tmap_f32(&j->tmap_ten, a.tensor, m, m, a.ld));
             SOPB_TRY(encode_tmap_f32(&j->tmap_linv, a.linv, 2 * kCT, kCT, kCT));
+            SOPB_TRY(encode_tmap_f32(&j->tmap_phi, a.plane_hi, 2 * L.plane_rows, L.plane_ld, L.plane_ld));
+            SOPB_TRY(encode_tmap_f32(&j->tmap_plo, a.plane_lo, 2 * L.plane_rows, L.plane_ld, L.plane_ld));
             // two streams per priority level, made here rather than during
             // a stream capture
             j->hi_streams = true;
@@ -876,7 +898,7 @@ int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     // i0, then the following tile columns from their diagonal tiles)
     auto update = [&](cudaStream_t s, int tiles, int jc0, int i0, int k0, int k1) {
         if (tiles > 0 && k1 > k0)
-            k_chol_tc<<<tiles, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_ten, Jp, a, jc0, i0, k0, k1, kTcUpdate);
+            k_chol_tc<<<tiles, kTcThreads, kTcSmem, s>>>(j->tmap_phi, j->tmap_plo, Jp, a, jc0, i0, k0, k1, kTcUpdate, W);
     };
     auto tiles_from = [&](int jc0, int i0, int jc1) {   // column jc0 from i0, then whole columns up to jc1
         int t = T - i0;
@@ -886,7 +908,7 @@ int chol_refresh(sopb_job* j, JobDev* Jp, cudaStream_t st) {
     auto solve = [&](cudaStream_t s, int J, int i0, int i1) {
         if (i1 > i0)
             k_chol_tc<<<i1 - i0, kTcThreads, kTcSmem, s>>>(j->tmap_ten, j->tmap_linv, Jp, a, J, i0, J * kCT,
-                                                           (J + 1) * kCT, kTcSolve);
+                                                           (J + 1) * kCT, kTcSolve, W);
     };
     // priorities relative to the caller's stream (numerically smaller is
     // higher)

@@ -446,17 +446,23 @@ k_chol_apply_rows(JobDev* __restrict__ Jp, GridAux aux, int jsplit) {
 // [k0, k1) of P_Ik P_Jk^T for lower tiles (I, J) in column order: column jc0
 // from row tile i0 down, then the tile columns jc0 + 1, ... from their
 // diagonal tiles down (gridDim.x tiles in all), P the factor's columns
-// k0..k1, lower entries of diagonal tiles only.  kTcSolve: C_IJ = A_IJ X^T
-// for the tiles I = i0 + blockIdx.x of column J = jc0, X = L_JJ^-1 from the
-// inverse buffer of J's parity (the tile-column solve as a product).
+// k0..k1 (one outer panel's, read from its TF32 hi and lo planes through
+// tmap_a and tmap_b), lower entries of diagonal tiles only.  kTcSolve: C_IJ
+// = A_IJ X^T for the tiles I = i0 + blockIdx.x of column J = jc0 (A from
+// the tensor through tmap_a), X = L_JJ^-1 from the inverse buffer of J's
+// parity (tmap_b) -- the tile-column solve as a product; the solved tile
+// goes to the tensor and, split into TF32 hi and lo, to the planes of its
+// outer panel (pw tile columns per panel) for the updates that read it.
 // Pipeline over 32-column K chunks, three stages of 64 KB in shared memory:
-//   warp 9 (one thread) loads the chunk of both operands with two TMA tile
-//     loads (128 rows x 32 FP32, 128-byte swizzle) onto the stage's "loaded"
-//     mbarrier;
-//   warps 0-7 split each value p into TF32 p_hi = rn(p), written back in
-//     place, and p_lo = rn(p - p_hi), written beside it in the same swizzled
-//     layout, then arrive on the stage's "converted" mbarrier;
-//   warp 8 (one thread) issues 12 MMAs per chunk (4 K steps of 8; hi.hi into
+//   warp 9 (one thread) loads the chunk onto the stage's "loaded" mbarrier:
+//     an update four TMA tile loads (hi and lo of both operands), a solve
+//     two (128 rows x 32 FP32 each, 128-byte swizzle);
+//   for a solve, warps 0-7 split each value p into TF32 p_hi = rn(p),
+//     written back in place, and p_lo = rn(p - p_hi), written beside it in
+//     the same swizzled layout, then arrive on the stage's "converted"
+//     mbarrier (an update's operands arrive split);
+//   warp 8 (one thread) waits for the stage ("loaded" for an update,
+//     "converted" for a solve) and issues 12 MMAs per chunk (4 K steps of 8; hi.hi into
 //     one of three accumulator banks in turn, hi.lo + lo.hi into a fourth,
 //     so that no bank accumulates a long K: the tensor cores' FP32
 //     accumulation truncates) and commits them to the stage's "empty"
@@ -527,7 +533,7 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
 
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_b,
-          JobDev* __restrict__ Jp, GridAux aux, int jc0, int i0, int k0, int k1, int mode) {
+          JobDev* __restrict__ Jp, GridAux aux, int jc0, int i0, int k0, int k1, int mode, int pw) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ int stop;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -550,9 +556,13 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
         I = top + b;
     }
     const int r0 = I * kCT, c0 = J * kCT;
-    // B operand rows and the column of its first chunk (the solve: the
-    // inverse buffer of J's parity, rows 128 (J & 1) of its map)
-    const int b_row = mode == kTcSolve ? (J & 1) * kCT : c0, b_col = mode == kTcSolve ? 0 : k0;
+    // operand rows and the column of the first chunk: an update reads the
+    // planes of the outer panel holding columns k0..k1 (rows by the panel's
+    // parity, columns from the panel's first); a solve reads A_IJ from the
+    // tensor and X from the inverse buffer of J's parity (rows 128 (J & 1))
+    const int upan = (k0 / kCT) / pw, ubase = (upan & 1) * aux.plane_rows;
+    const int a_row = mode == kTcSolve ? r0 : ubase + r0, a_col = mode == kTcSolve ? k0 : k0 - upan * pw * kCT;
+    const int b_row = mode == kTcSolve ? (J & 1) * kCT : ubase + c0, b_col = mode == kTcSolve ? 0 : a_col;
     const int nk = (k1 - k0 + kTcKC - 1) / kTcKC;
 
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tc_smem);
@@ -598,17 +608,24 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
                 }
                 const uint32_t st = sbuf + s * kTcStage;
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(loaded(s)),
-                             "r"(2 * kTcPart)
+                             "r"((mode == kTcSolve ? 2 : 4) * kTcPart)
                              : "memory");
-                tma_load_2d(st, &tmap_a, k0 + c * kTcKC, r0, loaded(s));
-                tma_load_2d(st + kTcPart, &tmap_b, b_col + c * kTcKC, b_row, loaded(s));
+                if (mode == kTcSolve) {
+                    tma_load_2d(st, &tmap_a, a_col + c * kTcKC, a_row, loaded(s));
+                    tma_load_2d(st + kTcPart, &tmap_b, b_col + c * kTcKC, b_row, loaded(s));
+                } else {   // hi of A and B from tmap_a, lo of A and B from tmap_b
+                    tma_load_2d(st, &tmap_a, a_col + c * kTcKC, a_row, loaded(s));
+                    tma_load_2d(st + kTcPart, &tmap_a, b_col + c * kTcKC, b_row, loaded(s));
+                    tma_load_2d(st + 2 * kTcPart, &tmap_b, a_col + c * kTcKC, a_row, loaded(s));
+                    tma_load_2d(st + 3 * kTcPart, &tmap_b, b_col + c * kTcKC, b_row, loaded(s));
+                }
             }
         }
     } else if (warp == 8) {
         if (lane == 0) {
             for (int c = 0; c < nk; ++c) {
                 const int s = c % kTcStages, round = c / kTcStages;
-                if (!mbar_wait(converted(s), (uint32_t)(round & 1), abort_flag)) {
+                if (!mbar_wait(mode == kTcSolve ? converted(s) : loaded(s), (uint32_t)(round & 1), abort_flag)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -640,9 +657,10 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
                          : "memory");
         }
     } else {
-        // converters: item u of thread tid covers row 8 g + r, 16-byte chunk q
-        // (swizzled position q ^ r); lanes r = 0..7 of one chunk hit eight banks
-        for (int c = 0; c < nk; ++c) {
+        // converters (a solve's operands only): item u of thread tid covers
+        // row 8 g + r, 16-byte chunk q (swizzled position q ^ r); lanes r =
+        // 0..7 of one chunk hit eight banks
+        for (int c = 0; c < (mode == kTcSolve ? nk : 0); ++c) {
             const int s = c % kTcStages, round = c / kTcStages;
             if (!mbar_wait(loaded(s), (uint32_t)(round & 1), abort_flag)) {
                 *abort_flag = 1;
@@ -715,14 +733,32 @@ k_chol_tc(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CU
                 const int gc = c0 + col;
                 float* dst = aux.tensor + (size_t)gr * ld + gc;
                 if (mode == kTcSolve) {
+                    // the tile's outer panel: its planes' rows and first column
+                    const int span = J / pw;
+                    const size_t po = (size_t)((span & 1) * aux.plane_rows + gr) * aux.plane_ld + (gc - span * pw * kCT);
+                    float* ph = aux.plane_hi + po;
+                    float* pl = aux.plane_lo + po;
 #pragma unroll
                     for (int e = 0; e < 32; e += 4) {
+                        float hv[4], lv[4];
+#pragma unroll
+                        for (int w = 0; w < 4; ++w) {
+                            const uint32_t h = tf32_rn(sum[e + w]);
+                            hv[w] = __uint_as_float(h);
+                            lv[w] = __uint_as_float(tf32_rn(sum[e + w] - hv[w]));
+                        }
                         if (gc + e + 3 < cmax) {
                             *reinterpret_cast<float4*>(dst + e) = make_float4(sum[e], sum[e + 1], sum[e + 2], sum[e + 3]);
+                            *reinterpret_cast<float4*>(ph + e) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+                            *reinterpret_cast<float4*>(pl + e) = make_float4(lv[0], lv[1], lv[2], lv[3]);
                         } else {
 #pragma unroll
                             for (int w = 0; w < 4; ++w)
-                                if (gc + e + w < cmax) dst[e + w] = sum[e + w];
+                                if (gc + e + w < cmax) {
+                                    dst[e + w] = sum[e + w];
+                                    ph[e + w] = hv[w];
+                                    pl[e + w] = lv[w];
+                                }
                         }
                     }
                 } else {

@@ -38,6 +38,10 @@ struct GridAux {
     float* tensor;       // Cholesky: (3n)^2 matrix, row-major
     int32_t ld;          // leading dimension of `tensor`
     float* linv;         // blocked Cholesky: inverses of the last two diagonal tiles' factors, 2 x 128 x 128
+    float* plane_hi;     // blocked Cholesky: the solved tiles of the last two outer panels split into
+    float* plane_lo;     //   TF32 hi and lo (bit patterns), [2 * plane_rows][plane_ld], by panel parity
+    int32_t plane_rows;  // tile rows x 128
+    int32_t plane_ld;    // outer-panel width in columns
     // reductions
     float4* part;        // per-CTA partial sums
     int32_t npart;

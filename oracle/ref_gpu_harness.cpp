@@ -1,7 +1,7 @@
 // ref_gpu_harness.cpp — drives the reference's own CUDA path (compiled from
 // the SOP-GPU source tree by oracle/build_ref.sh) for a given config and
-// dumps state at chosen steps.  Used on the GPU box to make golden fixtures
-// of the reference itself.  TEST INFRASTRUCTURE ONLY.
+// dumps state at chosen steps.  Run on a B200 to make golden fixtures of
+// the reference itself.  TEST INFRASTRUCTURE ONLY.
 //
 //   ref_gpu <config.sop> <outdir> <total_steps> <dump steps...>
 //

@@ -492,6 +492,7 @@ extern "C" int sopb_context_create(int32_t device, void* stream, sopb_context** 
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_potrf64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrfSmem));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+    CUDA_TRY(cudaFuncSetAttribute(k_chol_factor_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem));
     CUDA_TRY(cudaFuncSetAttribute(k_chol_apply_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kCholMaxBeads * 12));
     CUDA_TRY(cudaDeviceGetAttribute(&c->smem_reserved, cudaDevAttrReservedSharedMemoryPerBlock, device));
     *out = c;
@@ -1062,8 +1063,10 @@ int grid_launch(sopb_job* j, cudaStream_t st, bool updaters, int steps, int due 
             k_hi_prepare<<<nb, kGridBlock, 0, st>>>(Jp, a);
             if (j->n <= 128) {
                 k_chol_D<<<nb, kGridBlock, 0, st>>>(Jp, a, refresh ? 1 : 0);
-                if (refresh) k_chol_factor_small<<<1, 384, 0, st>>>(Jp, a);
-                k_chol_apply<<<nb, kGridBlock, 0, st>>>(Jp, a);
+                if (refresh && j->h.hi_bmode == SOPB_HI_B_REFCOMPAT) k_chol_factor_small<<<1, 384, 0, st>>>(Jp, a);
+                else if (refresh) k_chol_factor_panels<<<1, kSmallThreads, kSmallSmem, st>>>(Jp, a);
+                if (j->h.hi_bmode == SOPB_HI_B_REFCOMPAT) k_chol_apply<<<nb, kGridBlock, 0, st>>>(Jp, a);
+                else k_chol_apply_warp<<<(j->n + kApplyWarps - 1) / kApplyWarps, 32 * kApplyWarps, 0, st>>>(Jp, a);
             } else {
                 const dim3 tg((j->n + kHiTile - 1) / kHiTile, j->jsplit);
                 k_hi_df_partial<<<tg, kHiTile, 0, st>>>(Jp, a, j->jsplit);

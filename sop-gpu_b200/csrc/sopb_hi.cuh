@@ -362,6 +362,124 @@ k_chol_factor_small(JobDev* __restrict__ Jp, GridAux aux) {
     }
 }
 
+// The true factor L of D at n <= 128 (B = L), the same factorisation as
+// integrateCholesky_decompose (bdhitea_kernel.cu:154-190) in another order:
+// right-looking in 32-column panels, in one CTA.  The panel (its rows from
+// the diagonal down, at most 384 x 32) is factorised column by column with
+// one thread per row holding the row in registers (IEEE square root and
+// division, two barriers per column); it is written back, and the lower
+// triangle of the trailing matrix takes the panel's rank-32 update from L2
+// in 4 x 4 register tiles.  Only the lower triangle is written (the
+// reference also mirrors the factor into the upper one, which its
+// symmetrised noise matrix reads; that mode keeps k_chol_factor_small).
+constexpr int kSmallPanel = 32;
+constexpr int kSmallThreads = 512;                        // at least kSmallRows: one thread per panel row
+constexpr int kSmallRows = 384;                            // 3n for n <= 128
+constexpr int kSmallLd = kSmallPanel + 1;                  // floats per panel row in shared memory
+constexpr size_t kSmallSmem = (size_t)kSmallRows * kSmallLd * sizeof(float);
+static_assert(kSmallThreads >= kSmallRows, "one thread per panel row");
+
+__global__ void __launch_bounds__(kSmallThreads)
+k_chol_factor_panels(JobDev* __restrict__ Jp, GridAux aux) {
+    extern __shared__ float P[];                           // [rows][kSmallLd]
+    __shared__ float diag[kSmallPanel];
+    __shared__ float col_s[kSmallRows];                    // the scaled column of the panel
+    __shared__ float piv_s;
+    if (Jp->status) return;
+    const int m = 3 * Jp->n, ld = aux.ld, tid = threadIdx.x;
+    float* M = aux.tensor;
+    for (int p0 = 0; p0 < m; p0 += kSmallPanel) {
+        const int pb = min(kSmallPanel, m - p0), rows = m - p0;
+        for (int e = tid; e < rows * kSmallPanel; e += kSmallThreads) {
+            const int r = e / kSmallPanel, c = e % kSmallPanel;
+            P[r * kSmallLd + c] = c < pb && c <= r ? M[(size_t)(p0 + r) * ld + p0 + c] : 0.f;
+        }
+        __syncthreads();
+        // the panel, column by column: thread r holds panel row r in
+        // registers; per column the pivot's owner publishes it, every row
+        // below scales its entry and publishes it, then updates its row
+        {
+            const int r = tid;
+            const bool own = r < rows;
+            float row[kSmallPanel];
+#pragma unroll
+            for (int k = 0; k < kSmallPanel; ++k) row[k] = own ? P[r * kSmallLd + k] : 0.f;
+#pragma unroll
+            for (int c = 0; c < kSmallPanel; ++c) {   // unrolled: row[] indices are constants
+                if (c < pb) {                           // the same for the whole CTA
+                    if (r == c) piv_s = row[c];
+                    __syncthreads();
+                    const float d = __fsqrt_rn(piv_s);
+                    float lrc = 0.f;
+                    if (r == c) diag[c] = d;
+                    if (r > c && own) {
+                        lrc = __fdiv_rn(row[c], d);
+                        row[c] = lrc;
+                        col_s[r] = lrc;
+                    }
+                    __syncthreads();
+                    if (r > c && own) {
+#pragma unroll
+                        for (int k = c + 1; k < kSmallPanel; ++k)
+                            if (k < pb && k <= r) row[k] -= lrc * col_s[k];
+                    }
+                }
+            }
+            __syncthreads();
+            if (own) {
+#pragma unroll
+                for (int k = 0; k < kSmallPanel; ++k) P[r * kSmallLd + k] = row[k];
+            }
+            __syncthreads();
+        }
+        for (int e = tid; e < rows * kSmallPanel; e += kSmallThreads) {
+            const int r = e / kSmallPanel, c = e % kSmallPanel;
+            if (c < pb && c <= r) M[(size_t)(p0 + r) * ld + p0 + c] = r == c ? diag[c] : P[r * kSmallLd + c];
+        }
+        // trailing lower triangle: A22 -= L21 L21^T, 4 x 4 tiles (ti >= tj),
+        // consecutive threads along a tile row
+        const int n2 = rows - pb, nt = (n2 + 3) / 4, ntiles = nt * (nt + 1) / 2;
+        for (int t = tid; t < ntiles; t += kSmallThreads) {
+            int ti = (int)((sqrtf(8.f * (float)t + 1.f) - 1.f) * 0.5f);
+            while (ti * (ti + 1) / 2 > t) --ti;
+            while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+            const int tj = t - ti * (ti + 1) / 2;
+            float acc[4][4] = {};
+            const float* A = P + (size_t)(pb + 4 * ti) * kSmallLd;
+            const float* B = P + (size_t)(pb + 4 * tj) * kSmallLd;
+            for (int c = 0; c < pb; ++c) {
+                float a[4], b[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    a[u] = 4 * ti + u < n2 ? A[u * kSmallLd + c] : 0.f;
+                    b[u] = 4 * tj + u < n2 ? B[u * kSmallLd + c] : 0.f;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+#pragma unroll
+                    for (int v = 0; v < 4; ++v) acc[u][v] += a[u] * b[v];
+            }
+            // all sixteen entries loaded before any is stored (one L2 round trip)
+            float mv[4][4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int row = 4 * ti + u, col = 4 * tj + v;
+                    mv[u][v] = row < n2 && col <= row ? M[(size_t)(p0 + pb + row) * ld + p0 + pb + col] : 0.f;
+                }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int row = 4 * ti + u, col = 4 * tj + v;
+                    if (row < n2 && col <= row) M[(size_t)(p0 + pb + row) * ld + p0 + pb + col] = mv[u][v] - acc[u][v];
+                }
+        }
+        __syncthreads();
+    }
+}
+
 // integrateCholesky_L (bdhitea_kernel.cu:303-361): f_i = (D F)_i + sum_{q<=i}
 // B_iq (rho g)_q, then the fixed beads and the Ermak-McCammon move.
 __global__ void __launch_bounds__(kGridBlock)
@@ -394,6 +512,49 @@ k_chol_apply(JobDev* __restrict__ Jp, GridAux aux) {
                 f.z += acc[2];
             }
         }
+        if (J.pulling && J.flags[i] == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
+        const float4 xc = aux.xc[i];
+        const float dx = J.hOverZeta * f.x, dy = J.hOverZeta * f.y, dz = J.hOverZeta * f.z;
+        J.x[i] = make_float4(xc.x + dx, xc.y + dy, xc.z + dz, xc.w);
+        J.T[i] = J.T[i] + J.tempNorm * (dx * dx + dy * dy + dz * dz);
+    }
+}
+
+// integrateCholesky_L (bdhitea_kernel.cu:303-361) with the true factor at
+// n <= 128: a warp per bead; the lanes split the columns of the bead's three
+// rows of L (the noise vector rho g staged flat in shared memory), a fixed
+// xor-shuffle tree sums them, then (D F)_i, the fixed beads and the
+// Ermak-McCammon move as in k_chol_apply.
+constexpr int kApplyWarps = 8;
+__global__ void __launch_bounds__(32 * kApplyWarps)
+k_chol_apply_warp(JobDev* __restrict__ Jp, GridAux aux) {
+    __shared__ float gs[kSmallRows];
+    const JobDev& J = *Jp;
+    if (J.status) return;
+    const int n = J.n, ld = aux.ld, lane = threadIdx.x & 31;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const float4 g = aux.rf[q];
+        gs[3 * q] = g.x;
+        gs[3 * q + 1] = g.y;
+        gs[3 * q + 2] = g.z;
+    }
+    __syncthreads();
+    const float* M = aux.tensor;
+    const int i = blockIdx.x * kApplyWarps + (threadIdx.x >> 5);
+    if (i >= n) return;
+    float acc[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const int row = 3 * i + r;
+        const float* Lr = M + (size_t)row * ld;
+        float a = 0.f;
+        for (int c = lane; c <= row; c += 32) a += Lr[c] * gs[c];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        acc[r] = a;
+    }
+    if (lane == 0) {
+        const float4 dfi = aux.F[i];
+        float3 f = make_float3(dfi.x + acc[0], dfi.y + acc[1], dfi.z + acc[2]);
         if (J.pulling && J.flags[i] == FLAG_FIXED) f = make_float3(0.f, 0.f, 0.f);
         const float4 xc = aux.xc[i];
         const float dx = J.hOverZeta * f.x, dy = J.hOverZeta * f.y, dz = J.hOverZeta * f.z;

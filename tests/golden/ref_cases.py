@@ -114,6 +114,11 @@ CASES = {
     "speed_tea": dict(n=4000, sys_seed=4000, runs=1, total=20, dumps=[], speed=True, cfg={
         "run": "1", "seed": "777", "nav": "1000", "max_pairs": "1024", "max_possiblePairs": "4096",
         "hi_on": "yes", "hi_a": "3.8", "hi_unlisted": "yes", "hi_capricious": "no", "hi_epsilon_freq": "10"}),
+    # exact HI at the reference's largest size (CHOLSIZE = 3 x 128), the
+    # factor refreshed every step
+    "speed_exact": dict(n=128, sys_seed=29, runs=1, total=2000, dumps=[], speed=True, cfg={
+        "run": "1", "seed": "99", "nav": "1000", "max_pairs": "128", "max_possiblePairs": "128",
+        "hi_on": "yes", "hi_exact": "yes", "hi_a": "1.9"}),
     # the 198 000-bead shell indented by a 10 nm tip, 200 steps
     "speed_capsid": dict(n=198000, sys_seed=7, runs=1, total=200, dumps=[], speed=True, system="capsid", cfg={
         "run": "1", "seed": "5032015", "nav": "100", "pairs_threshold": "40.0", "max_possiblePairs": "2048",

@@ -67,8 +67,9 @@ def test_reference_noise_matrix_above_128_beads_is_unsupported(gpu_ctx):
     assert e.value.code == sopb.ERR_UNSUPPORTED
 
 
-@pytest.mark.parametrize("n", [129, 200, 451])
-def test_blocked_factor_matches_fp64_cholesky(gpu_ctx, n):
+@pytest.mark.parametrize("n", [20, 90, 128, 129, 200, 451])
+def test_factor_matches_fp64_cholesky(gpu_ctx, n):
+    # up to 128 beads the panel factor in one CTA, above it the tiled one
     sp = hi_spec(n, 37, "free", hi_exact=1)
     g = gpu_ctx.job(sp)
     x0 = g.read(sopb.COORDS)[:, :3].copy()

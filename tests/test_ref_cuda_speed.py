@@ -4,7 +4,8 @@ The reference's CUDA build (oracle/_ref/ref_gpu, compiled from the SOP-GPU
 tree for sm_100a by oracle/build_ref.sh) times its runGPU loop on the speed
 cases of tests/golden/ref_cases.py: the plain 200-bead ramp pull, 512
 force-clamp replicas of one 200-bead system (the reference runs replicas of
-one topology only) and TEA at 4000 beads.  The same configs go through this
+one topology only), TEA at 4000 beads, exact HI at 128 beads (the largest
+the reference runs) and the 198 000-bead capsid shell.  The same configs go through this
 library's C ABI on the same inputs.  Both sides are timed on the host around
 the whole loop with the device synchronised, set-up excluded.  Bar: this
 library is faster on every case.  With SOPB_SPEED_LOG set, the numbers are

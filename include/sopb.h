@@ -202,7 +202,10 @@ enum {
     SOPB_HISTATE = 7,  /* float[4]   TEA beta', epsilon (computeTEAeps), 0, 0 */
     SOPB_HIFACTOR = 8, /* float[9n^2] exact HI: the (3n)^2 tensor, row-major, */
                        /*            its lower triangle the Cholesky factor L */
-                       /*            of D at the last refresh (read only)     */
+                       /*            of D at the last refresh (read only);    */
+                       /*            the upper triangle is unspecified (the   */
+                       /*            reference-compatible noise mode keeps    */
+                       /*            the reference's mirrored factor there)   */
     SOPB_OBSERVABLES = 9 /* double[8] the .dat columns of the output manager,  */
                        /* computed on the device at the current coordinates: */
                        /* T (averaged over beads and the nav window), FENE,  */

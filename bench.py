@@ -78,15 +78,41 @@ def alg_bytes_per_bead_step(st, pairs_freq):
 FIGURES = os.path.join(REPO, "profiles", "ncu_figures.json")
 
 
+def strip_comments(src):
+    """C/C++/CUDA source without its comments and blank lines (string and
+    character literals kept), so that a comment edit leaves the hash of the
+    code unchanged."""
+    out, i, n = [], 0, len(src)
+    while i < n:
+        c = src[i]
+        if c in "\"'":
+            j = i + 1
+            while j < n and src[j] != c:
+                j += 2 if src[j] == "\\" else 1
+            out.append(src[i:j + 1])
+            i = j + 1
+        elif src.startswith("//", i):
+            j = src.find("\n", i)
+            i = n if j < 0 else j
+        elif src.startswith("/*", i):
+            j = src.find("*/", i + 2)
+            i = n if j < 0 else j + 2
+        else:
+            out.append(c)
+            i += 1
+    return "\n".join(l.rstrip() for l in "".join(out).splitlines() if l.strip())
+
+
 def source_hash():
+    """Hash of the CUDA sources' code (comments excluded)."""
     import hashlib
     h = hashlib.sha256()
     d = os.path.join(REPO, "sop-gpu_b200", "csrc")
     for f in sorted(os.listdir(d)):
         if f.endswith((".cu", ".cuh", ".cpp", ".h")):
             h.update(f.encode())
-            with open(os.path.join(d, f), "rb") as fh:
-                h.update(fh.read())
+            with open(os.path.join(d, f), encoding="utf-8") as fh:
+                h.update(strip_comments(fh.read()).encode())
     return h.hexdigest()[:16]
 
 

@@ -14,12 +14,13 @@
 // exclusions as a precomputed bitmask.  The Verlet list is a set of
 // bead-major, order-preserving index rows in global memory (the reference's
 // slot-major d_pairs transposed), cached in shared memory as a compact CSR
-// copy of u16 indices whenever the whole list fits the job's cache.  Both
+// copy (u16 byte offsets of the partners, in the lanes' order) as far as it
+// fits the job's cache.  Both
 // are rebuilt a warp per bead with ballots, so partners are always visited
 // in increasing j, the reference's list order.
 //
 // One step is two phases.  Forces: a group of `lpb` lanes (a power of two
-// <= 32, a whole warp by default) takes beads from a shared counter, strides
+// <= 32, four by default) takes beads from a shared counter, strides
 // over the bead's covalent, native and Verlet entries, combines the partial
 // forces with xor-shuffles and stores the bead's force in shared memory.
 // Integration: one thread per bead draws the noise and moves the bead.  A
@@ -136,10 +137,11 @@ __device__ __forceinline__ BondedView global_bonded(const JobDev& J) {
     return BondedView{J.cov_off, J.cov_j, J.cov_r0, J.nat_off, J.nat_j, J.nat_par};
 }
 
-// Verlet-pair terms of bead i, lane l of lpb taking entries l, l+lpb, ...
-// in that order, from the shared-memory cache when the list fits it, else
-// from the rows.  Four entries are fetched per iteration so four gathers are
-// in flight; the per-lane summation order is unchanged.
+// Verlet-pair terms of bead i from its global row (a bead beyond the
+// shared-memory cache, or forces outside a step), lane l of lpb taking
+// entries l, l+lpb, ... in that order.  Four entries are fetched per
+// iteration so four gathers are in flight; the per-lane summation order is
+// unchanged.
 template <typename Idx>
 __device__ __forceinline__ void pair_run(const JobDev& J, const float4* __restrict__ xs, const Idx* __restrict__ r,
                                          int cnt, float4 xi, int l, int lpb, float3& f) {

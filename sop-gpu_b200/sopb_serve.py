@@ -48,17 +48,24 @@ def on_grid_path(spec: "sopb.JobSpec") -> bool:
 
 def step_cost(spec: "sopb.JobSpec") -> float:
     """Device time of one step of a grid-path job alone, microseconds, on
-    B200 (sizes quanta and orders jobs): a per-step launch chain, all-pairs
-    O(n^2) sums for HI and, for exact HI, the factorisation amortised over
-    its refresh period, whose time is set by the chain of 3n/128 tile
-    columns (fitted to 85 us per TEA step and 2.1 ms per exact step with
-    refresh 10 at 4000 beads, 0.2 ms at 451 beads), O(n) otherwise."""
+    B200, which sizes a job's first quantum and orders jobs until its own
+    quanta have been timed: a per-step launch chain, all-pairs O(n^2) sums
+    for HI and, for exact HI, the factorisation amortised over its refresh
+    period -- up to 128 beads one CTA (about 0.023 n^2 us), above it the
+    chain of 3n/128 tile columns (about 3.8 n us) plus the O(n^2) apply --
+    (fitted to 66 us per TEA step and 1.79 ms per exact step with refresh 10
+    at 4000 beads, 71 and 224 us per exact step with refresh 1 at 40 and 90
+    beads), O(n) otherwise."""
     p, n = spec.params, float(spec.n)
     if not p.hi_on:
         return 20.0 + 5e-4 * n
-    cost = 40.0 + 3e-6 * n * n
+    cost = 40.0 + 2e-6 * n * n
     if p.hi_exact:
-        cost += 5.2 * n / max(1, int(p.hi_refresh))
+        refresh = max(1, int(p.hi_refresh))
+        if n <= 128:
+            cost += 25.0 + 0.023 * n * n / refresh
+        else:
+            cost += 8e-6 * n * n + 3.8 * n / refresh
     return cost
 
 
